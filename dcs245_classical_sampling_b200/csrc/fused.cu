@@ -1,0 +1,242 @@
+// Fused vertex steps over coset tiles in shared memory (complex64 tables, FP32 arithmetic).
+//
+// One launch = one group of consecutive vertex steps (see fused.py for the tile algebra).
+// Each CTA loops over tiles (persistent grid): it loads the entries of a tile that are
+// active before the group (128-byte rows of 2^low contiguous entries), applies every step of
+// the group in shared memory with the same orbit formulas as the per-step kernel
+// (reference: source/kernel_opt/inplace_gpu.py:29-58), and stores the entries that are
+// active after the group.  The power-of-two renormalisation is applied once per pass (on
+// load) from the previous pass's max; the pass's own max is reduced per CTA and published
+// with one atomicMax.
+#include <string.h>
+
+#include "common.cuh"
+
+using namespace dcs;
+
+namespace {
+
+constexpr int kMaxSteps = 24;
+constexpr int kThreads = 256;
+
+struct FusedStep {
+    uint64_t K, Ka, beta, enum_mask, pbit;
+    uint32_t tK, tKa, tpiv;
+    int32_t kind;
+    int32_t pidx;
+    int32_t pad;
+};
+
+struct FusedArgs {
+    int32_t count, tile_dim, low_bits, coset_m, ncoset_runs, group;
+    uint64_t in_mask_first, out_mask_last;
+    uint64_t basis[16];
+    uint32_t coset_runs[DCS_MAX_RUNS];
+    FusedStep st[kMaxSteps];
+};
+
+__device__ __forceinline__ float2 f2(float x, float y) { return make_float2(x, y); }
+
+__global__ void __launch_bounds__(kThreads)
+k_fused(float2* __restrict__ E, const __grid_constant__ FusedArgs A, const dcs_param* __restrict__ params,
+        unsigned long long* __restrict__ maxbits, dcs_scale* __restrict__ scale) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int T = 1 << A.tile_dim;
+    const int low = A.low_bits;
+    const int nhi = 1 << (A.tile_dim - low);
+    float2* sh = reinterpret_cast<float2*>(smem);
+    uint64_t* hi_tab = reinterpret_cast<uint64_t*>(smem + sizeof(float2) * (size_t)T);
+    __shared__ float4 fw[kMaxSteps];
+    __shared__ int ovy[kMaxSteps];
+
+    const double m2prev = (double)__uint_as_float((uint32_t)maxbits[A.group]);
+    const int e = scale_exponent(m2prev);
+    const float sc = (float)ldexp(1.0, -e);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        scale->logscale += (double)e * 0.69314718055994530942;
+        scale->exponent_sum += e;
+        if (!isfinite(m2prev)) scale->flags |= 1u;
+        else if (m2prev == 0.0) scale->flags |= 2u;
+    }
+    if (threadIdx.x < A.count) {
+        const dcs_param p = params[A.st[threadIdx.x].pidx];
+        fw[threadIdx.x] = make_float4((float)p.f0r, (float)p.f0i, (float)p.f1r, (float)p.f1i);
+        ovy[threadIdx.x] = (p.ov & 1) | ((p.y & 1) << 1);
+    }
+    for (int h = threadIdx.x; h < nhi; h += blockDim.x) {
+        uint64_t a = 0;
+        for (int i = 0; i < A.tile_dim - low; ++i)
+            if ((h >> i) & 1) a ^= A.basis[i];
+        hi_tab[h] = a;
+    }
+    __syncthreads();
+
+    const uint64_t lowmask = (1ull << low) - 1;
+    const uint64_t ntiles = 1ull << A.coset_m;
+    const uint64_t in_inactive = ~A.in_mask_first, out_inactive = ~A.out_mask_last;
+    float lm = 0.f;
+    for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const uint64_t base = deposit(tile, A.coset_runs, A.ncoset_runs);
+        // load (only entries active before the group; the rest are written before being read)
+        for (int t = threadIdx.x; t < T; t += kThreads) {
+            const uint64_t a = base ^ hi_tab[t >> low] ^ ((uint64_t)t & lowmask);
+            float2 v = f2(0.f, 0.f);
+            if (!(a & in_inactive)) {
+                v = E[a];
+                v.x *= sc;
+                v.y *= sc;
+            }
+            sh[t] = v;
+        }
+        __syncthreads();
+        for (int s = 0; s < A.count; ++s) {
+            const FusedStep& st = A.st[s];
+            const float4 w = fw[s];
+            const float2 f0 = f2(w.x, w.y), f1 = f2(w.z, w.w);
+            const int ov = ovy[s] & 1, y = ovy[s] >> 1;
+            const uint64_t notenum = ~st.enum_mask, beta = st.beta;
+            const int kind = st.kind;
+            for (int t = threadIdx.x; t < T; t += kThreads) {
+                const uint64_t a = base ^ hi_tab[t >> low] ^ ((uint64_t)t & lowmask);
+                if (a & notenum) continue;  // not an orbit representative of this step
+                const float2 x = sh[t];
+                switch (kind) {
+                    case DCS_KIND_GROW: {
+                        sh[t] = cmul(f0, x);
+                        sh[t ^ st.tpiv] = cmul(f1, cneg_if(x, neg_sign(a, beta, ov)));
+                    } break;
+                    case DCS_KIND_MIX: {
+                        const int td = t ^ st.tKa;
+                        const uint64_t d = a ^ st.Ka;
+                        const float2 b = sh[td];
+                        sh[t] = cadd(cmul(f0, x), cmul(f1, cneg_if(b, neg_sign(d, beta, ov))));
+                        sh[td] = cadd(cmul(f0, b), cmul(f1, cneg_if(x, neg_sign(a, beta, ov))));
+                    } break;
+                    case DCS_KIND_DIAG: {
+                        sh[t] = cmul(cadd(f0, cneg_if(f1, neg_sign(a, beta, ov))), x);
+                    } break;
+                    case DCS_KIND_REPLACE: {
+                        const int td = t ^ st.tK;
+                        const uint64_t d = a ^ st.K;
+                        const float2 b = sh[td];
+                        sh[t] = cmul(f0, cadd(x, b));
+                        sh[td] = cmul(f1, cadd(cneg_if(x, neg_sign(a, beta, ov)), cneg_if(b, neg_sign(d, beta, ov))));
+                    } break;
+                    case DCS_KIND_FIXED: {
+                        sh[t] = cmul(y ? cneg_if(f1, neg_sign(a, beta, ov)) : f0, x);
+                    } break;
+                    case DCS_KIND_FIXED_SHRINK: {
+                        const int td = t ^ st.tK;
+                        const uint64_t d = a ^ st.K;
+                        const float2 b = sh[td];
+                        sh[t] = y ? cmul(f1, cadd(cneg_if(x, neg_sign(a, beta, ov)), cneg_if(b, neg_sign(d, beta, ov))))
+                                  : cmul(f0, cadd(x, b));
+                    } break;
+                    case DCS_KIND_SHRINK4: {
+                        const int t1 = t ^ st.tK, td = t ^ st.tKa, td1 = td ^ st.tK;
+                        const uint64_t c1 = a ^ st.K, d = a ^ st.Ka, d1 = d ^ st.K;
+                        const float2 b = sh[t1], g = sh[td], h = sh[td1];
+                        sh[t] = cadd(cmul(f0, cadd(x, b)),
+                                     cmul(f1, cadd(cneg_if(g, neg_sign(d, beta, ov)), cneg_if(h, neg_sign(d1, beta, ov)))));
+                        sh[td] = cadd(cmul(f0, cadd(g, h)),
+                                      cmul(f1, cadd(cneg_if(x, neg_sign(a, beta, ov)), cneg_if(b, neg_sign(c1, beta, ov)))));
+                    } break;
+                    default: {  // DCS_KIND_SHRINK2
+                        const int td = t ^ st.tK;
+                        const uint64_t d = a ^ st.K;
+                        const float2 b = sh[td];
+                        sh[t] = cadd(cmul(cadd(f0, cneg_if(f1, neg_sign(a, beta, ov))), x),
+                                     cmul(cadd(f0, cneg_if(f1, neg_sign(d, beta, ov))), b));
+                    } break;
+                }
+            }
+            __syncthreads();
+        }
+        // store (only entries active after the group) and max
+        for (int t = threadIdx.x; t < T; t += kThreads) {
+            const uint64_t a = base ^ hi_tab[t >> low] ^ ((uint64_t)t & lowmask);
+            if (a & out_inactive) continue;
+            const float2 v = sh[t];
+            lm = fmaxf(lm, v.x * v.x + v.y * v.y);
+            E[a] = v;
+        }
+        __syncthreads();
+    }
+    const unsigned long long bm = block_max_u64(max_bits(lm));
+    if (threadIdx.x == 0 && bm) atomicMax(&maxbits[A.group + 1], bm);
+}
+
+}  // namespace
+
+extern "C" int dcs_fused_groups(void* table, const dcs_step* steps, int nsteps, const dcs_group* groups, int ngroups,
+                                const dcs_tile_step* tile_steps, const dcs_param* params, int g0, int ng,
+                                uint64_t* maxbits, dcs_scale* scale, void* stream) {
+    if (!table || !steps || !groups || !tile_steps || !params || !maxbits || !scale || g0 < 0 || ng < 0 ||
+        g0 + ng > ngroups) {
+        dcs_host::set_error("dcs_fused_groups: invalid arguments");
+        return DCS_E_ARG;
+    }
+    const int sms = dcs_host::sm_count();
+    if (sms <= 0) return DCS_E_CUDA;
+    cudaStream_t st = (cudaStream_t)stream;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+        dcs_host::set_error("dcs_fused_groups: no current device");
+        return DCS_E_CUDA;
+    }
+    static int max_smem_set[64] = {0};
+    for (int gi = g0; gi < g0 + ng; ++gi) {
+        const dcs_group& g = groups[gi];
+        if (g.count < 1 || g.count > kMaxSteps || g.first < 0 || g.first + g.count > nsteps || g.tile_dim < 0 ||
+            g.tile_dim > 14 || g.low_bits < 0 || g.low_bits > g.tile_dim || g.tile_dim - g.low_bits > 16 ||
+            g.ncoset_runs < 0 || g.ncoset_runs > DCS_MAX_RUNS || g.coset_m < 0 || g.coset_m > DCS_MAX_SLOTS) {
+            dcs_host::set_error("dcs_fused_groups: malformed group %d", gi);
+            return DCS_E_ARG;
+        }
+        FusedArgs A;
+        memset(&A, 0, sizeof(A));
+        A.count = g.count;
+        A.tile_dim = g.tile_dim;
+        A.low_bits = g.low_bits;
+        A.coset_m = g.coset_m;
+        A.ncoset_runs = g.ncoset_runs;
+        A.group = gi;
+        A.in_mask_first = steps[g.first].in_mask;
+        A.out_mask_last = g.out_mask;
+        for (int i = 0; i < 16; ++i) A.basis[i] = g.basis[i];
+        for (int r = 0; r < DCS_MAX_RUNS; ++r) A.coset_runs[r] = g.coset_runs[r];
+        for (int s = 0; s < g.count; ++s) {
+            const dcs_step& d = steps[g.first + s];
+            const dcs_tile_step& ts = tile_steps[g.step_tile_off + s];
+            FusedStep& f = A.st[s];
+            f.K = d.K; f.Ka = d.Ka; f.beta = d.beta; f.pbit = d.pivot_bit;
+            // orbit representatives: enumerated slots only (omitted pivots must be zero)
+            uint64_t en = 0;
+            for (int r = 0; r < d.nruns; ++r) {
+                const uint32_t w = d.runs[r];
+                const int dst = (w >> 8) & 255, len = (w >> 16) & 255;
+                en |= (len >= 64 ? ~0ull : ((1ull << len) - 1)) << dst;
+            }
+            f.enum_mask = en;
+            f.tK = ts.tK; f.tKa = ts.tKa; f.tpiv = ts.tpiv;
+            f.kind = d.kind;
+            f.pidx = g.first + s;
+        }
+        const size_t smem = sizeof(float2) * ((size_t)1 << g.tile_dim) +
+                            sizeof(uint64_t) * ((size_t)1 << (g.tile_dim - g.low_bits));
+        if (!max_smem_set[dev]) {
+            cudaError_t e = cudaFuncSetAttribute(k_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
+            if (e != cudaSuccess) return dcs_host::check_cuda(e, "k_fused smem attribute");
+            max_smem_set[dev] = 1;
+        }
+        const uint64_t ntiles = 1ull << g.coset_m;
+        int per_sm = (int)((220 * 1024) / (smem + 2048));
+        if (per_sm < 1) per_sm = 1;
+        if (per_sm > 8) per_sm = 8;
+        uint64_t grid = (uint64_t)sms * per_sm;
+        if (grid > ntiles) grid = ntiles;
+        k_fused<<<(unsigned)grid, kThreads, smem, st>>>((float2*)table, A, params, (unsigned long long*)maxbits, scale);
+        DCS_CHECK_LAUNCH("k_fused launch");
+    }
+    return DCS_OK;
+}

@@ -1,0 +1,385 @@
+"""Conditional-block engine on the B200: the drop-in for the reference's
+``InplaceConditionalBlockGPU`` (``source/sampling/conditional_block_inplace_gpu.py``,
+``source/sampling/conditional_block_gpu.py``).
+
+Same constructor ``(graph, unitaries, n, order, parity_operations, open_vertices)``, same
+``alloc(dtype, device)`` and ``block(x_bits, w=None, part=0, parts=1) -> (vector, meta)``,
+same errors.  The returned vector is a complex128 torch tensor on the engine's device,
+scaled by sqrt(2^(n-k)), index bit j <-> ``open_vertices[j]``.
+
+Execution modes (``alloc(..., mode=...)``):
+
+* ``"plain"``  — one launch per vertex step and a host read of the step's max after each
+  launch (the reference's control flow, ``kernel_opt/inplace_gpu.py:107-124``);
+* ``"device"`` — the renormalisation stays on the device; all steps of all slices are
+  enqueued without host synchronisation, several slices (work items) per launch when the
+  HBM budget allows (default);
+* ``"fused"``  — like ``device`` but several vertex steps per pass over the table
+  (coset-tiled fused kernel, complex64 only).
+
+Host work per block is the reference's bookkeeping (local vectors, slice coefficients,
+offset bits), vectorised over slices; the device does every pass over the tables.
+"""
+from __future__ import annotations
+
+import itertools
+import math
+import time
+
+import numpy as np
+import torch
+
+from . import _lib
+from .plan import (KIND_GROW, W_T, build_block_plan, deposit_runs, orbit_kind, slot_mask)
+
+LN2 = math.log(2.0)
+
+
+def device_steps(steps):
+    """OrbitStep list -> dcs_step array (host)."""
+    out = np.zeros(len(steps), dtype=_lib.STEP_DTYPE)
+    for i, st in enumerate(steps):
+        kind, omit = orbit_kind(st)
+        enum = [p for p in st.active_in if p not in omit]
+        runs = deposit_runs(slot_mask(enum))
+        if len(runs) > _lib.MAX_RUNS:
+            raise ValueError(f"step {i}: {len(runs)} deposit runs exceed {_lib.MAX_RUNS}")
+        r = out[i]
+        r["K"], r["Ka"], r["beta"] = st.K, st.Ka, st.beta
+        r["pivot_bit"] = (1 << st.pivot) if kind == KIND_GROW else 0
+        r["in_mask"], r["out_mask"] = slot_mask(st.active_in), slot_mask(st.active_out)
+        r["kind"], r["m"], r["nruns"], r["free_"] = kind, len(enum), len(runs), int(st.free)
+        for j, (src, dst, ln) in enumerate(runs):
+            r["runs"][j] = src | (dst << 8) | (ln << 16)
+    return out
+
+
+def pack_runs(slots):
+    runs = deposit_runs(slot_mask(slots))
+    arr = np.zeros(max(1, len(runs)), dtype=np.uint32)
+    for j, (src, dst, ln) in enumerate(runs):
+        arr[j] = src | (dst << 8) | (ln << 16)
+    return arr, len(runs)
+
+
+class SliceParams:
+    """Vectorised reference bookkeeping: per (prefix, slice) item, the per-step weights,
+    offset bits, slice coefficient and scatter xor (conditional_block_gpu.py:136-157,
+    inplace_gpu.py:111-114)."""
+
+    def __init__(self, plan):
+        p = self.plan = plan
+        self.nsteps = len(p.steps)
+        self.vert = np.array([st.v for st in p.steps], dtype=np.int64)         # reduced labels
+        self.free = np.array([st.free for st in p.steps], dtype=bool)
+        self.keep = np.array(p.keep, dtype=np.int64)
+        self.nslice = len(p.slices)
+        # reference vertices' bra . U (x-independent), data vertices' two rows
+        U = np.stack([np.asarray(p.U_full[q], np.complex128) for q in range(p.N_full)])
+        self.U = U
+        self.is_data = np.arange(p.N_full) < p.n
+        # neighbour-flip matrix: slice s -> kept vertices flipped
+        self.nbr = np.zeros((self.nslice, p.N), dtype=np.uint8)
+        for si, s in enumerate(p.slices):
+            for v in p.nbrs_in_keep[s]:
+                self.nbr[si, v] ^= 1
+        # fixed positions: offset contributions (bits of fut) before `stop` and the tail
+        fixed_pos = [j for j, st in enumerate(p.steps) if not st.free]
+        self.fixed_pos = np.array(fixed_pos, dtype=np.int64)
+        self.fixed_vert = self.vert[self.fixed_pos] if fixed_pos else np.zeros(0, np.int64)
+        F = np.zeros((len(fixed_pos), self.nsteps), dtype=np.uint8)
+        tail = np.zeros(len(fixed_pos), dtype=object)
+        for a, j in enumerate(fixed_pos):
+            fj = p.fut[j]
+            # bits at positions > j inside the step range; bits >= stop go to the final offset
+            for t in range(j + 1, self.nsteps):
+                if (fj >> t) & 1:
+                    F[a, t] = 1
+            tail[a] = fj >> p.stop
+        self.F = F
+        self.tail = tail
+        self.open_red = np.array(p.open_red, dtype=np.int64)
+        self.shift = (p.N_full - p.n + len(p.open_full)) * 0.5 * LN2
+
+    def full_vectors(self, x_bits, w=None):
+        """local_vectors for every full-graph vertex (scan_plan.py:108-120), shape (N_full, 2)."""
+        p = self.plan
+        f = np.empty((p.N_full, 2), dtype=np.complex128)
+        x = np.asarray(x_bits, dtype=np.int64)[: p.n]
+        f[: p.n] = self.U[np.arange(p.n), x]
+        if p.N_full > p.n:
+            refs = np.arange(p.n, p.N_full)
+            if isinstance(w, dict):
+                bras = np.stack([np.asarray(w[q], np.complex128) for q in refs])
+            else:
+                bras = np.broadcast_to(W_T if w is None else np.asarray(w, np.complex128), (len(refs), 2))
+            f[p.n:] = np.einsum("ri,rij->rj", bras, self.U[refs])
+        return f
+
+    def items(self, x_bits, w=None, part=0, parts=1):
+        """-> (count, list of slice items): each item = (coef, params (nsteps) PARAM_DTYPE, xor)."""
+        p = self.plan
+        ff = self.full_vectors(x_bits, w)
+        out = []
+        count = 0
+        for idx, bits in enumerate(itertools.product((0, 1), repeat=self.nslice)):
+            if idx % parts != part:
+                continue
+            count += 1
+            bits = np.array(bits, dtype=np.int64)
+            coef = complex(np.prod([ff[s][b] for s, b in zip(p.slices, bits)])) if self.nslice else 1 + 0j
+            par = sum(int(bits[p.slices.index(a)]) * int(bits[p.slices.index(b)]) for a, b in p.slice_edges)
+            coef *= (-1) ** par
+            if not coef:
+                continue
+            flips = (bits @ self.nbr) & 1 if self.nslice else np.zeros(p.N, dtype=np.int64)
+            f = ff[self.keep].copy()
+            f[:, 1] *= 1 - 2 * flips
+            params = np.zeros(self.nsteps, dtype=_lib.PARAM_DTYPE)
+            fs = f[self.vert]
+            params["f0r"], params["f0i"] = fs[:, 0].real, fs[:, 0].imag
+            params["f1r"], params["f1i"] = fs[:, 1].real, fs[:, 1].imag
+            xor_tail = 0
+            if len(self.fixed_pos):
+                y = (np.abs(f[self.fixed_vert, 0]) > 1e-12) == 0
+                params["y"][self.fixed_pos] = y.astype(np.int32)
+                ov = (y.astype(np.int64) @ self.F.astype(np.int64)) & 1
+                params["ov"] = ov.astype(np.int32)
+                for a in np.flatnonzero(y):
+                    xor_tail ^= int(self.tail[a])
+            freeflip = 0
+            for j, q in enumerate(self.open_red):
+                if flips[q]:
+                    freeflip |= 1 << j
+            out.append((coef, params, xor_tail ^ freeflip))
+        return count, out
+
+
+class InplaceConditionalBlockGPU:
+    """Drop-in for the reference engine of the same name (see module docstring)."""
+
+    def __init__(self, graph, unitaries, n, order, parity_operations, open_vertices):
+        self.plan = plan = build_block_plan(graph, unitaries, n, order, parity_operations, open_vertices)
+        # reference attribute surface (conditional_block_gpu.py:25-69)
+        self.N_full, self.n, self.N = plan.N_full, plan.n, plan.N
+        self.open_full, self.open_red = plan.open_full, plan.open_red
+        self.slices, self.slice_edges, self.nbrs_in_keep = plan.slices, plan.slice_edges, plan.nbrs_in_keep
+        self.relabel, self.keep, self.U_full = plan.relabel, plan.keep, plan.U_full
+        self.edges, self.order, self.fixed, self.fut = plan.edges, plan.order, plan.fixed, plan.fut
+        self.stop, self.rmax, self.work = plan.stop, plan.rmax, plan.work
+        self.open_edges = plan.open_edges
+        self.terminal_basis = plan.terminal_basis
+        self.terminal_rank = plan.terminal_rank
+        self.params = SliceParams(plan)
+        self._alloc = False
+
+    # ------------------------------------------------------------------ allocation
+    def alloc(self, dtype=np.complex64, device=0, fp64_kernel_path=None, mode="device", items=None,
+              hbm_budget=None):
+        """Allocate device buffers (conditional_block_inplace_gpu.py:18-34).
+
+        dtype: complex64 (FP32 arithmetic) or complex128 (FP64 arithmetic).
+        items: concurrent work items (slices) per launch; default = as many slices as fit
+        in the HBM budget (default 85% of free device memory)."""
+        if np.dtype(dtype) not in (np.dtype(np.complex64), np.dtype(np.complex128)):
+            raise ValueError(dtype)
+        if mode not in ("plain", "device", "fused"):
+            raise ValueError(mode)
+        if mode == "fused" and np.dtype(dtype) != np.dtype(np.complex64):
+            raise ValueError("the fused executor stores complex64 tables")
+        self.lib = _lib.load()
+        if not torch.cuda.is_available():
+            raise RuntimeError("InplaceConditionalBlockGPU needs a CUDA device")
+        self.device = torch.device("cuda", device)
+        torch.cuda.set_device(self.device)
+        self.mode = mode
+        self.inplace_fp64 = self.use_fp64 = np.dtype(dtype) == np.dtype(np.complex128)
+        self.dcode = _lib.C128 if self.use_fp64 else _lib.C64
+        plan = self.plan
+        self.inplace_steps = plan.steps
+        self.inplace_maxslots = plan.maxslots
+        self.inplace_rmax = plan.inplace_rmax
+        self.inplace_terminal_basis = dict(zip(plan.terminal_slots, plan.terminal_basis))
+        self.dsteps = device_steps(plan.steps)
+        self.nsteps = len(plan.steps)
+        tdtype = torch.complex128 if self.use_fp64 else torch.complex64
+        entry = 16 if self.use_fp64 else 8
+        table_entries = 1 << plan.maxslots
+        nslice_items = 1 << len(plan.slices)
+        if items is None:
+            free, _ = torch.cuda.mem_get_info(self.device)
+            budget = int((hbm_budget if hbm_budget is not None else 0.85 * free))
+            items = max(1, min(nslice_items, budget // (table_entries * entry)))
+        self.items = int(items)
+        if mode == "fused":
+            from .fused import build_fused_plan
+            self.fplan = build_fused_plan(plan)
+            self.items = 1
+        self.table = torch.empty(self.items * table_entries, dtype=tdtype, device=self.device)
+        self.table_stride = table_entries
+        self.maxbits = torch.zeros(self.items * (self._nmax() + 1), dtype=torch.int64, device=self.device)
+        self.scale = torch.zeros(self.items * _lib.SCALE_DTYPE.itemsize // 8, dtype=torch.int64,
+                                 device=self.device)
+        self.d_params = torch.zeros(self.items * self.nsteps * _lib.PARAM_DTYPE.itemsize // 8, dtype=torch.int64,
+                                    device=self.device)
+        self.one_bits = (np.array([1.0], np.float64).view(np.int64)[0] if self.use_fp64
+                         else int(np.array([1.0], np.float32).view(np.uint32)[0]))
+        self.term_runs, self.term_nruns = pack_runs(plan.terminal_slots)
+        self.tbasis = np.array(plan.terminal_basis + [0], dtype=np.uint64)
+        k = len(plan.open_full)
+        self.k = k
+        adj = np.zeros(max(1, k), dtype=np.uint32)
+        for a, b in plan.open_edges:
+            lo, hi = (a, b) if a < b else (b, a)
+            adj[lo] |= np.uint32(1 << hi)
+        self.adj_hi = adj
+        u = np.zeros((max(1, k), 8), dtype=np.float64)
+        for q, orig in enumerate(plan.open_full):
+            m = np.asarray(plan.U_full[orig], np.complex128)
+            u[q] = [m[0, 0].real, m[0, 0].imag, m[0, 1].real, m[0, 1].imag,
+                    m[1, 0].real, m[1, 0].imag, m[1, 1].real, m[1, 1].imag]
+        self.u_open = u
+        self._alloc = True
+        self.buf = True
+
+    def _nmax(self):
+        return len(self.fplan.groups) if self.mode == "fused" else self.nsteps
+
+    # ------------------------------------------------------------------ execution
+    def _stream(self):
+        return torch.cuda.current_stream(self.device).cuda_stream
+
+    def _reset_items(self, n_items):
+        nm = self._nmax() + 1
+        mb = self.maxbits.view(self.items, nm)
+        mb[:n_items].zero_()
+        mb[:n_items, 0] = self.one_bits
+        self.scale.view(self.items, -1)[:n_items].zero_()
+        # empty environment = 1 at address 0 of every item (inplace_gpu.py:108)
+        self.table.view(self.items, self.table_stride)[:n_items, 0] = 1
+
+    def _upload_params(self, plist):
+        host = np.concatenate(plist).view(np.int64)
+        t = torch.from_numpy(host).pin_memory()
+        self.d_params[: host.size].copy_(t, non_blocking=True)
+        return t  # keep the pinned buffer alive until the copy is consumed
+
+    def _run_steps(self, n_items):
+        lib, st = self.lib, self._stream()
+        nm = self._nmax() + 1
+        if self.mode == "fused":
+            f = self.fplan
+            _lib.check(lib.dcs_fused_groups(_lib.ptr(self.table), f.dsteps.ctypes.data, len(f.dsteps),
+                                            f.groups.ctypes.data, len(f.groups), f.tile_steps.ctypes.data,
+                                            _lib.ptr(self.d_params), 0, len(f.groups), _lib.ptr(self.maxbits),
+                                            _lib.ptr(self.scale), st))
+            return True
+        if self.mode == "plain":
+            mb = self.maxbits.view(self.items, nm)
+            for s in range(self.nsteps):
+                _lib.check(lib.dcs_slice_steps_batched(
+                    self.dcode, _lib.ptr(self.table), self.table_stride, self.dsteps.ctypes.data,
+                    _lib.ptr(self.d_params), self.nsteps, self.nsteps, s, 1, _lib.ptr(self.maxbits),
+                    _lib.ptr(self.scale), n_items, st))
+                bits = mb[:n_items, s + 1].cpu().numpy()  # host sync per step, as the reference
+                m2 = (bits.view(np.float64) if self.use_fp64 else bits.astype(np.uint32).view(np.float32))
+                if not np.all(np.isfinite(m2)):
+                    raise ArithmeticError("Nonfinite in-place environment")
+                if np.all(m2 == 0):
+                    return False
+            return True
+        _lib.check(lib.dcs_slice_steps_batched(
+            self.dcode, _lib.ptr(self.table), self.table_stride, self.dsteps.ctypes.data, _lib.ptr(self.d_params),
+            self.nsteps, self.nsteps, 0, self.nsteps, _lib.ptr(self.maxbits), _lib.ptr(self.scale), n_items, st))
+        return True
+
+    def _accumulate(self, items, total, nblocks_items):
+        """items: list of (coef, xor); nblocks_items: item_begin array (len nblocks+1)."""
+        lib = self.lib
+        n = len(items)
+        coefs = np.zeros(2 * max(1, n), np.float64)
+        xors = np.zeros(max(1, n), np.uint64)
+        for i, (c, x) in enumerate(items):
+            coefs[2 * i], coefs[2 * i + 1] = c.real, c.imag
+            xors[i] = x
+        dev = self.device
+        d_coefs = torch.from_numpy(coefs).to(dev, non_blocking=False)
+        d_xors = torch.from_numpy(xors.view(np.int64)).to(dev)
+        d_begin = torch.from_numpy(np.asarray(nblocks_items, np.int32)).to(dev)
+        nm = self._nmax() + 1
+        _lib.check(lib.dcs_accumulate_batched(
+            self.dcode, _lib.ptr(self.table), self.table_stride, self.plan.terminal_rank, self.term_runs.ctypes.data,
+            self.term_nruns, self.tbasis.ctypes.data, _lib.ptr(d_xors), _lib.ptr(d_coefs), _lib.ptr(d_begin),
+            len(nblocks_items) - 1, self.params.shift, _lib.ptr(self.scale),
+            _lib.ptr(self.maxbits[nm - 1:]), nm, _lib.ptr(total), self.k, n, self._stream()))
+        return d_coefs, d_xors, d_begin
+
+    def _check_flags(self, n_items):
+        sc = self.scale.view(self.items, -1)[:n_items].cpu().numpy().view(_lib.SCALE_DTYPE)
+        if np.any(sc["flags"] & 1):
+            raise ArithmeticError("Nonfinite in-place environment")
+
+    def block(self, x_bits, w=None, part=0, parts=1):
+        """Scaled conditional amplitudes of one prefix (conditional_block_gpu.py:128-177)."""
+        if not self._alloc:
+            self.alloc()
+        start = time.perf_counter()
+        k = self.k
+        total = torch.zeros(1 << k, dtype=torch.complex128, device=self.device)
+        count, items = self.params.items(x_bits, w, part, parts)
+        keep = []
+        for b0 in range(0, len(items), self.items):
+            chunk = items[b0:b0 + self.items]
+            self._reset_items(len(chunk))
+            hold = self._upload_params([it[1] for it in chunk])
+            ok = self._run_steps(len(chunk))
+            if ok:
+                keep.append(self._accumulate([(c, x) for c, _, x in chunk], total.view(torch.float64),
+                                             [0, len(chunk)]))
+            self._check_flags(len(chunk))
+            del hold
+        _lib.check(self.lib.dcs_block_tail(_lib.ptr(total), k, self.adj_hi.ctypes.data, self.u_open.ctypes.data, 1,
+                                           self._stream()))
+        torch.cuda.current_stream(self.device).synchronize()
+        return total, self._meta(time.perf_counter() - start, part, parts, count)
+
+    def _meta(self, seconds, part, parts, count):
+        return {"seconds": seconds, "part": part, "parts": parts, "slices_evaluated": count,
+                "prefix_dtype": "complex128" if self.use_fp64 else "complex64", "rmax": self.rmax,
+                "terminal_rank": self.terminal_rank, "work_per_slice": self.work,
+                "open_vertices": self.open_full,
+                "vector_scale": "sqrt(2^(n-k)); sum all complex parts before probabilities"}
+
+    # ------------------------------------------------------------------ batched prefixes
+    def blocks(self, x_list, w=None):
+        """Blocks of many prefixes: (prefix, slice) work items share launches.
+
+        Returns a complex128 tensor (len(x_list), 2^k) on the device."""
+        if not self._alloc:
+            self.alloc()
+        k = self.k
+        out = torch.zeros((len(x_list), 1 << k), dtype=torch.complex128, device=self.device)
+        work = []  # (block index, coef, params, xor)
+        for b, x in enumerate(x_list):
+            _, items = self.params.items(x, w)
+            work.extend((b, c, p, xo) for c, p, xo in items)
+        keep = []
+        for b0 in range(0, len(work), self.items):
+            chunk = work[b0:b0 + self.items]
+            self._reset_items(len(chunk))
+            hold = self._upload_params([it[2] for it in chunk])
+            self._run_steps(len(chunk))
+            # items of one launch are grouped by block in order; accumulate per block range
+            blocks_in = sorted(set(it[0] for it in chunk))
+            begin = [0]
+            for bb in blocks_in:
+                begin.append(begin[-1] + sum(1 for it in chunk if it[0] == bb))
+            lo, hi = blocks_in[0], blocks_in[-1]
+            assert blocks_in == list(range(lo, hi + 1))
+            keep.append(self._accumulate([(c, xo) for _, c, _, xo in chunk],
+                                         out[lo:hi + 1].view(torch.float64), begin))
+            self._check_flags(len(chunk))
+            del hold
+        _lib.check(self.lib.dcs_block_tail(_lib.ptr(out), k, self.adj_hi.ctypes.data, self.u_open.ctypes.data,
+                                           len(x_list), self._stream()))
+        return out

@@ -1,0 +1,183 @@
+"""Fused plan: several vertex steps per pass over the table, staged in shared memory.
+
+Every vertex step updates disjoint orbits {c, c^K, c^Ka, c^Ka^K} or {c, c|pivot}.  For a run
+of consecutive steps, let W be the GF(2) span of all their orbit vectors (K, Ka, grow pivot)
+plus the unit vectors of the lowest table slots (so that each tile row is a contiguous,
+aligned run of 2^low entries in HBM).  The cosets base ^ W partition the table and are closed
+under every orbit map of those steps, so each coset ("tile", 2^dim entries) can be loaded into
+shared memory once, pushed through all the steps, and written back once: HBM traffic drops
+from one read+write per step to one per group.
+
+Tile coordinates: W gets a reduced echelon basis — the low unit vectors e_0..e_{l-1}, then
+vectors w_i with distinct top bits p_i and no other basis vector touching p_i or a low bit.
+A vector v of W has coordinate bit(v, i) on e_i and bit(v, p_i) on w_i.  Coset bases are
+the table addresses that are zero on every pivot and low bit and lie in the group's slot
+universe U.  Entries are loaded only if active before the group and stored only if active
+after it; everything else inside a tile is written by a grow before any read (the grow
+pivot is in W), so the algorithmic bytes are 2^|in(first)| + 2^|out(last)| entries.
+
+The grouping is greedy: extend while dim W <= max_dim, |U| <= (largest rank in the group)
++ max_extra and the group has at most max_steps steps (bounding the growth of un-renormalised
+values inside a pass).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+from .engine import device_steps
+from .plan import KIND_GROW, deposit_runs, orbit_kind, slot_mask
+
+MAX_GROUP_STEPS = 24
+MAX_BASIS = 16
+
+
+def _orbit_vectors(st):
+    kind, _ = orbit_kind(st)
+    if kind == KIND_GROW:
+        return [1 << st.pivot]
+    vecs = []
+    if st.K and kind in (3, 5, 6, 7):
+        vecs.append(st.K)
+    if st.Ka and kind in (1, 6):
+        vecs.append(st.Ka)
+    return vecs
+
+
+def _low_bits(U, limit):
+    l = 0
+    while l < limit and (U >> l) & 1:
+        l += 1
+    return l
+
+
+def _reduced_basis(vectors, low):
+    """Reduced echelon basis (pivot = top bit) of span(vectors) with the low bits cleared."""
+    lowmask = (1 << low) - 1
+    piv = {}
+    for v in vectors:
+        v &= ~lowmask
+        while v:
+            t = v.bit_length() - 1
+            if t in piv:
+                v ^= piv[t]
+            else:
+                piv[t] = v
+                break
+    # full reduction: clear every pivot bit from the other vectors
+    keys = sorted(piv)
+    for t in keys:
+        for o in keys:
+            if o != t and (piv[o] >> t) & 1:
+                piv[o] ^= piv[t]
+    return [piv[t] for t in keys], keys
+
+
+def _dim(vectors, low):
+    return low + len(_reduced_basis(vectors, low)[0])
+
+
+@dataclass
+class FusedPlan:
+    groups: np.ndarray
+    tile_steps: np.ndarray
+    dsteps: np.ndarray
+    spans: list = field(default_factory=list)      # (first, count) per group
+    universe: list = field(default_factory=list)   # |U| per group
+    tiles: list = field(default_factory=list)      # tile count per group
+    dims: list = field(default_factory=list)
+
+    def algorithmic_bytes(self, plan, elem=8):
+        tot = 0
+        for first, count in self.spans:
+            tot += ((1 << len(plan.steps[first].active_in)) + (1 << len(plan.steps[first + count - 1].active_out))) * elem
+        return tot
+
+
+def group_steps(steps, max_dim=13, low=4, max_steps=MAX_GROUP_STEPS, max_extra=1):
+    """Greedy grouping -> list of (first, count)."""
+    spans = []
+    j = 0
+    S = len(steps)
+    while j < S:
+        vecs, U, rank = [], 0, 0
+        count = 0
+        while j + count < S and count < max_steps:
+            st = steps[j + count]
+            U2 = U | slot_mask(st.active_in) | slot_mask(st.active_out) | (
+                (1 << st.pivot) if orbit_kind(st)[0] == KIND_GROW else 0)
+            r2 = max(rank, len(st.active_in), len(st.active_out))
+            v2 = vecs + _orbit_vectors(st)
+            l2 = _low_bits(U2, low)
+            if count and (_dim(v2, l2) > max_dim or bin(U2).count("1") > r2 + max_extra):
+                break
+            vecs, U, rank = v2, U2, r2
+            count += 1
+        spans.append((j, count))
+        j += count
+    return spans
+
+
+def build_fused_plan(plan, max_dim=13, low=4, max_steps=MAX_GROUP_STEPS, max_extra=1, spans=None):
+    steps = plan.steps
+    if spans is None:
+        spans = group_steps(steps, max_dim, low, max_steps, max_extra)
+    groups = np.zeros(len(spans), dtype=_lib.GROUP_DTYPE)
+    tsteps = np.zeros(len(steps), dtype=_lib.TILE_STEP_DTYPE)
+    fp = FusedPlan(groups=groups, tile_steps=tsteps, dsteps=device_steps(steps), spans=list(spans))
+    for gi, (first, count) in enumerate(spans):
+        U = 0
+        vecs = []
+        for st in steps[first:first + count]:
+            U |= slot_mask(st.active_in) | slot_mask(st.active_out)
+            if orbit_kind(st)[0] == KIND_GROW:
+                U |= 1 << st.pivot
+            vecs += _orbit_vectors(st)
+        l = _low_bits(U, low)
+        basis, pivots = _reduced_basis(vecs, l)
+        if len(basis) > MAX_BASIS:
+            raise ValueError(f"group {gi}: {len(basis)} tile basis vectors exceed {MAX_BASIS}")
+        dim = l + len(basis)
+        for b in basis:
+            if b & ~U:
+                raise AssertionError("tile basis leaves the slot universe")
+        lowmask = (1 << l) - 1
+        cmask = U & ~lowmask
+        for p in pivots:
+            cmask &= ~(1 << p)
+        runs = deposit_runs(cmask)
+        if len(runs) > _lib.MAX_RUNS:
+            raise ValueError(f"group {gi}: {len(runs)} coset runs exceed {_lib.MAX_RUNS}")
+
+        def coords(v):
+            t = v & lowmask
+            acc = v & lowmask
+            for i, (b, p) in enumerate(zip(basis, pivots)):
+                if (v >> p) & 1:
+                    t |= 1 << (l + i)
+                    acc ^= b
+            if acc != v:
+                raise AssertionError("orbit vector outside the tile space")
+            return t
+
+        g = groups[gi]
+        g["first"], g["count"], g["tile_dim"], g["low_bits"] = first, count, dim, l
+        g["coset_m"], g["ncoset_runs"], g["step_tile_off"] = bin(cmask).count("1"), len(runs), first
+        g["out_mask"] = slot_mask(steps[first + count - 1].active_out)
+        for i, b in enumerate(basis):
+            g["basis"][i] = b
+        for r, (src, dst, ln) in enumerate(runs):
+            g["coset_runs"][r] = src | (dst << 8) | (ln << 16)
+        for s in range(first, first + count):
+            st = steps[s]
+            kind, _ = orbit_kind(st)
+            ts = tsteps[s]
+            ts["tK"] = coords(st.K) if kind in (3, 5, 6, 7) else 0
+            ts["tKa"] = coords(st.Ka) if kind in (1, 6) else 0
+            ts["tpiv"] = coords(1 << st.pivot) if kind == KIND_GROW else 0
+        fp.universe.append(bin(U).count("1"))
+        fp.tiles.append(1 << bin(cmask).count("1"))
+        fp.dims.append(dim)
+    return fp

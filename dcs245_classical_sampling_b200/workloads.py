@@ -1,0 +1,138 @@
+"""Seeded synthetic workloads standing in for the reference's circuits.
+
+Each workload is a seeded ring circuit (``circuits.ring_circuit``) with the
+stated qubit count, depth and T count, turned into an injected graph, plus the
+contraction order, the open (free) vertices and the parity operations.
+
+Order: the data qubits are swept outward from the ring position opposite the
+open arc, in both directions, each followed by its reference vertices (the
+reference's real order has the same shape: ``inputs/injected_graph.npz``
+``order`` starts opposite its open arc and ends on it).  The open vertices are
+the last k ring qubits.  Parity operations come from ``plan.choose_parity_slices``
+restricted to reference vertices and are cached in ``workloads.json`` so that
+machines running the bench do not repeat the greedy search.
+"""
+from __future__ import annotations
+
+import json
+from pathlib import Path
+
+import numpy as np
+
+from .circuits import build_ring_instance
+from .plan import choose_parity_slices
+
+HERE = Path(__file__).resolve().parent
+CACHE = HERE / "workloads.json"
+
+# name: (n qubits, depth, T count, circuit seed, open bits k, parity slices)
+WORKLOADS = {
+    "ring16_d20_t24_k8": (16, 20, 24, 1016, 8, 1),
+    "ring24_d24_t60_k10": (24, 24, 60, 1024, 10, 2),
+    "ring40_d45_t190_k16": (40, 45, 190, 1040, 16, 1),
+    "ring32_d37_t79_k14": (32, 37, 79, 1032, 14, 0),
+    "ring48_d55_t177_k17": (48, 55, 177, 1048, 17, 0),
+    "ring64_d73_t314_k20": (64, 73, 314, 1064, 20, 2),
+}
+
+
+def sweep_order(inst, open_vertices):
+    """Bidirectional ring sweep from the antipode of the open arc; references follow their qubit."""
+    n = int(inst["n"]) if "n" in inst else len(inst["ring"])
+    refs = {}
+    cur = None
+    for v in inst["natural_order"]:
+        v = int(v)
+        if v < n:
+            cur = v
+            refs[v] = []
+        else:
+            refs[cur].append(v)
+    openv = list(open_vertices)
+    k = len(openv)
+    center = (openv[0] + k // 2 + n // 2) % n if k else 0
+    def key(q):
+        return (min((q - center) % n, (center - q) % n), (q - center) % n)
+    order = []
+    for q in sorted(range(n), key=key):
+        order.append(q)
+        order.extend(refs[q])
+    return order
+
+
+def _edges(A):
+    return [(int(a), int(b)) for a, b in zip(*np.nonzero(np.triu(A, 1)))]
+
+
+def choose_reference_slices(A, n, order, count, open_vertices=(), seed=0):
+    """Greedy parity slices among reference vertices only (the engine refuses data vertices)."""
+    if count == 0:
+        return []
+    N = len(A)
+    # run the chooser on the graph whose data vertices are protected by removing them from
+    # the candidate window: they stay in the order, but every chosen op must be on w >= n.
+    ops = []
+    B = np.asarray(A, dtype=np.uint8).copy()
+    alive = list(order)
+    from .plan import apply_parity_operation, prefix_cut_ranks
+    rng = np.random.default_rng(seed)
+    for _ in range(count):
+        r = prefix_cut_ranks(B, alive)
+        m = int(r.max())
+        hot = [i for i, x in enumerate(r) if x == m]
+        lo, hi = max(0, min(hot) - 15), min(len(alive), max(hot) + 17)
+        cand = [w for w in alive[lo:hi] if w >= n]
+        if len(cand) > 60:
+            cand = list(rng.choice(cand, 60, replace=False))
+        best = None
+        alive_set = set(alive)
+        for w in cand:
+            rest = [x for x in alive if x != w]
+            trials = [("Z", w, None), ("Y", w, None)]
+            nb = [u for u in np.nonzero(B[w])[0] if u in alive_set]
+            for u in (rng.choice(nb, min(4, len(nb)), replace=False) if nb else []):
+                trials.append(("X", w, int(u)))
+            for kind, ww, u in trials:
+                C = B.copy()
+                apply_parity_operation(C, None, kind, ww, u)
+                rr = prefix_cut_ranks(C, rest)
+                mm = int(rr.max())
+                c = (mm, float(np.sum(2.0 ** (rr - mm))))
+                if best is None or c < best[0]:
+                    best = (c, kind, int(ww), u)
+        _, kind, w, u = best
+        apply_parity_operation(B, None, kind, w, u)
+        ops.append((kind, w, None if u is None else int(u)))
+        alive = [x for x in alive if x != w]
+    return ops
+
+
+def _load_cache():
+    if CACHE.exists():
+        return json.loads(CACHE.read_text())
+    return {}
+
+
+def build_workload(name, use_cache=True):
+    """-> dict(graph, unitaries, n, order, parity_operations, open_vertices, ring, meta)."""
+    n, depth, t, seed, k, npar = WORKLOADS[name]
+    inst = build_ring_instance(n, depth, t, seed)
+    openv = list(range(n - k, n))
+    order = sweep_order(inst, openv)
+    cache = _load_cache() if use_cache else {}
+    if name in cache:
+        ops = [tuple(op) for op in cache[name]["parity_operations"]]
+    else:
+        ops = choose_reference_slices(inst["graph"], n, order, npar, openv)
+    return {"name": name, "graph": inst["graph"], "unitaries": inst["unitaries"], "n": n,
+            "order": order, "parity_operations": [list(op) for op in ops], "open_vertices": openv,
+            "ring": inst["ring"], "depth": depth, "t_count": t, "seed": seed, "N": int(inst["N"])}
+
+
+def refresh_cache(names=None):
+    cache = _load_cache()
+    for name in names or WORKLOADS:
+        w = build_workload(name, use_cache=False)
+        cache[name] = {"parity_operations": w["parity_operations"]}
+    CACHE.write_text(json.dumps(cache, indent=1) + "\n")
+    return cache

@@ -1,0 +1,221 @@
+/*
+ * dcs245.h — C ABI of the B200 conditional-block contraction and free-bit sampler.
+ *
+ * Plain C: pointers, sizes and POD structs only.  Every entry point returns 0
+ * on success or a negative DCS_E_* code; dcs_last_error() gives the message of
+ * the last failure on the calling thread.  No C++ exception crosses the ABI.
+ * All device pointers are CUDA global-memory pointers of the current device;
+ * `stream` is a cudaStream_t (NULL = legacy default stream).  All work is
+ * enqueued asynchronously on `stream` unless stated otherwise.
+ *
+ * Reference interfaces replaced (paths inside the reference project):
+ *   dcs_inplace_step      kernel `inplace_step` + its launch,
+ *                         source/kernel_opt/inplace_gpu.py:20-63 and :117-119
+ *   dcs_slice_steps       the per-step host loop `prefix_inplace`,
+ *                         source/kernel_opt/inplace_gpu.py:107-124
+ *                         (renormalisation kept on the device, no host sync)
+ *   dcs_fused_groups      same loop, several steps per pass over the table
+ *   dcs_accumulate        terminal gather + syndrome scatter + coherent slice sum,
+ *                         source/kernel_opt/inplace_gpu.py:124 and
+ *                         source/sampling/conditional_block_gpu.py:155-158
+ *   dcs_block_tail        Walsh-Hadamard, open-edge phase and U_open passes,
+ *                         source/sampling/conditional_block_gpu.py:159-171
+ *   dcs_draw              FP64 CDF draw `draw_checked`,
+ *                         source/sampling/sampling_protocol.py:44-88
+ */
+#ifndef DCS245_H
+#define DCS245_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* the library is built with hidden visibility; everything declared here is exported */
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+#define DCS_ABI_VERSION 1
+
+/* error codes */
+#define DCS_OK 0
+#define DCS_E_ARG -1      /* invalid argument (size, kind, alignment, range) */
+#define DCS_E_CUDA -2     /* a CUDA runtime call failed */
+#define DCS_E_NONFINITE -3 /* nonfinite table (reference: ArithmeticError) */
+#define DCS_E_CDF -4      /* zero / nonfinite block or invalid outcome (reference: ArithmeticError) */
+
+/* storage types of the in-place table */
+#define DCS_C64 0  /* float2: complex64 storage, FP32 arithmetic */
+#define DCS_C128 1 /* double2: complex128 storage, FP64 arithmetic */
+
+/* orbit kinds (same numbering as the reference kernel's `kind`) */
+#define DCS_KIND_GROW 0
+#define DCS_KIND_MIX 1
+#define DCS_KIND_DIAG 2
+#define DCS_KIND_REPLACE 3
+#define DCS_KIND_FIXED 4
+#define DCS_KIND_FIXED_SHRINK 5
+#define DCS_KIND_SHRINK4 6
+#define DCS_KIND_SHRINK2 7
+
+#define DCS_MAX_RUNS 28
+#define DCS_MAX_SLOTS 40
+
+/* One vertex step of the preserved-coordinate plan (static per plan; HOST memory: the
+ * library passes it to the kernel by value, so a captured CUDA graph keeps it).
+ * Orbit representatives are enumerated by depositing x in [0, 2^m) into the slots of
+ * enum_mask; the deposit is stored as runs: run r copies `len` bits of x starting at bit
+ * `src` to bits starting at `dst` (packed src | dst << 8 | len << 16). */
+typedef struct dcs_step {
+    uint64_t K;        /* kernel vector (slot mask) */
+    uint64_t Ka;       /* Pauli shift (slot mask) */
+    uint64_t beta;     /* sign mask: parity(c & beta) */
+    uint64_t pivot_bit;/* grow: 1 << pivot; else 0 */
+    uint64_t in_mask;  /* active_in slots */
+    uint64_t out_mask; /* active_out slots */
+    int32_t kind;      /* DCS_KIND_* */
+    int32_t m;         /* log2 of the number of orbits */
+    int32_t nruns;
+    int32_t free_;     /* vertex is free (not structurally fixed) */
+    uint32_t runs[DCS_MAX_RUNS];
+} dcs_step;
+
+/* Per-(slice, step) contraction weights and offset bits (built on the host per block). */
+typedef struct dcs_param {
+    double f0r, f0i, f1r, f1i; /* f_v = (f0, f1) */
+    int32_t ov;                /* offset bit of this position */
+    int32_t y;                 /* fixed value (fixed kinds only) */
+} dcs_param;
+
+/* Device-resident renormalisation state of one work item (one slice of one prefix).
+ * maxbits[s] holds the bit pattern of max|x|^2 written by step s-1 (float bits in the low
+ * 32 bits for DCS_C64, double bits for DCS_C128); maxbits[0] must be the pattern of 1.0.
+ * Step s scales its writes by 2^-e with e = frexp(sqrt(maxbits[s]))'s exponent and adds
+ * e*ln2 to logscale (sequential FP64 sum, as the reference's host loop does). */
+typedef struct dcs_scale {
+    double logscale;
+    int64_t exponent_sum;
+    uint32_t flags; /* bit 0: a nonfinite maximum was seen; bit 1: the table became zero */
+    uint32_t pad;
+} dcs_scale;
+
+/* One fused pass: steps [first, first+count) applied to every coset tile of `tile_dim`
+ * dimensions.  Tile element t has address base ^ tile_addr(t); the tile basis vectors are
+ * in basis[0..tile_dim) (low `low_bits` of them are the unit vectors 1,2,4,..), and the
+ * coset bases are the deposit of x in [0, 2^coset_m) into coset_runs. */
+typedef struct dcs_group {
+    int32_t first, count;
+    int32_t tile_dim, low_bits;
+    int32_t coset_m, ncoset_runs;
+    int32_t step_tile_off; /* index into the per-step tile-mask table */
+    int32_t pad;
+    uint64_t out_mask;     /* active_out after the last step (for the max) */
+    uint64_t basis[16];    /* tile basis (slot masks) */
+    uint32_t coset_runs[DCS_MAX_RUNS];
+} dcs_group;
+
+/* Per-step tile-coordinate masks used by the fused kernel (one per step of each group). */
+typedef struct dcs_tile_step {
+    uint32_t tK, tKa, tpiv; /* tile-coordinate masks of K, Ka, grow pivot */
+    uint32_t pad;
+} dcs_tile_step;
+
+/* Result of one draw (device-side struct; the host copies it back). */
+typedef struct dcs_draw_result {
+    int64_t index;             /* A_index */
+    int32_t tie;               /* 1: the parallel CDF could not certify the index; the exact
+                                  sequential CDF was used */
+    int32_t status;            /* 0 ok, else DCS_E_CDF */
+    double total_cdf;          /* last value of the FP64 CDF before normalisation */
+    double total_exact;        /* compensated total (math.fsum equivalent) */
+    double selected_weight;    /* weights[index] */
+    double cdf_lower, cdf_upper;           /* normalised CDF at index-1 and index */
+    double cdf_lower_exact, cdf_upper_exact;/* compensated prefix / total */
+    double uniform;
+    double tv53;               /* 53-bit grid TV against the normalised weights */
+} dcs_draw_result;
+
+int dcs_abi_version(void);
+const char *dcs_last_error(void);
+/* Number of SMs of the current device (for grid sizing); negative on error. */
+int dcs_sm_count(void);
+/* sizeof of the ABI structs, so that bindings can check their layouts:
+ * 0 dcs_step, 1 dcs_param, 2 dcs_scale, 3 dcs_group, 4 dcs_tile_step, 5 dcs_draw_result. */
+size_t dcs_struct_size(int which);
+
+/* Reference-compatible single step (kernel `inplace_step`, inplace_gpu.py:20-63): the same
+ * arguments in the same order, with the address table T (nb x 256 uint64, device) and a
+ * host-chosen scale.  `dmax` receives atomicMax of the float/double bits of |x|^2 and must be
+ * zeroed by the caller (the reference does d_max.fill(0)).  grid <= 0 picks SMs*32. */
+int dcs_inplace_step(int dtype, void *E, uint64_t norbits, const uint64_t *T, int nb, int identity_map,
+                     int kind, uint64_t K, uint64_t Ka, int pivot, uint64_t beta, int ov,
+                     double f0r, double f0i, double f1r, double f1i, int fixed_y, double scale,
+                     void *dmax, int grid, void *stream);
+
+/* Steps [first, first+count) of one work item with device-resident renormalisation.
+ * table: 2^maxslots entries (device); steps: the plan (host array of nsteps); params: one
+ * dcs_param per step (device); maxbits: nsteps+1 words (device, maxbits[first] valid on
+ * entry); scale: device.  No host synchronisation. */
+int dcs_slice_steps(int dtype, void *table, const dcs_step *steps, const dcs_param *params, int nsteps,
+                    int first, int count, uint64_t *maxbits, dcs_scale *scale, void *stream);
+
+/* Batched variant: `nitems` independent work items that share the plan (one launch per step
+ * covers every item).  Item i uses table + i*table_stride entries, params + i*param_stride,
+ * maxbits + i*(nsteps+1) and scale + i. */
+int dcs_slice_steps_batched(int dtype, void *table, uint64_t table_stride, const dcs_step *steps,
+                            const dcs_param *params, uint64_t param_stride, int nsteps, int first, int count,
+                            uint64_t *maxbits, dcs_scale *scale, int nitems, void *stream);
+
+/* Fused passes over coset tiles (complex64 tables): groups [g0, g0+ng) of a fused plan.
+ * steps, groups and tile_steps are host arrays; params, maxbits (ngroups+1 words) and scale
+ * are device memory.  Renormalisation is per pass. */
+int dcs_fused_groups(void *table, const dcs_step *steps, int nsteps, const dcs_group *groups, int ngroups,
+                     const dcs_tile_step *tile_steps, const dcs_param *params, int g0, int ng,
+                     uint64_t *maxbits, dcs_scale *scale, void *stream);
+
+/* Terminal gather + syndrome scatter + coherent slice accumulation into complex128 blocks.
+ * For output block b, items item_begin[b] .. item_begin[b+1]-1 (slices, in slice order) add
+ *   total_b[synd(i) ^ xors[it]] += env_it(i) * (coefs[2it] + i coefs[2it+1]) * exp(logscale_it - log_shift)
+ * with env_it(i) = table[it*table_stride + deposit(i, terminal_runs)], synd(i) = XOR of
+ * tbasis[j] (host array, tr entries of k bits) over the bits j of i, i in [0, 2^tr).
+ * Items whose scale flags report a zero or nonfinite table, or whose final maximum
+ * (maxbits_final[it*mstride]) is zero, add nothing.  xors, coefs, item_begin, scale,
+ * maxbits_final and total are device memory; total holds nblocks * 2^k complex128. */
+int dcs_accumulate_batched(int dtype, const void *table, uint64_t table_stride, int tr,
+                           const uint32_t *terminal_runs, int nruns, const uint64_t *tbasis,
+                           const uint64_t *xors, const double *coefs, const int32_t *item_begin, int nblocks,
+                           double log_shift, dcs_scale *scale, const uint64_t *maxbits_final, uint64_t mstride,
+                           double *total, int k, int nitems, void *stream);
+
+/* Block tail for nblocks consecutive blocks of 2^k complex128: Walsh-Hadamard over k bits,
+ * multiply by (-1)^(sum over open edges of y_a y_b) (adj_hi[a] = mask of b > a adjacent to a),
+ * then apply u_open[q] (2x2 complex, row-major re/im interleaved: 8 doubles per bit) on bit q.
+ * adj_hi and u_open are host arrays. */
+int dcs_block_tail(double *total, int k, const uint32_t *adj_hi, const double *u_open, int nblocks, void *stream);
+
+/* FP64 draw from `nblocks` blocks of 2^k complex128 amplitudes with one uniform each
+ * (uniforms: device).  scratch: dcs_draw_scratch_bytes(k, nblocks) bytes of device memory.
+ * results: nblocks dcs_draw_result (device); status DCS_E_ARG = nonfinite block or uniform
+ * outside [0,1) (reference: ValueError), DCS_E_CDF = zero block / invalid outcome
+ * (reference: ArithmeticError). */
+size_t dcs_draw_scratch_bytes(int k, int nblocks);
+int dcs_draw(const double *blocks, int k, int nblocks, const double *uniforms, void *scratch,
+             dcs_draw_result *results, void *stream);
+
+/* Audit sums of two complex128 vectors (compensated FP64): out[0] = <ref,ref>,
+ * out[1] = <ap,ap>, out[2] + i out[3] = <ref,ap> = sum conj(ref) ap.  scratch: 16 KiB of
+ * device memory; out: 4 doubles of device memory.  Reference quantity:
+ * source/review/full_vector_audit_certificate.py:30-36. */
+int dcs_overlap(const double *ref, const double *ap, uint64_t len, double *out, void *scratch, void *stream);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DCS245_H */

@@ -1,0 +1,255 @@
+"""Generate the golden fixtures under tests/golden/ by running the REFERENCE itself.
+
+Run in a container that has the reference checkout (read-only) at REFERENCE_ROOT
+(default /root/reference); the GPU machines do not, which is why the outputs
+are committed.  The reference is imported unmodified:
+
+* ``qiskit`` and ``stim`` are stubbed (they are used only by circuit
+  preparation, which the fixtures replace with this project's seeded ring
+  circuits from ``dcs245_classical_sampling_b200.circuits``);
+* ``cupy`` is a NumPy-backed module (the same trick the reference uses in
+  ``source/production/make_synthetic_worker_fixture.py:53-59``);
+* the engine is ``InplaceConditionalBlockGPU`` (``sampling/conditional_block_inplace_gpu.py``)
+  with ``alloc`` rebuilt on NumPy and ``_prefix`` routed to the reference's exact
+  complex128 executor ``kernel_opt/inplace_plan.py:execute_inplace``; the slice
+  loop, syndrome scatter and Walsh-Hadamard tail are the reference's own
+  ``ConditionalBlockGPU.block`` (``sampling/conditional_block_gpu.py:128-177``).
+
+Outputs: ``<case>.json`` (inputs, reference plan, draws, meta) and
+``<case>.npz`` (graph, unitaries, reference blocks).
+
+    python tests/golden/make_golden.py [--cases c1 small c2 c64plan]
+"""
+import argparse
+import json
+import math
+import os
+import sys
+import types
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+REPO = HERE.parents[1]
+REF = Path(os.environ.get("REFERENCE_ROOT", "/root/reference")) / "source"
+
+
+def install_reference():
+    for name in ("qiskit", "stim"):
+        mod = types.ModuleType(name)
+        mod.QuantumCircuit = object
+        mod.transpile = lambda *a, **k: None
+        sys.modules.setdefault(name, mod)
+    cp = types.ModuleType("cupy")
+    for attr in ("zeros", "ones", "arange", "zeros_like", "empty", "uint64", "uint32",
+                 "complex128", "complex64", "float64", "asarray"):
+        setattr(cp, attr, getattr(np, attr))
+    cp.asnumpy = np.asarray
+    cuda = types.ModuleType("cupy.cuda")
+    cuda.get_current_stream = lambda: types.SimpleNamespace(synchronize=lambda: None)
+    cp.cuda = cuda
+    sys.modules["cupy"] = cp
+    sys.modules["cupy.cuda"] = cuda
+    for sub in ("", "sampling", "kernel_opt", "review", "production"):
+        p = str(REF / sub) if sub else str(REF)
+        if p not in sys.path:
+            sys.path.insert(0, p)
+    sys.path.insert(0, str(REPO))
+
+
+install_reference()
+from conditional_block_inplace_gpu import InplaceConditionalBlockGPU  # noqa: E402
+from inplace_plan import compile_inplace, execute_inplace  # noqa: E402
+from sampling_protocol import draw_checked, make_protocol, assemble_output  # noqa: E402
+from protocol_common import actual_cdf_law_vector  # noqa: E402
+from full_vector_audit_certificate import audit_vector_pair  # noqa: E402
+from dcs_rankwidth.parity_slicing import choose_parity_slices, prefix_ranks_matrix  # noqa: E402
+from dcs_rankwidth import scan_plan  # noqa: E402
+
+from dcs245_classical_sampling_b200.circuits import build_ring_instance  # noqa: E402
+from dcs245_classical_sampling_b200.workloads import build_workload  # noqa: E402
+
+
+class OracleEngine(InplaceConditionalBlockGPU):
+    """Reference engine with NumPy storage and the exact complex128 executor."""
+
+    def alloc(self, dtype=np.complex128, device=0):
+        self.cp = sys.modules["cupy"]
+        self.inplace_fp64 = True
+        self.use_fp64 = True
+        stop = len(self.steps)
+        self.inplace_steps, self.inplace_terminal_basis, self.inplace_maxslots = compile_inplace(
+            self.order, self.fut, self.fixed, stop)
+        self.inplace_rmax = max([0] + [len(s.active_out) for s in self.inplace_steps])
+        self.terminal_basis = [b >> self.stop for _, b in sorted(self.inplace_terminal_basis.items())]
+        self.terminal_rank = len(self.terminal_basis)
+        ids = np.arange(1 << self.terminal_rank, dtype=np.uint64)
+        self.d_syndrome_map = np.zeros_like(ids)
+        for j, b in enumerate(self.terminal_basis):
+            self.d_syndrome_map ^= ((ids >> np.uint64(j)) & np.uint64(1)) * np.uint64(b)
+        self.d_phase = np.ones(1 << len(self.open_full), np.float64)
+        ids = np.arange(len(self.d_phase), dtype=np.uint64)
+        for a, b in self.open_edges:
+            self.d_phase *= 1 - 2 * (((ids >> np.uint64(a)) & (ids >> np.uint64(b)) & np.uint64(1)).astype(np.float64))
+
+    def _prefix(self, f, yfix):
+        env, ls, offset, _ = execute_inplace(self.inplace_steps, f, yfix, self.fut, self.inplace_maxslots)
+        if not np.any(env):
+            return None, ls, offset >> self.stop
+        return env, ls, offset >> self.stop
+
+
+def plan_json(engine):
+    steps = []
+    for st in engine.inplace_steps:
+        steps.append({"v": st.v, "j": st.j, "kind": st.kind, "active_in": list(st.active_in),
+                      "active_out": list(st.active_out), "beta": st.beta, "K": st.K, "Ka": st.Ka,
+                      "pivot": st.pivot, "pivot_a": st.pivot_a, "free": bool(st.free)})
+    return {"steps": steps, "terminal_basis": [int(b) for b in engine.terminal_basis],
+            "terminal_slots": sorted(int(p) for p in engine.inplace_terminal_basis),
+            "maxslots": engine.inplace_maxslots, "inplace_rmax": engine.inplace_rmax,
+            "stop": engine.stop, "rmax": engine.rmax, "work": engine.work,
+            "open_edges": [list(map(int, e)) for e in engine.open_edges],
+            "order": list(map(int, engine.order)), "fixed": sorted(map(int, engine.fixed)),
+            "fut": [int(x) for x in engine.fut], "slices": list(map(int, engine.slices))}
+
+
+def jsonable(d):
+    out = {}
+    for k, v in d.items():
+        if isinstance(v, (np.integer,)):
+            v = int(v)
+        elif isinstance(v, (np.floating,)):
+            v = float(v)
+        out[k] = v
+    return out
+
+
+def make_case(name, workload, n_prefixes, n_uniforms, blocks=True, proto_seed=None):
+    w = build_workload(workload)
+    n, openv, order, ops = w["n"], w["open_vertices"], w["order"], w["parity_operations"]
+    A = w["graph"]
+    N = len(A)
+    inst = w
+    case = {"name": name, "workload": workload, "n": n, "depth": w["depth"], "t_count": w["t_count"],
+            "seed": w["seed"],
+            "open_vertices": openv, "order": list(map(int, order)),
+            "parity_operations": [[a, b, c] for a, b, c in ops], "N": N}
+    t0 = __import__("time").time()
+    eng = OracleEngine(A, inst["unitaries"], n, order, ops, openv)
+    eng.alloc()
+    case["plan"] = plan_json(eng)
+    case["prefix_cut_ranks_order"] = [int(x) for x in prefix_ranks_matrix(A.copy(), list(order))]
+    proto = make_protocol(proto_seed if proto_seed is not None else 1000 + w["seed"], n_prefixes, n, openv)
+    case["protocol"] = {"seed": proto["seed"], "records": [
+        {"sample_id": r["sample_id"], "input_data_bits": r["input_data_bits"],
+         "draw_uniform": r["draw_uniform"], "branch_uniform": r["branch_uniform"]}
+        for r in proto["records"]]}
+    arrays = {"graph": A, "unitaries": inst["unitaries"], "order": np.asarray(order)}
+    draws = []
+    if blocks:
+        rng = np.random.default_rng(7)
+        for r in proto["records"]:
+            x = np.asarray(list(map(int, r["input_data_bits"])), np.uint8)
+            v, meta = eng.block(x)
+            v = np.asarray(v)
+            arrays[f"block_{r['sample_id']}"] = v
+            us = [r["draw_uniform"]] + [float(u) for u in rng.random(n_uniforms - 1)]
+            for u in us:
+                d = draw_checked(v, u)
+                bits, qiskit = assemble_output(r["input_data_bits"], openv, d["A_index"], inst["ring"])
+                d = jsonable(d)
+                d["sample_id"] = r["sample_id"]
+                d["data_bits_ring_order"] = bits
+                d["bitstring_qiskit"] = qiskit
+                draws.append(d)
+            meta = {k2: v2 for k2, v2 in meta.items() if k2 != "seconds"}
+            case.setdefault("block_meta", []).append(jsonable(meta))
+        case["draws"] = draws
+    case["seconds"] = __import__("time").time() - t0
+    return case, arrays
+
+
+def sampler_cases():
+    """Known-answer cases of the reference sampler and audit helpers on fixed vectors."""
+    out = {"selftest": [], "law": [], "audit": []}
+    for weights in [np.array([0., 1., 0., 2., 3., 0., 4., 0.]),
+                    np.array([1e-100, 1., .5, 0., 7., 2e-100, 1., .1])]:
+        v = np.sqrt(weights) * np.exp(1j * np.arange(len(weights)))
+        cdf = np.cumsum(weights) / np.sum(weights)
+        for idx in np.flatnonzero(weights):
+            lo = cdf[idx - 1] if idx else 0.
+            if cdf[idx] == lo:
+                continue
+            u = (lo + cdf[idx]) / 2
+            d = draw_checked(v, u)
+            out["selftest"].append({"re": v.real.tolist(), "im": v.imag.tolist(), "u": u,
+                                    "draw": jsonable({k: d[k] for k in d if k != "replay_scope"})})
+    for a in [np.array([0, 1, 1j, 1 + 1j, 0, 2, 1 - 1j, 0], complex),
+              np.array([1e-15, 1e-8j, 1, 1j, 2 + 3j, .17, .21j, .01], complex)]:
+        law, meta = actual_cdf_law_vector(a)
+        d = draw_checked(a, .381245)
+        out["law"].append({"re": a.real.tolist(), "im": a.imag.tolist(), "law_re": law.real.tolist(),
+                           "law_im": law.imag.tolist(), "meta": jsonable(meta), "A_index": d["A_index"]})
+    rng = np.random.default_rng(3)
+    for _ in range(3):
+        ref = rng.normal(size=16) + 1j * rng.normal(size=16)
+        approx = (ref + 1e-3 * (rng.normal(size=16) + 1j * rng.normal(size=16))).astype(np.complex64)
+        approx = approx.astype(np.complex128)
+        out["audit"].append({"ref_re": ref.real.tolist(), "ref_im": ref.imag.tolist(),
+                             "ap_re": approx.real.tolist(), "ap_im": approx.imag.tolist(),
+                             "result": jsonable(audit_vector_pair(ref, approx, 0))})
+    proto = make_protocol(733245, 113, 6, [5, 1, 3], .45)
+    out["protocol_733245"] = [{"sample_id": r["sample_id"], "conditional_branch": r["conditional_branch"],
+                               "branch_uniform": r["branch_uniform"], "draw_uniform": r["draw_uniform"],
+                               "input_data_bits": r["input_data_bits"]} for r in proto["records"]]
+    out["assemble"] = [list(assemble_output("000000", [5, 1, 3], i, [5, 0, 4, 1, 3, 2])) for i in range(8)]
+    return out
+
+
+def chooser_case():
+    """Reference parity-slice chooser and cut ranks on a small synthetic graph (unfiltered)."""
+    inst = build_ring_instance(12, 10, 14, 77)
+    A = inst["graph"]
+    N = len(A)
+    edges = [(int(a), int(b)) for a, b in zip(*np.nonzero(np.triu(A, 1)))]
+    order = list(map(int, inst["natural_order"]))
+    ops, S = choose_parity_slices(N, edges, order, 3, seed=0, verbose=False)
+    return {"n": 12, "depth": 10, "t_count": 14, "seed": 77, "order": order,
+            "ops": [[a, b, c] for a, b, c in ops], "removed": S,
+            "cut_ranks": [int(x) for x in prefix_ranks_matrix(A.copy(), order)]}
+
+
+CASES = {
+    # 16-qubit ring, depth 20, 24 T, 8 open bits (the small CPU-runnable workload)
+    "c1": dict(workload="ring16_d20_t24_k8", n_prefixes=4, n_uniforms=4),
+    # a mid-size ring with two parity slices
+    "small": dict(workload="ring24_d24_t60_k10", n_prefixes=3, n_uniforms=3),
+    # 40-qubit ring, depth 45, 190 T, 16 open bits (one prefix; ~2^22 tables)
+    "c2": dict(workload="ring40_d45_t190_k16", n_prefixes=1, n_uniforms=4),
+    # plan only: 64-qubit ring, depth 73, 314 T, 20 open bits, two parity slices
+    "c64plan": dict(workload="ring64_d73_t314_k20", n_prefixes=2, n_uniforms=0, blocks=False),
+}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--cases", nargs="*", default=list(CASES) + ["sampler", "chooser"])
+    args = ap.parse_args()
+    for name in args.cases:
+        if name == "sampler":
+            (HERE / "sampler.json").write_text(json.dumps(sampler_cases(), indent=1))
+            continue
+        if name == "chooser":
+            (HERE / "chooser.json").write_text(json.dumps(chooser_case(), indent=1))
+            continue
+        case, arrays = make_case(name, **CASES[name])
+        (HERE / f"{name}.json").write_text(json.dumps(case, indent=1))
+        np.savez_compressed(HERE / f"{name}.npz", **arrays)
+        print(name, "N", case["N"], "rmax", case["plan"]["inplace_rmax"], "ops", case["parity_operations"],
+              "%.1fs" % case["seconds"], flush=True)
+
+
+if __name__ == "__main__":
+    main()

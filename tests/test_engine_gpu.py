@@ -1,0 +1,208 @@
+"""GPU parity: the CUDA path (through the C ABI) against the reference's outputs and the oracle."""
+import math
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+CASES = ["c1", "small", "c2"]
+
+
+def _engine(case, arrays, dtype, mode="device", **kw):
+    from dcs245_classical_sampling_b200.engine import InplaceConditionalBlockGPU
+    eng = InplaceConditionalBlockGPU(arrays["graph"], arrays["unitaries"], case["n"], case["order"],
+                                     case["parity_operations"], case["open_vertices"])
+    eng.alloc(dtype=dtype, mode=mode, **kw)
+    return eng
+
+
+def _x(rec):
+    return np.array([int(c) for c in rec["input_data_bits"]], np.uint8)
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_complex128_block_matches_reference(golden, name):
+    case, arrays = golden(name)
+    eng = _engine(case, arrays, np.complex128)
+    for rec in case["protocol"]["records"]:
+        v, meta = eng.block(_x(rec))
+        assert v.dtype == torch.complex128 and v.is_cuda
+        want = arrays[f"block_{rec['sample_id']}"]
+        assert rel_l2(v.cpu().numpy(), want) < 1e-13
+        ref_meta = case["block_meta"][rec["sample_id"]]
+        for key in ("slices_evaluated", "rmax", "terminal_rank", "work_per_slice", "prefix_dtype"):
+            assert meta[key] == ref_meta[key], key
+
+
+@pytest.mark.parametrize("mode", ["device", "plain", "fused"])
+@pytest.mark.parametrize("name", CASES)
+def test_complex64_block_matches_reference(golden, name, mode):
+    case, arrays = golden(name)
+    eng = _engine(case, arrays, np.complex64, mode=mode)
+    for rec in case["protocol"]["records"]:
+        v, meta = eng.block(_x(rec))
+        want = arrays[f"block_{rec['sample_id']}"]
+        err = rel_l2(v.cpu().numpy(), want)
+        assert err < 1e-5, err
+        assert meta["prefix_dtype"] == "complex64"
+
+
+def test_one_item_at_a_time_equals_batched_slices(golden):
+    case, arrays = golden("small")
+    a = _engine(case, arrays, np.complex128, items=1)
+    b = _engine(case, arrays, np.complex128)
+    assert b.items > 1
+    x = _x(case["protocol"]["records"][0])
+    va, _ = a.block(x)
+    vb, _ = b.block(x)
+    assert torch.equal(va, vb)  # slice order is kept: bitwise identical
+
+
+def test_parts_sum_to_the_block(golden):
+    case, arrays = golden("small")
+    eng = _engine(case, arrays, np.complex128)
+    x = _x(case["protocol"]["records"][1])
+    full, _ = eng.block(x)
+    parts = sum(eng.block(x, part=p, parts=3)[0] for p in range(3))
+    assert rel_l2(parts.cpu().numpy(), full.cpu().numpy()) < 1e-14
+
+
+def test_batched_prefixes_equal_single_blocks(golden):
+    case, arrays = golden("small")
+    eng = _engine(case, arrays, np.complex64)
+    xs = [_x(r) for r in case["protocol"]["records"]]
+    many = eng.blocks(xs)
+    for i, x in enumerate(xs):
+        one, _ = eng.block(x)
+        assert rel_l2(many[i].cpu().numpy(), one.cpu().numpy()) < 1e-6
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_draws_match_reference(golden, name):
+    from dcs245_classical_sampling_b200.sampling import draw_checked
+    case, arrays = golden(name)
+    for d in case["draws"]:
+        v = torch.from_numpy(arrays[f"block_{d['sample_id']}"]).cuda()
+        got = draw_checked(v, d["uniform"])
+        assert got["A_index"] == d["A_index"]
+        assert got["weights_sha256"] == d["weights_sha256"]
+        assert got["amplitudes_sha256"] == d["amplitudes_sha256"]
+        assert got["selected_scaled_weight"] == d["selected_scaled_weight"]
+        for key in ("cdf_lower_fsum", "cdf_upper_fsum", "scaled_mass_fsum"):
+            assert got[key] == pytest.approx(d[key], rel=4e-16, abs=1e-300), key
+        if not got["cdf_tie"]:
+            for key in ("cdf_lower_numpy", "cdf_upper_numpy"):
+                assert got[key] == pytest.approx(d[key], rel=1e-12, abs=1e-300), key
+        assert got["finite_53bit_draw_TV_against_computed_normalized_weights"] == pytest.approx(
+            d["finite_53bit_draw_TV_against_computed_normalized_weights"], rel=1e-3, abs=1e-15)
+
+
+def test_sampler_known_answers(golden):
+    from dcs245_classical_sampling_b200.sampling import draw_checked
+    s, _ = golden("sampler")
+    for c in s["selftest"]:
+        v = np.array(c["re"]) + 1j * np.array(c["im"])
+        got = draw_checked(v, c["u"])
+        assert got["A_index"] == c["draw"]["A_index"]
+    for c in s["law"]:
+        a = np.array(c["re"]) + 1j * np.array(c["im"])
+        assert draw_checked(a, .381245)["A_index"] == c["A_index"]
+
+
+def test_tie_path_is_numpy_exact():
+    """u placed exactly on a float64 CDF boundary: the device must fall back to the exact
+    sequential CDF and still return numpy's index."""
+    from dcs245_classical_sampling_b200.sampling import draw_checked
+    from oracle import sampler_ref
+    rng = np.random.default_rng(5)
+    v = rng.normal(size=1 << 12) + 1j * rng.normal(size=1 << 12)
+    w = v.real * v.real + v.imag * v.imag
+    cdf = np.cumsum(w) / np.cumsum(w)[-1]
+    for i in (3, 1000, 4000):
+        u = float(cdf[i])
+        got = draw_checked(v, u)
+        want = sampler_ref.draw(v, u)
+        assert got["A_index"] == want["A_index"]
+        assert got["cdf_tie"]
+
+
+def test_draw_errors():
+    from dcs245_classical_sampling_b200.sampling import draw_checked
+    with pytest.raises(ArithmeticError):
+        draw_checked(np.zeros(8, complex), 0.5)
+    with pytest.raises(ValueError):
+        draw_checked(np.array([np.nan, 1, 1, 1], complex), 0.5)
+    with pytest.raises(ValueError):
+        draw_checked(np.ones(6, complex), 0.5)
+
+
+def test_nonfinite_table_raises(golden):
+    case, arrays = golden("c1")
+    eng = _engine(case, arrays, np.complex64)
+    with pytest.raises(ArithmeticError):
+        eng.block(_x(case["protocol"]["records"][0]), w=np.array([np.nan, 1.0]))
+
+
+def test_reference_compatible_kernel(golden):
+    """dcs_inplace_step takes the reference kernel's own arguments (byte tables, host scale,
+    d_max): running the reference's host loop over it reproduces the oracle environment."""
+    from dcs245_classical_sampling_b200 import _lib
+    from dcs245_classical_sampling_b200 import plan as P
+    from oracle import block_ref
+    lib = _lib.load()
+    case, arrays = golden("small")
+    oe = block_ref.OracleEngine(arrays["graph"], arrays["unitaries"], case["n"], case["order"],
+                                case["parity_operations"], case["open_vertices"])
+    x = _x(case["protocol"]["records"][0])
+    coef, f, yfix, flips = next(s for s in oe.slice_inputs(x) if s[0])
+    want, wls, _ = block_ref.execute(oe.steps, f, yfix, oe.fut, oe.maxslots)
+    for dtype, tol in ((_lib.C128, 1e-13), (_lib.C64, 1e-6)):
+        E = torch.zeros(1 << oe.maxslots, dtype=torch.complex128 if dtype else torch.complex64, device="cuda")
+        dmax = torch.zeros(1, dtype=torch.int64, device="cuda")
+        E[0] = 1
+        offset, ls, maximum = 0, 0.0, 1.0
+        for st in oe.steps:
+            kind, omit = P.orbit_kind(P.OrbitStep(st["v"], st["j"], st["kind"], st["active_in"], st["active_out"],
+                                                   st["beta"], st["K"], st["Ka"], st["pivot"], st["pivot_a"],
+                                                   st["free"]))
+            slots = [p for p in st["active_in"] if p not in omit]
+            T = np.zeros((max(1, (len(slots) + 7) // 8), 256), np.uint64)
+            for b in range(T.shape[0]):
+                for val in range(256):
+                    acc = 0
+                    for t in range(8):
+                        i = 8 * b + t
+                        if i < len(slots) and (val >> t) & 1:
+                            acc ^= 1 << slots[i]
+                    T[b, val] = acc
+            dT = torch.from_numpy(T.reshape(-1).view(np.int64)).cuda()
+            identity = int(slots == list(range(len(slots))))
+            j = st["j"]
+            ov = (offset >> j) & 1
+            offset &= ~(1 << j)
+            y = 0
+            if not st["free"]:
+                y = int(yfix[st["v"]])
+                if y:
+                    offset ^= oe.fut[j]
+            f0, f1 = map(complex, f[st["v"]])
+            e = math.frexp(maximum)[1]
+            ls += e * math.log(2.0)
+            dmax.zero_()
+            _lib.check(lib.dcs_inplace_step(dtype, _lib.ptr(E), 1 << len(slots), _lib.ptr(dT), T.shape[0], identity,
+                                            kind, st["K"], st["Ka"], st["pivot"], st["beta"], ov, f0.real, f0.imag,
+                                            f1.real, f1.imag, y, math.ldexp(1.0, -e), _lib.ptr(dmax), 0,
+                                            torch.cuda.current_stream().cuda_stream))
+            bits = int(dmax.cpu().numpy()[0])
+            m2 = float(np.array([bits], np.uint64).view(np.float64)[0]) if dtype else \
+                float(np.array([bits & 0xffffffff], np.uint32).view(np.float32)[0])
+            if m2 == 0:
+                break
+            maximum = math.sqrt(m2)
+        term = block_ref._addr(oe.steps[-1]["active_out"]).astype(np.int64)
+        got = E.cpu().numpy()[term].astype(np.complex128)
+        assert rel_l2(got * math.exp(ls), want * math.exp(wls)) < tol

@@ -1,0 +1,66 @@
+"""Host planner (product) bit-exact against the reference's compiled plans."""
+import numpy as np
+import pytest
+
+from dcs245_classical_sampling_b200 import plan as P
+from dcs245_classical_sampling_b200.workloads import build_workload, WORKLOADS
+
+
+@pytest.mark.parametrize("name", ["c1", "small", "c2", "c64plan"])
+def test_block_plan_matches_reference(golden, name):
+    case, arrays = golden(name)
+    bp = P.build_block_plan(arrays["graph"], arrays["unitaries"], case["n"], case["order"],
+                            case["parity_operations"], case["open_vertices"])
+    ref = case["plan"]
+    assert bp.order == ref["order"]
+    assert sorted(bp.fixed) == ref["fixed"]
+    assert bp.fut == ref["fut"]
+    assert bp.stop == ref["stop"]
+    assert bp.rmax == ref["rmax"] and bp.work == ref["work"]
+    assert bp.maxslots == ref["maxslots"] and bp.inplace_rmax == ref["inplace_rmax"]
+    assert list(bp.terminal_slots) == ref["terminal_slots"]
+    assert bp.terminal_basis == ref["terminal_basis"]
+    assert [list(e) for e in bp.open_edges] == ref["open_edges"]
+    for mine, theirs in zip(bp.steps, ref["steps"]):
+        assert (mine.v, mine.j, mine.kind, mine.beta, mine.K, mine.Ka, mine.pivot, mine.pivot_a, mine.free) == \
+            (theirs["v"], theirs["j"], theirs["kind"], theirs["beta"], theirs["K"], theirs["Ka"],
+             theirs["pivot"], theirs["pivot_a"], theirs["free"])
+        assert list(mine.active_in) == theirs["active_in"] and list(mine.active_out) == theirs["active_out"]
+
+
+def test_cut_ranks_and_chooser_match_reference(golden):
+    c, _ = golden("chooser")
+    from dcs245_classical_sampling_b200.circuits import build_ring_instance
+    inst = build_ring_instance(c["n"], c["depth"], c["t_count"], c["seed"])
+    A = inst["graph"]
+    assert list(P.prefix_cut_ranks(A, c["order"])) == c["cut_ranks"]
+    edges = [(int(a), int(b)) for a, b in zip(*np.nonzero(np.triu(A, 1)))]
+    ops, S = P.choose_parity_slices(len(A), edges, c["order"], 3, seed=0)
+    assert [list(o) for o in ops] == c["ops"] and S == c["removed"]
+
+
+def test_reference_errors():
+    from dcs245_classical_sampling_b200.circuits import build_ring_instance
+    inst = build_ring_instance(4, 3, 2, 1)
+    args = (inst["graph"], inst["unitaries"], 4, list(inst["order"]))
+    with pytest.raises(ValueError):
+        P.build_block_plan(*args, [], [1, 1])            # repeated free vertex
+    with pytest.raises(ValueError):
+        P.build_block_plan(*args, [], [5])               # not a data vertex
+    with pytest.raises(ValueError):
+        P.build_block_plan(*args, [("Z", 0, None)], [1])  # slicing a data vertex
+    with pytest.raises(ValueError):
+        P.build_block_plan(*args, [("Q", 4, None)], [1])  # unknown parity kind
+
+
+def test_workload_cache_is_reproducible():
+    for name in ["ring16_d20_t24_k8", "ring24_d24_t60_k10"]:
+        cached = build_workload(name)
+        fresh = build_workload(name, use_cache=False)
+        assert cached["parity_operations"] == fresh["parity_operations"]
+
+
+def test_workload_sizes():
+    for name, (n, depth, t, seed, k, npar) in WORKLOADS.items():
+        w = build_workload(name)
+        assert w["N"] == n + t and len(w["open_vertices"]) == k and len(w["parity_operations"]) == npar
