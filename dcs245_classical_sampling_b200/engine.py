@@ -258,90 +258,142 @@ class InplaceConditionalBlockGPU:
         # empty environment = 1 at address 0 of every item (inplace_gpu.py:108)
         self.table.view(self.items, self.table_stride)[:n_items, 0] = 1
 
-    def _upload_params(self, plist):
-        host = np.concatenate(plist).view(np.int64)
-        t = torch.from_numpy(host).pin_memory()
-        self.d_params[: host.size].copy_(t, non_blocking=True)
-        return t  # keep the pinned buffer alive until the copy is consumed
+    def prepare(self, x_list, w=None, part=0, parts=1):
+        """Host bookkeeping for a batch of prefixes and ONE host->device upload.
 
-    def _run_steps(self, n_items):
+        Work items are the (prefix, slice) pairs with a nonzero slice coefficient, in prefix
+        order then slice order; they run `self.items` at a time."""
+        work, counts = [], []
+        for b, x in enumerate(x_list):
+            cnt, items = self.params.items(x, w, part, parts)
+            counts.append(cnt)
+            work.extend((b, c, p, xo) for c, p, xo in items)
+        n = len(work)
+        chunks = []
+        begin_all = []
+        for c0 in range(0, n, self.items):
+            chunk = work[c0:c0 + self.items]
+            blocks_in = []
+            for it in chunk:
+                if not blocks_in or blocks_in[-1] != it[0]:
+                    blocks_in.append(it[0])
+            begin = [0]
+            for bb in blocks_in:
+                begin.append(begin[-1] + sum(1 for it in chunk if it[0] == bb))
+            chunks.append((c0, len(chunk), blocks_in[0], len(blocks_in), len(begin_all)))
+            begin_all.extend(begin)
+        host_params = (np.concatenate([it[2] for it in work]) if n else
+                       np.zeros(1, _lib.PARAM_DTYPE)).view(np.int64)
+        coefs = np.zeros(2 * max(1, n), np.float64)
+        xors = np.zeros(max(1, n), np.uint64)
+        for i, (_, c, _, xo) in enumerate(work):
+            coefs[2 * i], coefs[2 * i + 1] = c.real, c.imag
+            xors[i] = xo
+        blob = np.concatenate([host_params, coefs.view(np.int64), xors.view(np.int64),
+                               np.asarray(begin_all or [0], np.int64)])
+        pinned = torch.from_numpy(blob).pin_memory()
+        dev = torch.empty(blob.size, dtype=torch.int64, device=self.device)
+        dev.copy_(pinned, non_blocking=True)
+        o1 = host_params.size
+        o2 = o1 + coefs.size
+        o3 = o2 + xors.size
+        return {"n_items": n, "chunks": chunks, "counts": counts, "nblocks": len(x_list), "dev": dev,
+                "pinned": pinned, "params": dev[:o1], "coefs": dev[o1:o2].view(torch.float64),
+                "xors": dev[o2:o3], "begin": dev[o3:].to(torch.int32), "h2d_bytes": blob.nbytes}
+
+    def _run_steps(self, params_ptr, n_items):
         lib, st = self.lib, self._stream()
         nm = self._nmax() + 1
         if self.mode == "fused":
             f = self.fplan
             _lib.check(lib.dcs_fused_groups(_lib.ptr(self.table), f.dsteps.ctypes.data, len(f.dsteps),
                                             f.groups.ctypes.data, len(f.groups), f.tile_steps.ctypes.data,
-                                            _lib.ptr(self.d_params), 0, len(f.groups), _lib.ptr(self.maxbits),
+                                            params_ptr, 0, len(f.groups), _lib.ptr(self.maxbits),
                                             _lib.ptr(self.scale), st))
-            return True
+            return
         if self.mode == "plain":
             mb = self.maxbits.view(self.items, nm)
             for s in range(self.nsteps):
                 _lib.check(lib.dcs_slice_steps_batched(
-                    self.dcode, _lib.ptr(self.table), self.table_stride, self.dsteps.ctypes.data,
-                    _lib.ptr(self.d_params), self.nsteps, self.nsteps, s, 1, _lib.ptr(self.maxbits),
-                    _lib.ptr(self.scale), n_items, st))
+                    self.dcode, _lib.ptr(self.table), self.table_stride, self.dsteps.ctypes.data, params_ptr,
+                    self.nsteps, self.nsteps, s, 1, _lib.ptr(self.maxbits), _lib.ptr(self.scale), n_items, st))
                 bits = mb[:n_items, s + 1].cpu().numpy()  # host sync per step, as the reference
                 m2 = (bits.view(np.float64) if self.use_fp64 else bits.astype(np.uint32).view(np.float32))
                 if not np.all(np.isfinite(m2)):
                     raise ArithmeticError("Nonfinite in-place environment")
                 if np.all(m2 == 0):
-                    return False
-            return True
+                    break  # the remaining steps act on zero tables (the reference returns None here)
+            return
         _lib.check(lib.dcs_slice_steps_batched(
-            self.dcode, _lib.ptr(self.table), self.table_stride, self.dsteps.ctypes.data, _lib.ptr(self.d_params),
+            self.dcode, _lib.ptr(self.table), self.table_stride, self.dsteps.ctypes.data, params_ptr,
             self.nsteps, self.nsteps, 0, self.nsteps, _lib.ptr(self.maxbits), _lib.ptr(self.scale), n_items, st))
-        return True
 
-    def _accumulate(self, items, total, nblocks_items):
-        """items: list of (coef, xor); nblocks_items: item_begin array (len nblocks+1)."""
+    def enqueue(self, prep, out):
+        """Device work for a prepared batch into `out` ((nblocks, 2^k) complex128, zeroed):
+        contraction of every work item, accumulation, tail.  No host synchronisation
+        (except in "plain" mode).  Returns the number of library kernel launches."""
         lib = self.lib
-        n = len(items)
-        coefs = np.zeros(2 * max(1, n), np.float64)
-        xors = np.zeros(max(1, n), np.uint64)
-        for i, (c, x) in enumerate(items):
-            coefs[2 * i], coefs[2 * i + 1] = c.real, c.imag
-            xors[i] = x
-        dev = self.device
-        d_coefs = torch.from_numpy(coefs).to(dev, non_blocking=False)
-        d_xors = torch.from_numpy(xors.view(np.int64)).to(dev)
-        d_begin = torch.from_numpy(np.asarray(nblocks_items, np.int32)).to(dev)
         nm = self._nmax() + 1
-        _lib.check(lib.dcs_accumulate_batched(
-            self.dcode, _lib.ptr(self.table), self.table_stride, self.plan.terminal_rank, self.term_runs.ctypes.data,
-            self.term_nruns, self.tbasis.ctypes.data, _lib.ptr(d_xors), _lib.ptr(d_coefs), _lib.ptr(d_begin),
-            len(nblocks_items) - 1, self.params.shift, _lib.ptr(self.scale),
-            _lib.ptr(self.maxbits[nm - 1:]), nm, _lib.ptr(total), self.k, n, self._stream()))
-        return d_coefs, d_xors, d_begin
+        entry = _lib.PARAM_DTYPE.itemsize
+        launches = 0
+        for c0, cn, b0, nb, boff in prep["chunks"]:
+            self._reset_items(cn)
+            self._run_steps(_lib.ptr(prep["params"]) + c0 * self.nsteps * entry, cn)
+            launches += len(self.fplan.groups) if self.mode == "fused" else self.nsteps
+            flat = out[b0:b0 + nb].view(torch.float64)
+            _lib.check(lib.dcs_accumulate_batched(
+                self.dcode, _lib.ptr(self.table), self.table_stride, self.plan.terminal_rank,
+                self.term_runs.ctypes.data, self.term_nruns, self.tbasis.ctypes.data,
+                _lib.ptr(prep["xors"]) + 8 * c0, _lib.ptr(prep["coefs"]) + 16 * c0,
+                _lib.ptr(prep["begin"]) + 4 * boff, nb, self.params.shift, _lib.ptr(self.scale),
+                _lib.ptr(self.maxbits[nm - 1:]), nm, _lib.ptr(flat), self.k, cn, self._stream()))
+            launches += 2
+        _lib.check(lib.dcs_block_tail(_lib.ptr(out), self.k, self.adj_hi.ctypes.data, self.u_open.ctypes.data,
+                                      prep["nblocks"], self._stream()))
+        launches += 2 if self.k <= 12 else 4
+        return launches
 
-    def _check_flags(self, n_items):
-        sc = self.scale.view(self.items, -1)[:n_items].cpu().numpy().view(_lib.SCALE_DTYPE)
-        if np.any(sc["flags"] & 1):
+    def _flags_tensor(self):
+        return torch.zeros(self.items, dtype=torch.int64, device=self.device)
+
+    def check_scale_flags(self, n_items=None):
+        """Raise the reference's ArithmeticError if the last chunk saw a nonfinite table."""
+        sc = self.scale.view(self.items, -1)[: n_items or self.items, 2].cpu().numpy()
+        if np.any(sc & 1):
             raise ArithmeticError("Nonfinite in-place environment")
+
+    def _run(self, x_list, w=None, part=0, parts=1):
+        prep = self.prepare(x_list, w, part, parts)
+        out = torch.zeros((len(x_list), 1 << self.k), dtype=torch.complex128, device=self.device)
+        flags = self._flags_tensor()
+        lib = self.lib
+        nm = self._nmax() + 1
+        entry = _lib.PARAM_DTYPE.itemsize
+        for c0, cn, b0, nb, boff in prep["chunks"]:
+            self._reset_items(cn)
+            self._run_steps(_lib.ptr(prep["params"]) + c0 * self.nsteps * entry, cn)
+            flat = out[b0:b0 + nb].view(torch.float64)
+            _lib.check(lib.dcs_accumulate_batched(
+                self.dcode, _lib.ptr(self.table), self.table_stride, self.plan.terminal_rank,
+                self.term_runs.ctypes.data, self.term_nruns, self.tbasis.ctypes.data,
+                _lib.ptr(prep["xors"]) + 8 * c0, _lib.ptr(prep["coefs"]) + 16 * c0,
+                _lib.ptr(prep["begin"]) + 4 * boff, nb, self.params.shift, _lib.ptr(self.scale),
+                _lib.ptr(self.maxbits[nm - 1:]), nm, _lib.ptr(flat), self.k, cn, self._stream()))
+            flags[:cn] |= self.scale.view(self.items, -1)[:cn, 2]
+        _lib.check(lib.dcs_block_tail(_lib.ptr(out), self.k, self.adj_hi.ctypes.data, self.u_open.ctypes.data,
+                                      len(x_list), self._stream()))
+        if bool(((flags & 1) != 0).any()):  # one small device->host read per call
+            raise ArithmeticError("Nonfinite in-place environment")
+        return out, prep
 
     def block(self, x_bits, w=None, part=0, parts=1):
         """Scaled conditional amplitudes of one prefix (conditional_block_gpu.py:128-177)."""
         if not self._alloc:
             self.alloc()
         start = time.perf_counter()
-        k = self.k
-        total = torch.zeros(1 << k, dtype=torch.complex128, device=self.device)
-        count, items = self.params.items(x_bits, w, part, parts)
-        keep = []
-        for b0 in range(0, len(items), self.items):
-            chunk = items[b0:b0 + self.items]
-            self._reset_items(len(chunk))
-            hold = self._upload_params([it[1] for it in chunk])
-            ok = self._run_steps(len(chunk))
-            if ok:
-                keep.append(self._accumulate([(c, x) for c, _, x in chunk], total.view(torch.float64),
-                                             [0, len(chunk)]))
-            self._check_flags(len(chunk))
-            del hold
-        _lib.check(self.lib.dcs_block_tail(_lib.ptr(total), k, self.adj_hi.ctypes.data, self.u_open.ctypes.data, 1,
-                                           self._stream()))
+        out, prep = self._run([x_bits], w, part, parts)
         torch.cuda.current_stream(self.device).synchronize()
-        return total, self._meta(time.perf_counter() - start, part, parts, count)
+        return out[0], self._meta(time.perf_counter() - start, part, parts, prep["counts"][0])
 
     def _meta(self, seconds, part, parts, count):
         return {"seconds": seconds, "part": part, "parts": parts, "slices_evaluated": count,
@@ -350,36 +402,11 @@ class InplaceConditionalBlockGPU:
                 "open_vertices": self.open_full,
                 "vector_scale": "sqrt(2^(n-k)); sum all complex parts before probabilities"}
 
-    # ------------------------------------------------------------------ batched prefixes
     def blocks(self, x_list, w=None):
-        """Blocks of many prefixes: (prefix, slice) work items share launches.
+        """Blocks of many prefixes; (prefix, slice) work items share launches.
 
         Returns a complex128 tensor (len(x_list), 2^k) on the device."""
         if not self._alloc:
             self.alloc()
-        k = self.k
-        out = torch.zeros((len(x_list), 1 << k), dtype=torch.complex128, device=self.device)
-        work = []  # (block index, coef, params, xor)
-        for b, x in enumerate(x_list):
-            _, items = self.params.items(x, w)
-            work.extend((b, c, p, xo) for c, p, xo in items)
-        keep = []
-        for b0 in range(0, len(work), self.items):
-            chunk = work[b0:b0 + self.items]
-            self._reset_items(len(chunk))
-            hold = self._upload_params([it[2] for it in chunk])
-            self._run_steps(len(chunk))
-            # items of one launch are grouped by block in order; accumulate per block range
-            blocks_in = sorted(set(it[0] for it in chunk))
-            begin = [0]
-            for bb in blocks_in:
-                begin.append(begin[-1] + sum(1 for it in chunk if it[0] == bb))
-            lo, hi = blocks_in[0], blocks_in[-1]
-            assert blocks_in == list(range(lo, hi + 1))
-            keep.append(self._accumulate([(c, xo) for _, c, _, xo in chunk],
-                                         out[lo:hi + 1].view(torch.float64), begin))
-            self._check_flags(len(chunk))
-            del hold
-        _lib.check(self.lib.dcs_block_tail(_lib.ptr(out), k, self.adj_hi.ctypes.data, self.u_open.ctypes.data,
-                                           len(x_list), self._stream()))
+        out, _ = self._run(list(x_list), w)
         return out

@@ -13,9 +13,23 @@
 
 typedef double complex cplx;
 
-static inline uint64_t deposit(uint64_t x, const int *slots, int m) {
+/* byte address tables, as the reference's executors use (scan_plan.py:133-145):
+ * c = XOR over bytes b of T[b][(x >> 8b) & 255] */
+static void make_tables(const int *slots, int m, uint64_t T[8][256]) {
+    for (int b = 0; b < 8; ++b)
+        for (int v = 0; v < 256; ++v) {
+            uint64_t acc = 0;
+            for (int t = 0; t < 8; ++t) {
+                const int i = 8 * b + t;
+                if (i < m && ((v >> t) & 1)) acc |= 1ull << slots[i];
+            }
+            T[b][v] = acc;
+        }
+}
+
+static inline uint64_t deposit_t(uint64_t x, uint64_t T[8][256], int nb) {
     uint64_t c = 0;
-    for (int i = 0; i < m; ++i) c |= ((x >> i) & 1ull) << slots[i];
+    for (int b = 0; b < nb; ++b) c ^= T[b][(x >> (8 * b)) & 255];
     return c;
 }
 
@@ -46,9 +60,13 @@ double oracle_run_steps(const uint64_t *steps, const double *params, int first, 
         const int m = mask_slots(d[5], slots);
         const int mo = mask_slots(d[6], oslots);
         const int64_t n = (int64_t)1 << m;
+        static uint64_t Ti[8][256], To[8][256];
+        make_tables(slots, m, Ti);
+        make_tables(oslots, mo, To);
+        const int nbi = (m + 7) / 8, nbo = (mo + 7) / 8;
 #pragma omp parallel for schedule(static)
         for (int64_t x = 0; x < n; ++x) {
-            const uint64_t c = deposit((uint64_t)x, slots, m);
+            const uint64_t c = deposit_t((uint64_t)x, Ti, nbi);
             const cplx a = E[c];
             switch (kind) {
                 case 0: E[c] = f0 * a; E[c | pbit] = f1 * a * sgn(c, beta, ov); break;
@@ -72,7 +90,7 @@ double oracle_run_steps(const uint64_t *steps, const double *params, int first, 
         double mx = 0.0;
 #pragma omp parallel for reduction(max : mx) schedule(static)
         for (int64_t x = 0; x < no; ++x) {
-            const double v = cabs(E[deposit((uint64_t)x, oslots, mo)]);
+            const double v = cabs(E[deposit_t((uint64_t)x, To, nbo)]);
             if (v > mx) mx = v;
         }
         if (mx > 0.0) {
@@ -80,7 +98,7 @@ double oracle_run_steps(const uint64_t *steps, const double *params, int first, 
             frexp(mx, &e);
             const double sc = ldexp(1.0, -e);
 #pragma omp parallel for schedule(static)
-            for (int64_t x = 0; x < no; ++x) E[deposit((uint64_t)x, oslots, mo)] *= sc;
+            for (int64_t x = 0; x < no; ++x) E[deposit_t((uint64_t)x, To, nbo)] *= sc;
             ls += e * log(2.0);
         }
     }
