@@ -47,6 +47,7 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--seed", type=int, default=24520)
+    ap.add_argument("--tune", action="store_true", help="autotune the fused tile shape before timing")
     return ap.parse_args()
 
 
@@ -207,6 +208,9 @@ def gpu_arm(args):
     eng = InplaceConditionalBlockGPU(w["graph"], w["unitaries"], w["n"], w["order"], w["parity_operations"],
                                      w["open_vertices"])
     eng.alloc(np.complex64, device=local, mode=args.mode)
+    tune_report = None
+    if args.mode == "fused" and args.tune:
+        tune_report = eng.autotune()
     setup_s = time.perf_counter() - t0
     k = eng.k
     total = args.warmup + args.steps
@@ -295,6 +299,7 @@ def gpu_arm(args):
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         e2e_elapsed = float(t.item())
 
+    fused_cfg = getattr(eng, "fused_config", None)
     # ---- plain per-sample path (one launch + one host max read per step), same workload
     plain = None
     if not args.no_plain and args.plain_samples > 0 and rank == 0:
@@ -348,7 +353,9 @@ def gpu_arm(args):
                 "plain": plain, "speedup_vs_plain": (value / plain["value"]) if plain else None,
                 "draws": {"indices": [int(d["index"]) for d in draws[args.warmup:total]],
                           "ties": int(sum(int(d["tie"]) for d in draws[args.warmup:total]))},
-                "clocks": clk, "setup_s": setup_s, "cpu_baseline": cb}
+                "clocks": clk, "setup_s": setup_s, "cpu_baseline": cb,
+                "fused_config": fused_cfg,
+                "autotune": tune_report}
         print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.barrier()

@@ -1,0 +1,96 @@
+"""Autotuner for the fused executor's tile shape.
+
+For a plan, each candidate (max tile dimension, contiguous low bits, max steps per group)
+gives a different grouping of the vertex steps (``fused.group_steps``).  The tuner times one
+slice contraction per candidate with CUDA events on the engine's own table and keeps the
+fastest; results are cached per plan fingerprint in ``autotune_cache.json`` next to this file.
+"""
+from __future__ import annotations
+
+import hashlib
+import json
+from pathlib import Path
+
+import numpy as np
+
+from . import _lib
+
+CACHE = Path(__file__).resolve().parent / "autotune_cache.json"
+CANDIDATES = [(13, 4, 24), (12, 4, 24), (13, 3, 24), (14, 4, 24), (13, 5, 24), (12, 3, 24), (11, 4, 24),
+              (13, 4, 12)]
+
+
+def fingerprint(plan):
+    h = hashlib.sha256()
+    for st in plan.steps:
+        h.update(repr((st.kind, st.active_in, st.active_out, st.beta, st.K, st.Ka, st.pivot, st.pivot_a)).encode())
+    return h.hexdigest()[:20]
+
+
+def _load():
+    if CACHE.exists():
+        try:
+            return json.loads(CACHE.read_text())
+        except ValueError:
+            return {}
+    return {}
+
+
+def cached(plan, device_name):
+    return _load().get(f"{fingerprint(plan)}|{device_name}")
+
+
+def tune(engine, params_dev, candidates=CANDIDATES, repeats=1, save=True):
+    """Time each candidate on the engine (mode "fused", already allocated) and install the best.
+
+    params_dev: device params of one work item (nsteps dcs_param).  Returns the report."""
+    import torch
+    from .fused import build_fused_plan
+    lib = engine.lib
+    stream = torch.cuda.current_stream(engine.device)
+    report = []
+    best = None
+    for cand in candidates:
+        max_dim, low, max_steps = cand
+        try:
+            fp = build_fused_plan(engine.plan, max_dim=max_dim, low=low, max_steps=max_steps)
+        except ValueError:
+            continue
+        need = len(fp.groups) + 1
+        if engine.maxbits.numel() < need:
+            engine.maxbits = torch.zeros(need, dtype=torch.int64, device=engine.device)
+        times = []
+        for _ in range(repeats + 1):
+            mb = engine.maxbits
+            mb.zero_()
+            mb[0] = engine.one_bits
+            engine.scale.zero_()
+            engine.table.view(engine.items, engine.table_stride)[:1, 0] = 1
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            _lib.check(lib.dcs_fused_groups(_lib.ptr(engine.table), fp.dsteps.ctypes.data, len(fp.dsteps),
+                                            fp.groups.ctypes.data, len(fp.groups), fp.tile_steps.ctypes.data,
+                                            _lib.ptr(params_dev), 0, len(fp.groups), _lib.ptr(mb),
+                                            _lib.ptr(engine.scale), stream.cuda_stream))
+            b.record(stream)
+            torch.cuda.synchronize(engine.device)
+            times.append(a.elapsed_time(b) / 1000.0)
+        t = min(times[1:]) if len(times) > 1 else times[0]
+        report.append({"max_dim": max_dim, "low": low, "max_steps": max_steps, "groups": len(fp.groups),
+                       "seconds": t})
+        if best is None or t < best[0]:
+            best = (t, cand, fp)
+    engine.fplan = best[2]
+    nm = len(best[2].groups) + 1
+    engine.maxbits = torch.zeros(engine.items * nm, dtype=torch.int64, device=engine.device)
+    if save:
+        data = _load()
+        data[f"{fingerprint(engine.plan)}|{torch.cuda.get_device_name(engine.device)}"] = {
+            "max_dim": best[1][0], "low": best[1][1], "max_steps": best[1][2], "seconds": best[0]}
+        try:
+            CACHE.write_text(json.dumps(data, indent=1) + "\n")
+        except OSError:
+            pass
+    return {"best": {"max_dim": best[1][0], "low": best[1][1], "max_steps": best[1][2], "seconds": best[0]},
+            "candidates": report}

@@ -20,12 +20,15 @@ constexpr int kMaxSteps = 24;
 constexpr int kThreads = 256;
 
 struct FusedStep {
-    uint64_t K, Ka, beta, enum_mask, pbit;
-    uint32_t tK, tKa, tpiv;
-    int32_t kind;
-    int32_t pidx;
-    int32_t pad;
+    uint64_t K, Ka, beta, notin;
+    uint32_t tK, tKa, tpiv, tbeta;
+    int32_t kind, pidx;
+    uint8_t sK, sKa, nins, rho1, rho2, rb1, rb2, pad;
 };
+
+__device__ __forceinline__ uint32_t insert0(uint32_t o, int p) {
+    return ((o >> p) << (p + 1)) | (o & ((1u << p) - 1u));
+}
 
 struct FusedArgs {
     int32_t count, tile_dim, low_bits, coset_m, ncoset_runs, group;
@@ -93,60 +96,69 @@ k_fused(float2* __restrict__ E, const __grid_constant__ FusedArgs A, const dcs_p
             const FusedStep& st = A.st[s];
             const float4 w = fw[s];
             const float2 f0 = f2(w.x, w.y), f1 = f2(w.z, w.w);
-            const int ov = ovy[s] & 1, y = ovy[s] >> 1;
-            const uint64_t notenum = ~st.enum_mask, beta = st.beta;
+            const int y = ovy[s] >> 1;
+            // tile-constant part of the sign: parity(base & beta) ^ ov
+            const int cs = (__popcll(base & st.beta) & 1) ^ (ovy[s] & 1);
             const int kind = st.kind;
-            for (int t = threadIdx.x; t < T; t += kThreads) {
-                const uint64_t a = base ^ hi_tab[t >> low] ^ ((uint64_t)t & lowmask);
-                if (a & notenum) continue;  // not an orbit representative of this step
+            const int nrep = T >> st.nins;
+            for (int o = threadIdx.x; o < nrep; o += kThreads) {
+                uint32_t t = (uint32_t)o;
+                if (st.nins >= 1) t = insert0(t, st.rho1);
+                if (st.nins == 2) t = insert0(t, st.rho2);
+                uint64_t a = base ^ hi_tab[t >> low] ^ ((uint64_t)t & lowmask);
+                // role: the orbit entry whose pivot slots are zero
+                if (kind == DCS_KIND_GROW) {
+                    if ((a >> st.rb1) & 1) { t ^= st.tpiv; a ^= 1ull << st.rb1; }
+                } else if (kind == DCS_KIND_MIX) {
+                    if ((a >> st.rb1) & 1) { t ^= st.tKa; a ^= st.Ka; }
+                } else if (kind == DCS_KIND_SHRINK4) {
+                    if ((a >> st.rb1) & 1) { t ^= st.tK; a ^= st.K; }
+                    if ((a >> st.rb2) & 1) { t ^= st.tKa; a ^= st.Ka; }
+                } else if (kind != DCS_KIND_DIAG && kind != DCS_KIND_FIXED) {
+                    if ((a >> st.rb1) & 1) { t ^= st.tK; a ^= st.K; }
+                }
+                if (a & st.notin) continue;  // orbit outside the active slots of this step
+                const int sc_ = (__popc(t & st.tbeta) & 1) ^ cs;
                 const float2 x = sh[t];
                 switch (kind) {
                     case DCS_KIND_GROW: {
                         sh[t] = cmul(f0, x);
-                        sh[t ^ st.tpiv] = cmul(f1, cneg_if(x, neg_sign(a, beta, ov)));
+                        sh[t ^ st.tpiv] = cmul(f1, cneg_if(x, sc_));
                     } break;
                     case DCS_KIND_MIX: {
-                        const int td = t ^ st.tKa;
-                        const uint64_t d = a ^ st.Ka;
+                        const uint32_t td = t ^ st.tKa;
                         const float2 b = sh[td];
-                        sh[t] = cadd(cmul(f0, x), cmul(f1, cneg_if(b, neg_sign(d, beta, ov))));
-                        sh[td] = cadd(cmul(f0, b), cmul(f1, cneg_if(x, neg_sign(a, beta, ov))));
+                        sh[t] = cadd(cmul(f0, x), cmul(f1, cneg_if(b, sc_ ^ st.sKa)));
+                        sh[td] = cadd(cmul(f0, b), cmul(f1, cneg_if(x, sc_)));
                     } break;
                     case DCS_KIND_DIAG: {
-                        sh[t] = cmul(cadd(f0, cneg_if(f1, neg_sign(a, beta, ov))), x);
+                        sh[t] = cmul(cadd(f0, cneg_if(f1, sc_)), x);
                     } break;
                     case DCS_KIND_REPLACE: {
-                        const int td = t ^ st.tK;
-                        const uint64_t d = a ^ st.K;
+                        const uint32_t td = t ^ st.tK;
                         const float2 b = sh[td];
                         sh[t] = cmul(f0, cadd(x, b));
-                        sh[td] = cmul(f1, cadd(cneg_if(x, neg_sign(a, beta, ov)), cneg_if(b, neg_sign(d, beta, ov))));
+                        sh[td] = cmul(f1, cadd(cneg_if(x, sc_), cneg_if(b, sc_ ^ st.sK)));
                     } break;
                     case DCS_KIND_FIXED: {
-                        sh[t] = cmul(y ? cneg_if(f1, neg_sign(a, beta, ov)) : f0, x);
+                        sh[t] = cmul(y ? cneg_if(f1, sc_) : f0, x);
                     } break;
                     case DCS_KIND_FIXED_SHRINK: {
-                        const int td = t ^ st.tK;
-                        const uint64_t d = a ^ st.K;
+                        const uint32_t td = t ^ st.tK;
                         const float2 b = sh[td];
-                        sh[t] = y ? cmul(f1, cadd(cneg_if(x, neg_sign(a, beta, ov)), cneg_if(b, neg_sign(d, beta, ov))))
-                                  : cmul(f0, cadd(x, b));
+                        sh[t] = y ? cmul(f1, cadd(cneg_if(x, sc_), cneg_if(b, sc_ ^ st.sK))) : cmul(f0, cadd(x, b));
                     } break;
                     case DCS_KIND_SHRINK4: {
-                        const int t1 = t ^ st.tK, td = t ^ st.tKa, td1 = td ^ st.tK;
-                        const uint64_t c1 = a ^ st.K, d = a ^ st.Ka, d1 = d ^ st.K;
+                        const uint32_t t1 = t ^ st.tK, td = t ^ st.tKa, td1 = td ^ st.tK;
                         const float2 b = sh[t1], g = sh[td], h = sh[td1];
-                        sh[t] = cadd(cmul(f0, cadd(x, b)),
-                                     cmul(f1, cadd(cneg_if(g, neg_sign(d, beta, ov)), cneg_if(h, neg_sign(d1, beta, ov)))));
-                        sh[td] = cadd(cmul(f0, cadd(g, h)),
-                                      cmul(f1, cadd(cneg_if(x, neg_sign(a, beta, ov)), cneg_if(b, neg_sign(c1, beta, ov)))));
+                        const int sd = sc_ ^ st.sKa;
+                        sh[t] = cadd(cmul(f0, cadd(x, b)), cmul(f1, cadd(cneg_if(g, sd), cneg_if(h, sd ^ st.sK))));
+                        sh[td] = cadd(cmul(f0, cadd(g, h)), cmul(f1, cadd(cneg_if(x, sc_), cneg_if(b, sc_ ^ st.sK))));
                     } break;
                     default: {  // DCS_KIND_SHRINK2
-                        const int td = t ^ st.tK;
-                        const uint64_t d = a ^ st.K;
+                        const uint32_t td = t ^ st.tK;
                         const float2 b = sh[td];
-                        sh[t] = cadd(cmul(cadd(f0, cneg_if(f1, neg_sign(a, beta, ov))), x),
-                                     cmul(cadd(f0, cneg_if(f1, neg_sign(d, beta, ov))), b));
+                        sh[t] = cadd(cmul(cadd(f0, cneg_if(f1, sc_)), x), cmul(cadd(f0, cneg_if(f1, sc_ ^ st.sK)), b));
                     } break;
                 }
             }
@@ -209,18 +221,17 @@ extern "C" int dcs_fused_groups(void* table, const dcs_step* steps, int nsteps, 
             const dcs_step& d = steps[g.first + s];
             const dcs_tile_step& ts = tile_steps[g.step_tile_off + s];
             FusedStep& f = A.st[s];
-            f.K = d.K; f.Ka = d.Ka; f.beta = d.beta; f.pbit = d.pivot_bit;
-            // orbit representatives: enumerated slots only (omitted pivots must be zero)
-            uint64_t en = 0;
-            for (int r = 0; r < d.nruns; ++r) {
-                const uint32_t w = d.runs[r];
-                const int dst = (w >> 8) & 255, len = (w >> 16) & 255;
-                en |= (len >= 64 ? ~0ull : ((1ull << len) - 1)) << dst;
-            }
-            f.enum_mask = en;
-            f.tK = ts.tK; f.tKa = ts.tKa; f.tpiv = ts.tpiv;
+            f.K = d.K; f.Ka = d.Ka; f.beta = d.beta; f.notin = ~d.in_mask;
+            f.tK = ts.tK; f.tKa = ts.tKa; f.tpiv = ts.tpiv; f.tbeta = ts.tbeta;
+            f.sK = ts.sK; f.sKa = ts.sKa; f.nins = ts.nins; f.rho1 = ts.rho1; f.rho2 = ts.rho2;
+            f.rb1 = ts.rb1; f.rb2 = ts.rb2;
             f.kind = d.kind;
             f.pidx = g.first + s;
+            if (f.nins > 2 || (f.nins >= 1 && f.rho1 >= g.tile_dim) || (f.nins == 2 && (f.rho2 >= g.tile_dim ||
+                f.rho2 <= f.rho1)) || f.rb1 > 63 || f.rb2 > 63 || (f.tK | f.tKa | f.tpiv) >> g.tile_dim) {
+                dcs_host::set_error("dcs_fused_groups: malformed tile step %d", g.first + s);
+                return DCS_E_ARG;
+            }
         }
         const size_t smem = sizeof(float2) * ((size_t)1 << g.tile_dim) +
                             sizeof(uint64_t) * ((size_t)1 << (g.tile_dim - g.low_bits));

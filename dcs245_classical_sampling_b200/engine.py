@@ -212,8 +212,12 @@ class InplaceConditionalBlockGPU:
             items = max(1, min(nslice_items, budget // (table_entries * entry)))
         self.items = int(items)
         if mode == "fused":
+            from .autotune import cached
             from .fused import build_fused_plan
-            self.fplan = build_fused_plan(plan)
+            cfg = cached(plan, torch.cuda.get_device_name(self.device)) or {}
+            self.fused_config = {"max_dim": cfg.get("max_dim", 13), "low": cfg.get("low", 4),
+                                 "max_steps": cfg.get("max_steps", 24)}
+            self.fplan = build_fused_plan(plan, **self.fused_config)
             self.items = 1
         self.table = torch.empty(self.items * table_entries, dtype=tdtype, device=self.device)
         self.table_stride = table_entries
@@ -244,6 +248,20 @@ class InplaceConditionalBlockGPU:
 
     def _nmax(self):
         return len(self.fplan.groups) if self.mode == "fused" else self.nsteps
+
+    def autotune(self, x_bits=None, candidates=None):
+        """Time the fused tile-shape candidates on this engine's table and keep the fastest."""
+        from . import autotune as at
+        if self.mode != "fused":
+            return None
+        x = np.zeros(self.n, np.uint8) if x_bits is None else x_bits
+        _, items = self.params.items(x)
+        prm = torch.from_numpy(items[0][1].view(np.int64).copy()).to(self.device)
+        rep = at.tune(self, prm, **({"candidates": candidates} if candidates else {}))
+        self.fused_config = {k: rep["best"][k] for k in ("max_dim", "low", "max_steps")}
+        self.scale = torch.zeros(self.items * _lib.SCALE_DTYPE.itemsize // 8, dtype=torch.int64,
+                                 device=self.device)
+        return rep
 
     # ------------------------------------------------------------------ execution
     def _stream(self):

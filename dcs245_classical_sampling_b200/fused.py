@@ -174,9 +174,37 @@ def build_fused_plan(plan, max_dim=13, low=4, max_steps=MAX_GROUP_STEPS, max_ext
             st = steps[s]
             kind, _ = orbit_kind(st)
             ts = tsteps[s]
-            ts["tK"] = coords(st.K) if kind in (3, 5, 6, 7) else 0
-            ts["tKa"] = coords(st.Ka) if kind in (1, 6) else 0
-            ts["tpiv"] = coords(1 << st.pivot) if kind == KIND_GROW else 0
+            tK = coords(st.K) if kind in (3, 5, 6, 7) else 0
+            tKa = coords(st.Ka) if kind in (1, 6) else 0
+            tpiv = coords(1 << st.pivot) if kind == KIND_GROW else 0
+            ts["tK"], ts["tKa"], ts["tpiv"] = tK, tKa, tpiv
+            # sign functional in tile coordinates: parity(a(t) & beta) = parity(base & beta) ^ parity(t & tbeta)
+            tbeta = st.beta & lowmask
+            for i, b in enumerate(basis):
+                if bin(b & st.beta).count("1") & 1:
+                    tbeta |= 1 << (l + i)
+            ts["tbeta"] = tbeta
+            par = lambda v: bin(v).count("1") & 1
+            ts["sK"], ts["sKa"] = par(tK & tbeta), par(tKa & tbeta)
+            # orbit representatives: zero bits inserted at rho1 (and rho2 for four-entry orbits)
+            if kind == KIND_GROW:
+                ins, rb1 = [tpiv.bit_length() - 1], st.pivot
+            elif kind == 1:
+                ins, rb1 = [tKa.bit_length() - 1], st.pivot_a
+            elif kind in (3, 5, 7):
+                ins, rb1 = [tK.bit_length() - 1], st.pivot
+            elif kind == 6:
+                r1 = tK.bit_length() - 1
+                t2 = tKa ^ (tK if (tKa >> r1) & 1 else 0)
+                ins, rb1 = [r1, t2.bit_length() - 1], st.pivot
+            else:
+                ins, rb1 = [], 0
+            ins = sorted(ins)
+            ts["nins"] = len(ins)
+            ts["rho1"] = ins[0] if ins else 0
+            ts["rho2"] = ins[1] if len(ins) > 1 else 0
+            ts["rb1"] = max(rb1, 0)
+            ts["rb2"] = max(st.pivot_a, 0) if kind == 6 else 0
         fp.universe.append(bin(U).count("1"))
         fp.tiles.append(1 << bin(cmask).count("1"))
         fp.dims.append(dim)

@@ -33,6 +33,9 @@ WORKLOADS = {
     "ring32_d37_t79_k14": (32, 37, 79, 1032, 14, 0),
     "ring48_d55_t177_k17": (48, 55, 177, 1048, 17, 0),
     "ring64_d73_t314_k20": (64, 73, 314, 1064, 20, 2),
+    # the complex128 audit plan of the same circuit: one more parity slice (rmax 33 -> 128 GiB
+    # complex128), like the reference's inplace_k3_fp64 next to inplace_k2_fp32
+    "ring64_d73_t314_k20_audit": (64, 73, 314, 1064, 20, 3),
 }
 
 

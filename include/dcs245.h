@@ -117,10 +117,18 @@ typedef struct dcs_group {
     uint32_t coset_runs[DCS_MAX_RUNS];
 } dcs_group;
 
-/* Per-step tile-coordinate masks used by the fused kernel (one per step of each group). */
+/* Per-step tile-coordinate data used by the fused kernel (one per step of each group).
+ * Orbit representatives are enumerated by inserting `nins` zero bits at tile bits rho1 < rho2;
+ * the representative's role (which entry is the one with zero pivot slots rb1, rb2) is fixed
+ * from its address.  Signs: parity(a & beta) = parity(base & beta) ^ parity(t & tbeta); the
+ * partner t ^ tK (t ^ tKa) flips it by sK (sKa). */
 typedef struct dcs_tile_step {
     uint32_t tK, tKa, tpiv; /* tile-coordinate masks of K, Ka, grow pivot */
-    uint32_t pad;
+    uint32_t tbeta;         /* sign functional in tile coordinates */
+    uint8_t sK, sKa;        /* parity(tK & tbeta), parity(tKa & tbeta) */
+    uint8_t nins, rho1, rho2;
+    uint8_t rb1, rb2;       /* physical pivot slots deciding the roles */
+    uint8_t pad;
 } dcs_tile_step;
 
 /* Result of one draw (device-side struct; the host copies it back). */

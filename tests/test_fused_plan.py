@@ -56,44 +56,71 @@ def emulate(bp, fp, params):
         sh = np.where((A & np.uint64(~inm & (2**64 - 1))) == 0, E[A.astype(np.int64)] * sc, 0)
         for s in range(first, first + count):
             st = steps[s]
-            kind, omit = P.orbit_kind(st)
-            enum = P.slot_mask([p for p in st.active_in if p not in omit])
+            kind, _ = P.orbit_kind(st)
             ts = fp.tile_steps[s]
             pr = params[s]
             f0, f1 = complex(pr["f0r"], pr["f0i"]), complex(pr["f1r"], pr["f1i"])
             ov, y = int(pr["ov"]), int(pr["y"])
-            rep = (A & np.uint64(~enum & (2**64 - 1))) == 0
-            ti, tj = np.nonzero(rep)
-            a = A[ti, tj]
+            tK, tKa, tpiv, tb = int(ts["tK"]), int(ts["tKa"]), int(ts["tpiv"]), int(ts["tbeta"])
+            nins = int(ts["nins"])
+            o = np.arange((1 << dim) >> nins, dtype=np.int64)
+            for rho in ([int(ts["rho1"])] if nins >= 1 else []) + ([int(ts["rho2"])] if nins == 2 else []):
+                o = ((o >> rho) << (rho + 1)) | (o & ((1 << rho) - 1))
+            t = np.broadcast_to(o, (len(bases), len(o))).copy()
+            a = A[np.arange(len(bases))[:, None], t]
+            def flip(cond, tm, am):
+                nonlocal t, a
+                t = np.where(cond, t ^ tm, t)
+                a = np.where(cond, a ^ np.uint64(am), a)
+            bit = lambda q: ((a >> np.uint64(q)) & np.uint64(1)).astype(bool)
+            if kind == P.KIND_GROW:
+                flip(bit(int(ts["rb1"])), tpiv, 1 << int(ts["rb1"]))
+            elif kind == P.KIND_MIX:
+                flip(bit(int(ts["rb1"])), tKa, st.Ka)
+            elif kind == P.KIND_SHRINK4:
+                flip(bit(int(ts["rb1"])), tK, st.K)
+                flip(bit(int(ts["rb2"])), tKa, st.Ka)
+            elif kind not in (P.KIND_DIAG, P.KIND_FIXED):
+                flip(bit(int(ts["rb1"])), tK, st.K)
+            inm = P.slot_mask(st.active_in)
+            act = (a & np.uint64(~inm & (2**64 - 1))) == 0
+            ti = np.nonzero(act)[0]
+            tj = t[act]
+            # tile-coordinate sign functional against the direct physical parity
+            cs = np.array([bin(int(bb) & st.beta).count("1") & 1 for bb in bases], np.int64)[ti] ^ ov
+            pc = np.array([bin(int(v) & tb).count("1") & 1 for v in tj], np.int64)
+            sc = pc ^ cs
+            assert np.array_equal(sc, _neg(a[act], st.beta, ov).astype(np.int64))
+            sgn = lambda bits: np.where(bits, -1.0, 1.0)
             x = sh[ti, tj].copy()
-            sg = lambda addr: np.where(_neg(addr, st.beta, ov), -1.0, 1.0)
+            sK, sKa = int(ts["sK"]), int(ts["sKa"])
             if kind == P.KIND_GROW:
                 sh[ti, tj] = f0 * x
-                sh[ti, tj ^ int(ts["tpiv"])] = f1 * x * sg(a)
+                sh[ti, tj ^ tpiv] = f1 * x * sgn(sc)
             elif kind == P.KIND_MIX:
-                td = tj ^ int(ts["tKa"]); b = sh[ti, td].copy(); d = a ^ np.uint64(st.Ka)
-                sh[ti, tj] = f0 * x + f1 * sg(d) * b
-                sh[ti, td] = f0 * b + f1 * sg(a) * x
+                td = tj ^ tKa; b = sh[ti, td].copy()
+                sh[ti, tj] = f0 * x + f1 * sgn(sc ^ sKa) * b
+                sh[ti, td] = f0 * b + f1 * sgn(sc) * x
             elif kind == P.KIND_DIAG:
-                sh[ti, tj] = (f0 + f1 * sg(a)) * x
+                sh[ti, tj] = (f0 + f1 * sgn(sc)) * x
             elif kind == P.KIND_REPLACE:
-                td = tj ^ int(ts["tK"]); b = sh[ti, td].copy(); d = a ^ np.uint64(st.K)
+                td = tj ^ tK; b = sh[ti, td].copy()
                 sh[ti, tj] = f0 * (x + b)
-                sh[ti, td] = f1 * (sg(a) * x + sg(d) * b)
+                sh[ti, td] = f1 * (sgn(sc) * x + sgn(sc ^ sK) * b)
             elif kind == P.KIND_FIXED:
-                sh[ti, tj] = (f1 * sg(a) if y else f0) * x
+                sh[ti, tj] = (f1 * sgn(sc) if y else f0) * x
             elif kind == P.KIND_FIXED_SHRINK:
-                td = tj ^ int(ts["tK"]); b = sh[ti, td].copy(); d = a ^ np.uint64(st.K)
-                sh[ti, tj] = f1 * (sg(a) * x + sg(d) * b) if y else f0 * (x + b)
+                td = tj ^ tK; b = sh[ti, td].copy()
+                sh[ti, tj] = f1 * (sgn(sc) * x + sgn(sc ^ sK) * b) if y else f0 * (x + b)
             elif kind == P.KIND_SHRINK4:
-                t1 = tj ^ int(ts["tK"]); td = tj ^ int(ts["tKa"]); td1 = td ^ int(ts["tK"])
+                t1 = tj ^ tK; td = tj ^ tKa; td1 = td ^ tK
                 b, gg, h = sh[ti, t1].copy(), sh[ti, td].copy(), sh[ti, td1].copy()
-                c1 = a ^ np.uint64(st.K); d = a ^ np.uint64(st.Ka); d1 = d ^ np.uint64(st.K)
-                sh[ti, tj] = f0 * (x + b) + f1 * (sg(d) * gg + sg(d1) * h)
-                sh[ti, td] = f0 * (gg + h) + f1 * (sg(a) * x + sg(c1) * b)
+                sd = sc ^ sKa
+                sh[ti, tj] = f0 * (x + b) + f1 * (sgn(sd) * gg + sgn(sd ^ sK) * h)
+                sh[ti, td] = f0 * (gg + h) + f1 * (sgn(sc) * x + sgn(sc ^ sK) * b)
             else:
-                td = tj ^ int(ts["tK"]); b = sh[ti, td].copy(); d = a ^ np.uint64(st.K)
-                sh[ti, tj] = (f0 + f1 * sg(a)) * x + (f0 + f1 * sg(d)) * b
+                td = tj ^ tK; b = sh[ti, td].copy()
+                sh[ti, tj] = (f0 + f1 * sgn(sc)) * x + (f0 + f1 * sgn(sc ^ sK)) * b
         outm = P.slot_mask(steps[first + count - 1].active_out)
         keep = (A & np.uint64(~outm & (2**64 - 1))) == 0
         E[A[keep].astype(np.int64)] = sh[keep]
