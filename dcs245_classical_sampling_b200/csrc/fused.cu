@@ -17,7 +17,7 @@ using namespace dcs;
 namespace {
 
 constexpr int kMaxSteps = 24;
-constexpr int kThreads = 256;
+constexpr int kThreads = 512;
 
 struct FusedStep {
     uint64_t K, Ka, beta, notin;
@@ -25,10 +25,6 @@ struct FusedStep {
     int32_t kind, pidx;
     uint8_t sK, sKa, nins, rho1, rho2, rb1, rb2, pad;
 };
-
-__device__ __forceinline__ uint32_t insert0(uint32_t o, int p) {
-    return ((o >> p) << (p + 1)) | (o & ((1u << p) - 1u));
-}
 
 struct FusedArgs {
     int32_t count, tile_dim, low_bits, coset_m, ncoset_runs, group;
@@ -39,6 +35,86 @@ struct FusedArgs {
 };
 
 __device__ __forceinline__ float2 f2(float x, float y) { return make_float2(x, y); }
+
+__device__ __forceinline__ uint32_t insert0(uint32_t o, int p) {
+    return ((o >> p) << (p + 1)) | (o & ((1u << p) - 1u));
+}
+
+// (-1)^s * a by flipping the sign bits
+__device__ __forceinline__ float2 negif(float2 a, int s) {
+    const uint32_t m = (uint32_t)s << 31;
+    return f2(__uint_as_float(__float_as_uint(a.x) ^ m), __uint_as_float(__float_as_uint(a.y) ^ m));
+}
+// f * x
+__device__ __forceinline__ float2 fmul(float2 f, float2 x) {
+    return f2(fmaf(f.x, x.x, -f.y * x.y), fmaf(f.x, x.y, f.y * x.x));
+}
+// acc + f * x
+__device__ __forceinline__ float2 fmadd(float2 f, float2 x, float2 acc) {
+    return f2(fmaf(f.x, x.x, fmaf(-f.y, x.y, acc.x)), fmaf(f.x, x.y, fmaf(f.y, x.x, acc.y)));
+}
+
+// One vertex step over every orbit representative of the tile.  Representatives are the tile
+// indices with zero bits at the role-slot coordinates (rho1, rho2); orbits whose entries are
+// inactive at this step are computed too: they contain only inactive entries, which are
+// rewritten by a grow before any active read, and are neither stored nor in the max.
+template <int KIND>
+__device__ __forceinline__ void run_step(float2* __restrict__ sh, int T, const FusedStep& st, float2 f0, float2 f1,
+                                         int cs, int y) {
+    constexpr int nins = (KIND == DCS_KIND_SHRINK4) ? 2 : (KIND == DCS_KIND_DIAG || KIND == DCS_KIND_FIXED) ? 0 : 1;
+    const int nrep = T >> nins;
+    const uint32_t tbeta = st.tbeta;
+    const int rho1 = st.rho1, rho2 = st.rho2;
+    for (int o = threadIdx.x; o < nrep; o += kThreads) {
+        uint32_t t = (uint32_t)o;
+        if constexpr (nins >= 1) t = insert0(t, rho1);
+        if constexpr (nins == 2) t = insert0(t, rho2);
+        const int sc = (__popc(t & tbeta) & 1) ^ cs;
+        const float2 x = sh[t];
+        if constexpr (KIND == DCS_KIND_GROW) {
+            sh[t] = fmul(f0, x);
+            sh[t ^ st.tpiv] = negif(fmul(f1, x), sc);
+        } else if constexpr (KIND == DCS_KIND_MIX) {
+            const uint32_t td = t ^ st.tKa;
+            const float2 b = sh[td];
+            sh[t] = fmadd(f0, x, negif(fmul(f1, b), sc ^ st.sKa));
+            sh[td] = fmadd(f0, b, negif(fmul(f1, x), sc));
+        } else if constexpr (KIND == DCS_KIND_DIAG) {
+            sh[t] = fmadd(f0, x, negif(fmul(f1, x), sc));
+        } else if constexpr (KIND == DCS_KIND_REPLACE) {
+            const uint32_t td = t ^ st.tK;
+            const float2 b = sh[td];
+            sh[t] = fmul(f0, f2(x.x + b.x, x.y + b.y));
+            const float2 u = negif(x, sc), v = negif(b, sc ^ st.sK);
+            sh[td] = fmul(f1, f2(u.x + v.x, u.y + v.y));
+        } else if constexpr (KIND == DCS_KIND_FIXED) {
+            sh[t] = y ? negif(fmul(f1, x), sc) : fmul(f0, x);
+        } else if constexpr (KIND == DCS_KIND_FIXED_SHRINK) {
+            const uint32_t td = t ^ st.tK;
+            const float2 b = sh[td];
+            if (y) {
+                const float2 u = negif(x, sc), v = negif(b, sc ^ st.sK);
+                sh[t] = fmul(f1, f2(u.x + v.x, u.y + v.y));
+            } else {
+                sh[t] = fmul(f0, f2(x.x + b.x, x.y + b.y));
+            }
+        } else if constexpr (KIND == DCS_KIND_SHRINK4) {
+            const uint32_t t1 = t ^ st.tK, td = t ^ st.tKa, td1 = td ^ st.tK;
+            const float2 b = sh[t1], g = sh[td], h = sh[td1];
+            const int sd = sc ^ st.sKa;
+            const float2 gg = negif(g, sd), hh = negif(h, sd ^ st.sK);
+            const float2 xx = negif(x, sc), bb = negif(b, sc ^ st.sK);
+            sh[t] = fmadd(f1, f2(gg.x + hh.x, gg.y + hh.y), fmul(f0, f2(x.x + b.x, x.y + b.y)));
+            sh[td] = fmadd(f1, f2(xx.x + bb.x, xx.y + bb.y), fmul(f0, f2(g.x + h.x, g.y + h.y)));
+        } else {  // DCS_KIND_SHRINK2
+            const uint32_t td = t ^ st.tK;
+            const float2 b = sh[td];
+            const float2 u = negif(x, sc), v = negif(b, sc ^ st.sK);
+            // (f0 + s_c f1) x + (f0 + s_d f1) b = f0 (x + b) + f1 (s_c x + s_d b)
+            sh[t] = fmadd(f1, f2(u.x + v.x, u.y + v.y), fmul(f0, f2(x.x + b.x, x.y + b.y)));
+        }
+    }
+}
 
 __global__ void __launch_bounds__(kThreads)
 k_fused(float2* __restrict__ E, const __grid_constant__ FusedArgs A, const dcs_param* __restrict__ params,
@@ -99,68 +175,15 @@ k_fused(float2* __restrict__ E, const __grid_constant__ FusedArgs A, const dcs_p
             const int y = ovy[s] >> 1;
             // tile-constant part of the sign: parity(base & beta) ^ ov
             const int cs = (__popcll(base & st.beta) & 1) ^ (ovy[s] & 1);
-            const int kind = st.kind;
-            const int nrep = T >> st.nins;
-            for (int o = threadIdx.x; o < nrep; o += kThreads) {
-                uint32_t t = (uint32_t)o;
-                if (st.nins >= 1) t = insert0(t, st.rho1);
-                if (st.nins == 2) t = insert0(t, st.rho2);
-                uint64_t a = base ^ hi_tab[t >> low] ^ ((uint64_t)t & lowmask);
-                // role: the orbit entry whose pivot slots are zero
-                if (kind == DCS_KIND_GROW) {
-                    if ((a >> st.rb1) & 1) { t ^= st.tpiv; a ^= 1ull << st.rb1; }
-                } else if (kind == DCS_KIND_MIX) {
-                    if ((a >> st.rb1) & 1) { t ^= st.tKa; a ^= st.Ka; }
-                } else if (kind == DCS_KIND_SHRINK4) {
-                    if ((a >> st.rb1) & 1) { t ^= st.tK; a ^= st.K; }
-                    if ((a >> st.rb2) & 1) { t ^= st.tKa; a ^= st.Ka; }
-                } else if (kind != DCS_KIND_DIAG && kind != DCS_KIND_FIXED) {
-                    if ((a >> st.rb1) & 1) { t ^= st.tK; a ^= st.K; }
-                }
-                if (a & st.notin) continue;  // orbit outside the active slots of this step
-                const int sc_ = (__popc(t & st.tbeta) & 1) ^ cs;
-                const float2 x = sh[t];
-                switch (kind) {
-                    case DCS_KIND_GROW: {
-                        sh[t] = cmul(f0, x);
-                        sh[t ^ st.tpiv] = cmul(f1, cneg_if(x, sc_));
-                    } break;
-                    case DCS_KIND_MIX: {
-                        const uint32_t td = t ^ st.tKa;
-                        const float2 b = sh[td];
-                        sh[t] = cadd(cmul(f0, x), cmul(f1, cneg_if(b, sc_ ^ st.sKa)));
-                        sh[td] = cadd(cmul(f0, b), cmul(f1, cneg_if(x, sc_)));
-                    } break;
-                    case DCS_KIND_DIAG: {
-                        sh[t] = cmul(cadd(f0, cneg_if(f1, sc_)), x);
-                    } break;
-                    case DCS_KIND_REPLACE: {
-                        const uint32_t td = t ^ st.tK;
-                        const float2 b = sh[td];
-                        sh[t] = cmul(f0, cadd(x, b));
-                        sh[td] = cmul(f1, cadd(cneg_if(x, sc_), cneg_if(b, sc_ ^ st.sK)));
-                    } break;
-                    case DCS_KIND_FIXED: {
-                        sh[t] = cmul(y ? cneg_if(f1, sc_) : f0, x);
-                    } break;
-                    case DCS_KIND_FIXED_SHRINK: {
-                        const uint32_t td = t ^ st.tK;
-                        const float2 b = sh[td];
-                        sh[t] = y ? cmul(f1, cadd(cneg_if(x, sc_), cneg_if(b, sc_ ^ st.sK))) : cmul(f0, cadd(x, b));
-                    } break;
-                    case DCS_KIND_SHRINK4: {
-                        const uint32_t t1 = t ^ st.tK, td = t ^ st.tKa, td1 = td ^ st.tK;
-                        const float2 b = sh[t1], g = sh[td], h = sh[td1];
-                        const int sd = sc_ ^ st.sKa;
-                        sh[t] = cadd(cmul(f0, cadd(x, b)), cmul(f1, cadd(cneg_if(g, sd), cneg_if(h, sd ^ st.sK))));
-                        sh[td] = cadd(cmul(f0, cadd(g, h)), cmul(f1, cadd(cneg_if(x, sc_), cneg_if(b, sc_ ^ st.sK))));
-                    } break;
-                    default: {  // DCS_KIND_SHRINK2
-                        const uint32_t td = t ^ st.tK;
-                        const float2 b = sh[td];
-                        sh[t] = cadd(cmul(cadd(f0, cneg_if(f1, sc_)), x), cmul(cadd(f0, cneg_if(f1, sc_ ^ st.sK)), b));
-                    } break;
-                }
+            switch (st.kind) {
+                case DCS_KIND_GROW: run_step<DCS_KIND_GROW>(sh, T, st, f0, f1, cs, y); break;
+                case DCS_KIND_MIX: run_step<DCS_KIND_MIX>(sh, T, st, f0, f1, cs, y); break;
+                case DCS_KIND_DIAG: run_step<DCS_KIND_DIAG>(sh, T, st, f0, f1, cs, y); break;
+                case DCS_KIND_REPLACE: run_step<DCS_KIND_REPLACE>(sh, T, st, f0, f1, cs, y); break;
+                case DCS_KIND_FIXED: run_step<DCS_KIND_FIXED>(sh, T, st, f0, f1, cs, y); break;
+                case DCS_KIND_FIXED_SHRINK: run_step<DCS_KIND_FIXED_SHRINK>(sh, T, st, f0, f1, cs, y); break;
+                case DCS_KIND_SHRINK4: run_step<DCS_KIND_SHRINK4>(sh, T, st, f0, f1, cs, y); break;
+                default: run_step<DCS_KIND_SHRINK2>(sh, T, st, f0, f1, cs, y); break;
             }
             __syncthreads();
         }
@@ -243,7 +266,7 @@ extern "C" int dcs_fused_groups(void* table, const dcs_step* steps, int nsteps, 
         const uint64_t ntiles = 1ull << g.coset_m;
         int per_sm = (int)((220 * 1024) / (smem + 2048));
         if (per_sm < 1) per_sm = 1;
-        if (per_sm > 8) per_sm = 8;
+        if (per_sm > 4) per_sm = 4;  // 512 threads per CTA: at most 4 CTAs per SM
         uint64_t grid = (uint64_t)sms * per_sm;
         if (grid > ntiles) grid = ntiles;
         k_fused<<<(unsigned)grid, kThreads, smem, st>>>((float2*)table, A, params, (unsigned long long*)maxbits, scale);

@@ -137,6 +137,19 @@ def build_fused_plan(plan, max_dim=13, low=4, max_steps=MAX_GROUP_STEPS, max_ext
             vecs += _orbit_vectors(st)
         l = _low_bits(U, low)
         basis, pivots = _reduced_basis(vecs, l)
+        # pad small tiles with unit vectors of the slot universe (longer contiguous rows first)
+        nU = bin(U).count("1")
+        while l + len(basis) < min(max_dim, nU):
+            if l < 6 and (U >> l) & 1 and l not in pivots:
+                l += 1
+                basis, pivots = _reduced_basis(vecs, l)
+                continue
+            span_piv = set(pivots) | set(range(l))
+            extra = next((q for q in range(64) if (U >> q) & 1 and q not in span_piv), None)
+            if extra is None:
+                break
+            vecs = vecs + [1 << extra]
+            basis, pivots = _reduced_basis(vecs, l)
         if len(basis) > MAX_BASIS:
             raise ValueError(f"group {gi}: {len(basis)} tile basis vectors exceed {MAX_BASIS}")
         dim = l + len(basis)
@@ -186,24 +199,28 @@ def build_fused_plan(plan, max_dim=13, low=4, max_steps=MAX_GROUP_STEPS, max_ext
             ts["tbeta"] = tbeta
             par = lambda v: bin(v).count("1") & 1
             ts["sK"], ts["sKa"] = par(tK & tbeta), par(tKa & tbeta)
-            # orbit representatives: zero bits inserted at rho1 (and rho2 for four-entry orbits)
+            # orbit representatives: the role slots (pivots of K, Ka, grow) are pivot positions of
+            # the reduced tile basis, so "slot q is zero" is "tile bit tbit(q) is zero"; inserting
+            # zero bits there enumerates exactly the entries c of the reference kernel
+            def tbit(q):
+                if q < l:
+                    return q
+                return l + pivots.index(q)
             if kind == KIND_GROW:
-                ins, rb1 = [tpiv.bit_length() - 1], st.pivot
+                ins = [tbit(st.pivot)]
             elif kind == 1:
-                ins, rb1 = [tKa.bit_length() - 1], st.pivot_a
+                ins = [tbit(st.pivot_a)]
             elif kind in (3, 5, 7):
-                ins, rb1 = [tK.bit_length() - 1], st.pivot
+                ins = [tbit(st.pivot)]
             elif kind == 6:
-                r1 = tK.bit_length() - 1
-                t2 = tKa ^ (tK if (tKa >> r1) & 1 else 0)
-                ins, rb1 = [r1, t2.bit_length() - 1], st.pivot
+                ins = [tbit(st.pivot), tbit(st.pivot_a)]
             else:
-                ins, rb1 = [], 0
+                ins = []
             ins = sorted(ins)
             ts["nins"] = len(ins)
             ts["rho1"] = ins[0] if ins else 0
             ts["rho2"] = ins[1] if len(ins) > 1 else 0
-            ts["rb1"] = max(rb1, 0)
+            ts["rb1"] = max(st.pivot_a if kind == 1 else st.pivot, 0)  # role slot(s), for checking
             ts["rb2"] = max(st.pivot_a, 0) if kind == 6 else 0
         fp.universe.append(bin(U).count("1"))
         fp.tiles.append(1 << bin(cmask).count("1"))

@@ -227,3 +227,22 @@ def test_reference_compatible_kernel(golden):
         term = block_ref._addr(oe.steps[-1]["active_out"]).astype(np.int64)
         got = E.cpu().numpy()[term].astype(np.complex128)
         assert rel_l2(got * math.exp(ls), want * math.exp(wls)) < tol
+
+
+def test_audit_pair_matches_reference_record(golden):
+    from dcs245_classical_sampling_b200.audit import audit_vector_pair, relative_l2
+    s, _ = golden("sampler")
+    for c in s["audit"]:
+        ref = np.array(c["ref_re"]) + 1j * np.array(c["ref_im"])
+        ap = np.array(c["ap_re"]) + 1j * np.array(c["ap_im"])
+        got = audit_vector_pair(ref, ap, 0)
+        for key in ("normalized_conditional_overlap_abs", "uncapped_overlap_witness", "reference_scaled_mass",
+                    "approximate_input_mass", "loss"):
+            assert got[key] == pytest.approx(c["result"][key], rel=1e-14, abs=1e-15), key
+    case, arrays = golden("c2")
+    want = arrays["block_0"]
+    eng = _engine(case, arrays, np.complex64, mode="fused")
+    v, _ = eng.block(_x(case["protocol"]["records"][0]))
+    rec = audit_vector_pair(torch.from_numpy(want).cuda(), v, 0)
+    assert rec["normalized_conditional_overlap_abs"] >= 0.9999
+    assert relative_l2(torch.from_numpy(want).cuda(), v) < 1e-5

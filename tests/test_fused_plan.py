@@ -68,29 +68,19 @@ def emulate(bp, fp, params):
                 o = ((o >> rho) << (rho + 1)) | (o & ((1 << rho) - 1))
             t = np.broadcast_to(o, (len(bases), len(o))).copy()
             a = A[np.arange(len(bases))[:, None], t]
-            def flip(cond, tm, am):
-                nonlocal t, a
-                t = np.where(cond, t ^ tm, t)
-                a = np.where(cond, a ^ np.uint64(am), a)
             bit = lambda q: ((a >> np.uint64(q)) & np.uint64(1)).astype(bool)
-            if kind == P.KIND_GROW:
-                flip(bit(int(ts["rb1"])), tpiv, 1 << int(ts["rb1"]))
-            elif kind == P.KIND_MIX:
-                flip(bit(int(ts["rb1"])), tKa, st.Ka)
-            elif kind == P.KIND_SHRINK4:
-                flip(bit(int(ts["rb1"])), tK, st.K)
-                flip(bit(int(ts["rb2"])), tKa, st.Ka)
-            elif kind not in (P.KIND_DIAG, P.KIND_FIXED):
-                flip(bit(int(ts["rb1"])), tK, st.K)
-            inm = P.slot_mask(st.active_in)
-            act = (a & np.uint64(~inm & (2**64 - 1))) == 0
-            ti = np.nonzero(act)[0]
-            tj = t[act]
-            # tile-coordinate sign functional against the direct physical parity
+            # every enumerated representative is the reference's c (zero role slots)
+            if nins >= 1:
+                assert not bit(int(ts["rb1"])).any()
+            if nins == 2:
+                assert not bit(int(ts["rb2"])).any()
+            # inactive orbits are computed too (the kernel does not test activity per orbit)
+            ti = np.repeat(np.arange(len(bases)), t.shape[1])
+            tj = t.reshape(-1)
             cs = np.array([bin(int(bb) & st.beta).count("1") & 1 for bb in bases], np.int64)[ti] ^ ov
             pc = np.array([bin(int(v) & tb).count("1") & 1 for v in tj], np.int64)
             sc = pc ^ cs
-            assert np.array_equal(sc, _neg(a[act], st.beta, ov).astype(np.int64))
+            assert np.array_equal(sc, _neg(a.reshape(-1), st.beta, ov).astype(np.int64))
             sgn = lambda bits: np.where(bits, -1.0, 1.0)
             x = sh[ti, tj].copy()
             sK, sKa = int(ts["sK"]), int(ts["sKa"])
