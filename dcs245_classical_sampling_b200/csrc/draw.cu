@@ -224,11 +224,13 @@ k_locate_elem(const double* __restrict__ w, int k, const dd* __restrict__ chunk_
     __syncthreads();
     if (found >= 0 && (unsigned long long)found == best) {
         dcs_draw_result& r = res[b];
-        const double lo = dd_div(p_before, T), hi = dd_div(p_at, T);
+        // math.fsum rounds each sum to double before the division (sampling_protocol.py:67-69);
+        // a normalised double-double's high word is that rounding
+        const double lo = __ddiv_rn(p_before.hi, T.hi), hi = __ddiv_rn(p_at.hi, T.hi);
         const double wi = loc[found - (int64_t)start - (int64_t)threadIdx.x * kPer];
         r.index = found;
         r.selected_weight = wi;
-        r.total_exact = T.hi + T.lo;
+        r.total_exact = T.hi;
         r.total_cdf = r.total_exact;
         r.cdf_lower_exact = lo;
         r.cdf_upper_exact = hi;
@@ -245,7 +247,7 @@ k_locate_elem(const double* __restrict__ w, int k, const dd* __restrict__ chunk_
     if (threadIdx.x == 0 && best == ~0ull) {
         // u*T beyond every accurate prefix (possible only within rounding of T): sequential path decides
         res[b].tie = 1;
-        res[b].total_exact = T.hi + T.lo;
+        res[b].total_exact = T.hi;
     }
 }
 
@@ -275,8 +277,8 @@ __global__ void k_sequential(const double* __restrict__ w, int k, BlockState* __
     }
     const dd T = state[b].total;
     r.cdf_lower = idx ? prev : 0.0;
-    r.cdf_lower_exact = dd_div(exact_prev, T);
-    r.cdf_upper_exact = dd_div(exact, T);
+    r.cdf_lower_exact = __ddiv_rn(exact_prev.hi, T.hi);
+    r.cdf_upper_exact = __ddiv_rn(exact.hi, T.hi);
     r.index = (int64_t)idx;
     r.total_cdf = S;
     r.selected_weight = wb[idx];

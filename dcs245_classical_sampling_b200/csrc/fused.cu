@@ -20,10 +20,11 @@ constexpr int kMaxSteps = 24;
 constexpr int kThreads = 512;
 
 struct FusedStep {
-    uint64_t K, Ka, beta, notin;
+    uint64_t beta, cskip;
     uint32_t tK, tKa, tpiv, tbeta;
     int32_t kind, pidx;
-    uint8_t sK, sKa, nins, rho1, rho2, rb1, rb2, pad;
+    uint8_t sK, sKa, nins, pad;
+    uint8_t ins[16];
 };
 
 struct FusedArgs {
@@ -54,22 +55,31 @@ __device__ __forceinline__ float2 fmadd(float2 f, float2 x, float2 acc) {
     return f2(fmaf(f.x, x.x, fmaf(-f.y, x.y, acc.x)), fmaf(f.x, x.y, fmaf(f.y, x.x, acc.y)));
 }
 
-// One vertex step over every orbit representative of the tile.  Representatives are the tile
-// indices with zero bits at the role-slot coordinates (rho1, rho2); orbits whose entries are
-// inactive at this step are computed too: they contain only inactive entries, which are
-// rewritten by a grow before any active read, and are neither stored nor in the max.
+// Spread the bits of o over the positions that are not in ins[0..n) (ascending): the inserted
+// positions become zero.  A bit injection, so spread(a | b) = spread(a) | spread(b).
+__device__ __forceinline__ uint32_t spread(uint32_t o, const uint8_t* ins, int n) {
+    for (int i = 0; i < n; ++i) o = insert0(o, ins[i]);
+    return o;
+}
+
+// One vertex step over every active orbit representative of the tile.  Representatives are the
+// tile indices with zero bits at ins[]: the role slots (so the index is the reference's entry c)
+// and the tile bits of slots inactive at this step (so every orbit touched is active).  The
+// index o = tid + 512 k is spread as spread(tid) | spread(512 k): the first part is fixed per
+// thread and step, the second is the same for every thread of the block.
 template <int KIND>
 __device__ __forceinline__ void run_step(float2* __restrict__ sh, int T, const FusedStep& st, float2 f0, float2 f1,
                                          int cs, int y) {
-    constexpr int nins = (KIND == DCS_KIND_SHRINK4) ? 2 : (KIND == DCS_KIND_DIAG || KIND == DCS_KIND_FIXED) ? 0 : 1;
+    const int nins = st.nins;
     const int nrep = T >> nins;
     const uint32_t tbeta = st.tbeta;
-    const int rho1 = st.rho1, rho2 = st.rho2;
-    for (int o = threadIdx.x; o < nrep; o += kThreads) {
-        uint32_t t = (uint32_t)o;
-        if constexpr (nins >= 1) t = insert0(t, rho1);
-        if constexpr (nins == 2) t = insert0(t, rho2);
-        const int sc = (__popc(t & tbeta) & 1) ^ cs;
+    const uint32_t tp = spread(threadIdx.x, st.ins, nins);
+    const int hs = (__popc(tp & tbeta) & 1) ^ cs;
+    for (int k = 0; (k * kThreads) < nrep; ++k) {
+        if ((int)threadIdx.x + k * kThreads >= nrep) break;
+        const uint32_t tu = spread((uint32_t)(k * kThreads), st.ins, nins);
+        const uint32_t t = tp | tu;
+        const int sc = hs ^ (__popc(tu & tbeta) & 1);
         const float2 x = sh[t];
         if constexpr (KIND == DCS_KIND_GROW) {
             sh[t] = fmul(f0, x);
@@ -175,7 +185,7 @@ k_fused(float2* __restrict__ E, const __grid_constant__ FusedArgs A, const dcs_p
             const int y = ovy[s] >> 1;
             // tile-constant part of the sign: parity(base & beta) ^ ov
             const int cs = (__popcll(base & st.beta) & 1) ^ (ovy[s] & 1);
-            switch (st.kind) {
+            if (!(base & st.cskip)) switch (st.kind) {
                 case DCS_KIND_GROW: run_step<DCS_KIND_GROW>(sh, T, st, f0, f1, cs, y); break;
                 case DCS_KIND_MIX: run_step<DCS_KIND_MIX>(sh, T, st, f0, f1, cs, y); break;
                 case DCS_KIND_DIAG: run_step<DCS_KIND_DIAG>(sh, T, st, f0, f1, cs, y); break;
@@ -244,14 +254,18 @@ extern "C" int dcs_fused_groups(void* table, const dcs_step* steps, int nsteps, 
             const dcs_step& d = steps[g.first + s];
             const dcs_tile_step& ts = tile_steps[g.step_tile_off + s];
             FusedStep& f = A.st[s];
-            f.K = d.K; f.Ka = d.Ka; f.beta = d.beta; f.notin = ~d.in_mask;
+            f.beta = d.beta;
+            f.cskip = ts.cskip;
             f.tK = ts.tK; f.tKa = ts.tKa; f.tpiv = ts.tpiv; f.tbeta = ts.tbeta;
-            f.sK = ts.sK; f.sKa = ts.sKa; f.nins = ts.nins; f.rho1 = ts.rho1; f.rho2 = ts.rho2;
-            f.rb1 = ts.rb1; f.rb2 = ts.rb2;
+            f.sK = ts.sK; f.sKa = ts.sKa; f.nins = ts.nins;
             f.kind = d.kind;
             f.pidx = g.first + s;
-            if (f.nins > 2 || (f.nins >= 1 && f.rho1 >= g.tile_dim) || (f.nins == 2 && (f.rho2 >= g.tile_dim ||
-                f.rho2 <= f.rho1)) || f.rb1 > 63 || f.rb2 > 63 || (f.tK | f.tKa | f.tpiv) >> g.tile_dim) {
+            bool bad = f.nins > 16 || f.nins > g.tile_dim || (f.tK | f.tKa | f.tpiv | f.tbeta) >> g.tile_dim;
+            for (int i = 0; i < f.nins && !bad; ++i) {
+                f.ins[i] = ts.ins[i];
+                bad = ts.ins[i] >= g.tile_dim || (i && ts.ins[i] <= ts.ins[i - 1]);
+            }
+            if (bad) {
                 dcs_host::set_error("dcs_fused_groups: malformed tile step %d", g.first + s);
                 return DCS_E_ARG;
             }

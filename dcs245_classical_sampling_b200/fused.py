@@ -206,20 +206,29 @@ def build_fused_plan(plan, max_dim=13, low=4, max_steps=MAX_GROUP_STEPS, max_ext
                 if q < l:
                     return q
                 return l + pivots.index(q)
+            role = []
             if kind == KIND_GROW:
-                ins = [tbit(st.pivot)]
+                role = [st.pivot]
             elif kind == 1:
-                ins = [tbit(st.pivot_a)]
+                role = [st.pivot_a]
             elif kind in (3, 5, 7):
-                ins = [tbit(st.pivot)]
+                role = [st.pivot]
             elif kind == 6:
-                ins = [tbit(st.pivot), tbit(st.pivot_a)]
-            else:
-                ins = []
-            ins = sorted(ins)
+                role = [st.pivot, st.pivot_a]
+            tilepos = set(range(l)) | set(pivots)
+            inactive = [q for q in range(64) if (U >> q) & 1 and not (slot_mask(st.active_in) >> q) & 1
+                        and q not in role]
+            ins = sorted([tbit(q) for q in role] + [tbit(q) for q in inactive if q in tilepos])
+            cskip = 0
+            for q in inactive:
+                if q not in tilepos:
+                    cskip |= 1 << q
+            if len(ins) > 16 or len(set(ins)) != len(ins):
+                raise ValueError(f"step {s}: {len(ins)} inserted tile bits")
             ts["nins"] = len(ins)
-            ts["rho1"] = ins[0] if ins else 0
-            ts["rho2"] = ins[1] if len(ins) > 1 else 0
+            for i, b in enumerate(ins):
+                ts["ins"][i] = b
+            ts["cskip"] = cskip
             ts["rb1"] = max(st.pivot_a if kind == 1 else st.pivot, 0)  # role slot(s), for checking
             ts["rb2"] = max(st.pivot_a, 0) if kind == 6 else 0
         fp.universe.append(bin(U).count("1"))

@@ -118,17 +118,21 @@ typedef struct dcs_group {
 } dcs_group;
 
 /* Per-step tile-coordinate data used by the fused kernel (one per step of each group).
- * Orbit representatives are enumerated by inserting `nins` zero bits at tile bits rho1 < rho2;
- * the representative's role (which entry is the one with zero pivot slots rb1, rb2) is fixed
- * from its address.  Signs: parity(a & beta) = parity(base & beta) ^ parity(t & tbeta); the
- * partner t ^ tK (t ^ tKa) flips it by sK (sKa). */
+ * Orbit representatives of step s are the tile indices with zero bits at ins[0..nins)
+ * (ascending): the role slots of the step (the zero pivots of the reference's entry c) and the
+ * slots of the group universe that are inactive at the step and lie on tile bits.  Inactive
+ * slots that are coset bits are in cskip: a tile whose base has one of them set skips the step.
+ * Signs: parity(a & beta) = parity(base & beta) ^ parity(t & tbeta); the partner t ^ tK
+ * (t ^ tKa) flips it by sK (sKa). */
 typedef struct dcs_tile_step {
+    uint64_t cskip;         /* inactive coset slots */
     uint32_t tK, tKa, tpiv; /* tile-coordinate masks of K, Ka, grow pivot */
     uint32_t tbeta;         /* sign functional in tile coordinates */
     uint8_t sK, sKa;        /* parity(tK & tbeta), parity(tKa & tbeta) */
-    uint8_t nins, rho1, rho2;
-    uint8_t rb1, rb2;       /* physical pivot slots deciding the roles */
-    uint8_t pad;
+    uint8_t nins;           /* number of inserted zero bits (<= 16) */
+    uint8_t rb1, rb2;       /* physical role slots (for checking) */
+    uint8_t pad[3];
+    uint8_t ins[16];        /* inserted tile bits, ascending */
 } dcs_tile_step;
 
 /* Result of one draw (device-side struct; the host copies it back). */

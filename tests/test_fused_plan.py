@@ -64,18 +64,23 @@ def emulate(bp, fp, params):
             tK, tKa, tpiv, tb = int(ts["tK"]), int(ts["tKa"]), int(ts["tpiv"]), int(ts["tbeta"])
             nins = int(ts["nins"])
             o = np.arange((1 << dim) >> nins, dtype=np.int64)
-            for rho in ([int(ts["rho1"])] if nins >= 1 else []) + ([int(ts["rho2"])] if nins == 2 else []):
+            for rho in [int(v) for v in ts["ins"][:nins]]:
                 o = ((o >> rho) << (rho + 1)) | (o & ((1 << rho) - 1))
             t = np.broadcast_to(o, (len(bases), len(o))).copy()
             a = A[np.arange(len(bases))[:, None], t]
             bit = lambda q: ((a >> np.uint64(q)) & np.uint64(1)).astype(bool)
-            # every enumerated representative is the reference's c (zero role slots)
-            if nins >= 1:
+            # every enumerated representative is the reference's c (zero role slots) and active,
+            # except in tiles skipped through an inactive coset slot
+            live = (bases & np.uint64(int(ts["cskip"]))) == 0
+            t, a = t[live], a[live]
+            bit = lambda q: ((a >> np.uint64(q)) & np.uint64(1)).astype(bool)
+            if kind in (0, 1, 3, 5, 6, 7):
                 assert not bit(int(ts["rb1"])).any()
-            if nins == 2:
+            if kind == 6:
                 assert not bit(int(ts["rb2"])).any()
-            # inactive orbits are computed too (the kernel does not test activity per orbit)
-            ti = np.repeat(np.arange(len(bases)), t.shape[1])
+            inm = P.slot_mask(st.active_in)
+            assert ((a & np.uint64(~inm & (2**64 - 1))) == 0).all()
+            ti = np.repeat(np.flatnonzero(live), t.shape[1])
             tj = t.reshape(-1)
             cs = np.array([bin(int(bb) & st.beta).count("1") & 1 for bb in bases], np.int64)[ti] ^ ov
             pc = np.array([bin(int(v) & tb).count("1") & 1 for v in tj], np.int64)
