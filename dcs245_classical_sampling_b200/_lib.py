@@ -33,7 +33,7 @@ GROUP_DTYPE = np.dtype([
 ])
 TILE_STEP_DTYPE = np.dtype([("cskip", "<u8"), ("tK", "<u4"), ("tKa", "<u4"), ("tpiv", "<u4"), ("tbeta", "<u4"),
                             ("sK", "<u1"), ("sKa", "<u1"), ("nins", "<u1"), ("rb1", "<u1"), ("rb2", "<u1"),
-                            ("pad", "<u1", (3,)), ("ins", "<u1", (16,))])
+                            ("pad", "<u1", (3,)), ("ins", "<u1", (16,)), ("mhi", "<u4"), ("pad2", "<u4")])
 DRAW_DTYPE = np.dtype([
     ("index", "<i8"), ("tie", "<i4"), ("status", "<i4"), ("total_cdf", "<f8"), ("total_exact", "<f8"),
     ("selected_weight", "<f8"), ("cdf_lower", "<f8"), ("cdf_upper", "<f8"), ("cdf_lower_exact", "<f8"),

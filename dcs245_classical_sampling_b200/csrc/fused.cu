@@ -25,6 +25,7 @@ struct FusedStep {
     int32_t kind, pidx;
     uint8_t sK, sKa, nins, pad;
     uint8_t ins[16];
+    uint32_t mhi;
 };
 
 struct FusedArgs {
@@ -66,18 +67,21 @@ __device__ __forceinline__ uint32_t spread(uint32_t o, const uint8_t* ins, int n
 // tile indices with zero bits at ins[]: the role slots (so the index is the reference's entry c)
 // and the tile bits of slots inactive at this step (so every orbit touched is active).  The
 // index o = tid + 512 k is spread as spread(tid) | spread(512 k): the first part is fixed per
-// thread and step, the second is the same for every thread of the block.
+// thread and step; the second is the same for every thread and walks the tile bits in mhi in
+// increasing order with ((v | ~mhi) + 1) & mhi.
 template <int KIND>
 __device__ __forceinline__ void run_step(float2* __restrict__ sh, int T, const FusedStep& st, float2 f0, float2 f1,
                                          int cs, int y) {
     const int nins = st.nins;
-    const int nrep = T >> nins;
+    const int nrep = T >> nins;  // a power of two
+    if ((int)threadIdx.x >= nrep) return;
     const uint32_t tbeta = st.tbeta;
     const uint32_t tp = spread(threadIdx.x, st.ins, nins);
     const int hs = (__popc(tp & tbeta) & 1) ^ cs;
-    for (int k = 0; (k * kThreads) < nrep; ++k) {
-        if ((int)threadIdx.x + k * kThreads >= nrep) break;
-        const uint32_t tu = spread((uint32_t)(k * kThreads), st.ins, nins);
+    const uint32_t mhi = st.mhi;
+    const int niter = nrep > kThreads ? nrep / kThreads : 1;
+    uint32_t tu = 0;  // spread(512 k), advanced by a masked increment over mhi
+    for (int k = 0; k < niter; ++k, tu = ((tu | ~mhi) + 1u) & mhi) {
         const uint32_t t = tp | tu;
         const int sc = hs ^ (__popc(tu & tbeta) & 1);
         const float2 x = sh[t];
@@ -257,7 +261,7 @@ extern "C" int dcs_fused_groups(void* table, const dcs_step* steps, int nsteps, 
             f.beta = d.beta;
             f.cskip = ts.cskip;
             f.tK = ts.tK; f.tKa = ts.tKa; f.tpiv = ts.tpiv; f.tbeta = ts.tbeta;
-            f.sK = ts.sK; f.sKa = ts.sKa; f.nins = ts.nins;
+            f.sK = ts.sK; f.sKa = ts.sKa; f.nins = ts.nins; f.mhi = ts.mhi;
             f.kind = d.kind;
             f.pidx = g.first + s;
             bool bad = f.nins > 16 || f.nins > g.tile_dim || (f.tK | f.tKa | f.tpiv | f.tbeta) >> g.tile_dim;
