@@ -17,7 +17,8 @@ using namespace dcs;
 namespace {
 
 constexpr int kMaxSteps = 24;
-constexpr int kThreads = 512;
+constexpr int kThreads = 256;
+constexpr int kThreadLog = 8;
 
 struct FusedStep {
     uint64_t beta, cskip;
@@ -66,7 +67,7 @@ __device__ __forceinline__ uint32_t spread(uint32_t o, const uint8_t* ins, int n
 // One vertex step over every active orbit representative of the tile.  Representatives are the
 // tile indices with zero bits at ins[]: the role slots (so the index is the reference's entry c)
 // and the tile bits of slots inactive at this step (so every orbit touched is active).  The
-// index o = tid + 512 k is spread as spread(tid) | spread(512 k): the first part is fixed per
+// index o = tid + 256 k is spread as spread(tid) | spread(256 k): the first part is fixed per
 // thread and step; the second is the same for every thread and walks the tile bits in mhi in
 // increasing order with ((v | ~mhi) + 1) & mhi.
 template <int KIND>
@@ -79,53 +80,57 @@ __device__ __forceinline__ void run_step(float2* __restrict__ sh, int T, const F
     const uint32_t tp = spread(threadIdx.x, st.ins, nins);
     const int hs = (__popc(tp & tbeta) & 1) ^ cs;
     const uint32_t mhi = st.mhi;
-    const int niter = nrep > kThreads ? nrep / kThreads : 1;
-    uint32_t tu = 0;  // spread(512 k), advanced by a masked increment over mhi
-    for (int k = 0; k < niter; ++k, tu = ((tu | ~mhi) + 1u) & mhi) {
+    const int niter = nrep > kThreads ? nrep >> kThreadLog : 1;
+    // partner-sign factors of this step, (-1)^sK and (-1)^sKa, and f0 +- f1 for the diagonal kinds
+    const float gK = st.sK ? -1.f : 1.f, gKa = st.sKa ? -1.f : 1.f;
+    const float2 fp = f2(f0.x + f1.x, f0.y + f1.y), fm = f2(f0.x - f1.x, f0.y - f1.y);
+    const float2 f1a = f2(gKa * f1.x, gKa * f1.y);  // f1 (-1)^sKa
+    const uint32_t tK = st.tK, tKa = st.tKa, tpiv = st.tpiv;
+    uint32_t tu = 0;  // spread(256 k), advanced by a masked increment over mhi
+#pragma unroll 4
+    for (int k = 0; k < niter; ++k) {
         const uint32_t t = tp | tu;
         const int sc = hs ^ (__popc(tu & tbeta) & 1);
+        tu = ((tu | ~mhi) + 1u) & mhi;
         const float2 x = sh[t];
         if constexpr (KIND == DCS_KIND_GROW) {
             sh[t] = fmul(f0, x);
-            sh[t ^ st.tpiv] = negif(fmul(f1, x), sc);
+            sh[t ^ tpiv] = negif(fmul(f1, x), sc);
         } else if constexpr (KIND == DCS_KIND_MIX) {
-            const uint32_t td = t ^ st.tKa;
+            // o0 = f0 x + s_c f1 (-1)^sKa b ;  o1 = f0 b + s_c f1 x
+            const uint32_t td = t ^ tKa;
             const float2 b = sh[td];
-            sh[t] = fmadd(f0, x, negif(fmul(f1, b), sc ^ st.sKa));
+            sh[t] = fmadd(f0, x, negif(fmul(f1a, b), sc));
             sh[td] = fmadd(f0, b, negif(fmul(f1, x), sc));
         } else if constexpr (KIND == DCS_KIND_DIAG) {
-            sh[t] = fmadd(f0, x, negif(fmul(f1, x), sc));
+            sh[t] = fmul(sc ? fm : fp, x);
         } else if constexpr (KIND == DCS_KIND_REPLACE) {
-            const uint32_t td = t ^ st.tK;
+            // o0 = f0 (x + b) ;  o1 = s_c f1 (x + (-1)^sK b)
+            const uint32_t td = t ^ tK;
             const float2 b = sh[td];
             sh[t] = fmul(f0, f2(x.x + b.x, x.y + b.y));
-            const float2 u = negif(x, sc), v = negif(b, sc ^ st.sK);
-            sh[td] = fmul(f1, f2(u.x + v.x, u.y + v.y));
+            sh[td] = negif(fmul(f1, f2(fmaf(gK, b.x, x.x), fmaf(gK, b.y, x.y))), sc);
         } else if constexpr (KIND == DCS_KIND_FIXED) {
             sh[t] = y ? negif(fmul(f1, x), sc) : fmul(f0, x);
         } else if constexpr (KIND == DCS_KIND_FIXED_SHRINK) {
-            const uint32_t td = t ^ st.tK;
+            const uint32_t td = t ^ tK;
             const float2 b = sh[td];
-            if (y) {
-                const float2 u = negif(x, sc), v = negif(b, sc ^ st.sK);
-                sh[t] = fmul(f1, f2(u.x + v.x, u.y + v.y));
-            } else {
-                sh[t] = fmul(f0, f2(x.x + b.x, x.y + b.y));
-            }
+            sh[t] = y ? negif(fmul(f1, f2(fmaf(gK, b.x, x.x), fmaf(gK, b.y, x.y))), sc)
+                      : fmul(f0, f2(x.x + b.x, x.y + b.y));
         } else if constexpr (KIND == DCS_KIND_SHRINK4) {
-            const uint32_t t1 = t ^ st.tK, td = t ^ st.tKa, td1 = td ^ st.tK;
+            // o0 = f0 (x + b) + s_d f1 (g + (-1)^sK h) ;  o1 = f0 (g + h) + s_c f1 (x + (-1)^sK b)
+            const uint32_t t1 = t ^ tK, td = t ^ tKa, td1 = td ^ tK;
             const float2 b = sh[t1], g = sh[td], h = sh[td1];
             const int sd = sc ^ st.sKa;
-            const float2 gg = negif(g, sd), hh = negif(h, sd ^ st.sK);
-            const float2 xx = negif(x, sc), bb = negif(b, sc ^ st.sK);
-            sh[t] = fmadd(f1, f2(gg.x + hh.x, gg.y + hh.y), fmul(f0, f2(x.x + b.x, x.y + b.y)));
-            sh[td] = fmadd(f1, f2(xx.x + bb.x, xx.y + bb.y), fmul(f0, f2(g.x + h.x, g.y + h.y)));
-        } else {  // DCS_KIND_SHRINK2
-            const uint32_t td = t ^ st.tK;
+            sh[t] = fmadd(f0, f2(x.x + b.x, x.y + b.y),
+                          negif(fmul(f1, f2(fmaf(gK, h.x, g.x), fmaf(gK, h.y, g.y))), sd));
+            sh[td] = fmadd(f0, f2(g.x + h.x, g.y + h.y),
+                           negif(fmul(f1, f2(fmaf(gK, b.x, x.x), fmaf(gK, b.y, x.y))), sc));
+        } else {  // DCS_KIND_SHRINK2: f0 (x + b) + s_c f1 (x + (-1)^sK b)
+            const uint32_t td = t ^ tK;
             const float2 b = sh[td];
-            const float2 u = negif(x, sc), v = negif(b, sc ^ st.sK);
-            // (f0 + s_c f1) x + (f0 + s_d f1) b = f0 (x + b) + f1 (s_c x + s_d b)
-            sh[t] = fmadd(f1, f2(u.x + v.x, u.y + v.y), fmul(f0, f2(x.x + b.x, x.y + b.y)));
+            sh[t] = fmadd(f0, f2(x.x + b.x, x.y + b.y),
+                          negif(fmul(f1, f2(fmaf(gK, b.x, x.x), fmaf(gK, b.y, x.y))), sc));
         }
     }
 }
@@ -284,7 +289,7 @@ extern "C" int dcs_fused_groups(void* table, const dcs_step* steps, int nsteps, 
         const uint64_t ntiles = 1ull << g.coset_m;
         int per_sm = (int)((220 * 1024) / (smem + 2048));
         if (per_sm < 1) per_sm = 1;
-        if (per_sm > 4) per_sm = 4;  // 512 threads per CTA: at most 4 CTAs per SM
+        if (per_sm > 8) per_sm = 8;
         uint64_t grid = (uint64_t)sms * per_sm;
         if (grid > ntiles) grid = ntiles;
         k_fused<<<(unsigned)grid, kThreads, smem, st>>>((float2*)table, A, params, (unsigned long long*)maxbits, scale);

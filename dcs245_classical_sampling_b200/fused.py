@@ -230,7 +230,7 @@ def build_fused_plan(plan, max_dim=13, low=4, max_steps=MAX_GROUP_STEPS, max_ext
                 ts["ins"][i] = b
             ts["cskip"] = cskip
             free = [b for b in range(dim) if b not in ins]
-            ts["mhi"] = sum(1 << b for b in free[9:])  # 512 threads: index bits >= 9
+            ts["mhi"] = sum(1 << b for b in free[8:])  # 256 threads: index bits >= 8
             ts["rb1"] = max(st.pivot_a if kind == 1 else st.pivot, 0)  # role slot(s), for checking
             ts["rb2"] = max(st.pivot_a, 0) if kind == 6 else 0
         fp.universe.append(bin(U).count("1"))

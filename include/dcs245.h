@@ -133,7 +133,7 @@ typedef struct dcs_tile_step {
     uint8_t rb1, rb2;       /* physical role slots (for checking) */
     uint8_t pad[3];
     uint8_t ins[16];        /* inserted tile bits, ascending */
-    uint32_t mhi;           /* tile bits receiving representative-index bits 9 and up */
+    uint32_t mhi;           /* tile bits receiving representative-index bits 8 and up (256 threads) */
     uint32_t pad2;
 } dcs_tile_step;
 
