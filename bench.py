@@ -349,7 +349,7 @@ def gpu_arm(args):
                              "peak_source": f"{how} (MEASURED_PEAKS.json hbm_gbs)" if how == "measured" else
                              "fallback 6650 GB/s", "launches": dom["launches"],
                              "alg_bytes_per_launch": dom["alg_bytes_per_launch"],
-                             "avg_launch_ms": dom["avg_launch_s"] * 1e3},
+                             "avg_launch_ms": dom["avg_launch_s"] * 1e3, "launch_ms": dom["launch_ms"]},
                 "plain": plain, "speedup_vs_plain": (value / plain["value"]) if plain else None,
                 "draws": {"indices": [int(d["index"]) for d in draws[args.warmup:total]],
                           "ties": int(sum(int(d["tie"]) for d in draws[args.warmup:total]))},
@@ -416,7 +416,8 @@ def kernel_roofline(eng, prep, out, stream):
     tot_t = sum(a.elapsed_time(b) for a, b, _ in evs) / 1000.0
     tot_b = sum(x for _, _, x in evs)
     n = len(evs)
-    return {"kernel": kernel, "launches": n, "avg_launch_s": tot_t / n, "alg_bytes_per_launch": tot_b / n}
+    return {"kernel": kernel, "launches": n, "avg_launch_s": tot_t / n, "alg_bytes_per_launch": tot_b / n,
+            "launch_ms": [round(a.elapsed_time(b), 3) for a, b, _ in evs]}
 
 
 def main():

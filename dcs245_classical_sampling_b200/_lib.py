@@ -28,7 +28,7 @@ PARAM_DTYPE = np.dtype([("f0r", "<f8"), ("f0i", "<f8"), ("f1r", "<f8"), ("f1i", 
 SCALE_DTYPE = np.dtype([("logscale", "<f8"), ("exponent_sum", "<i8"), ("flags", "<u4"), ("pad", "<u4")])
 GROUP_DTYPE = np.dtype([
     ("first", "<i4"), ("count", "<i4"), ("tile_dim", "<i4"), ("low_bits", "<i4"),
-    ("coset_m", "<i4"), ("ncoset_runs", "<i4"), ("step_tile_off", "<i4"), ("pad", "<i4"),
+    ("coset_m", "<i4"), ("ncoset_runs", "<i4"), ("step_tile_off", "<i4"), ("variant", "<i4"),
     ("out_mask", "<u8"), ("basis", "<u8", (16,)), ("coset_runs", "<u4", (MAX_RUNS,)),
 ])
 TILE_STEP_DTYPE = np.dtype([("cskip", "<u8"), ("tK", "<u4"), ("tKa", "<u4"), ("tpiv", "<u4"), ("tbeta", "<u4"),

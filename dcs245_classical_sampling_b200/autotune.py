@@ -16,8 +16,8 @@ import numpy as np
 from . import _lib
 
 CACHE = Path(__file__).resolve().parent / "autotune_cache.json"
-CANDIDATES = [(13, 4, 24), (12, 4, 24), (13, 3, 24), (14, 4, 24), (13, 5, 24), (12, 3, 24), (11, 4, 24),
-              (13, 4, 12)]
+CANDIDATES = [(13, 4, 24, 0), (13, 4, 24, 1), (12, 4, 24, 0), (12, 4, 24, 1), (13, 3, 24, 0), (13, 5, 24, 0),
+              (13, 4, 12, 0), (14, 4, 24, 1)]
 
 
 def fingerprint(plan):
@@ -51,9 +51,9 @@ def tune(engine, params_dev, candidates=CANDIDATES, repeats=1, save=True):
     report = []
     best = None
     for cand in candidates:
-        max_dim, low, max_steps = cand
+        max_dim, low, max_steps, variant = cand
         try:
-            fp = build_fused_plan(engine.plan, max_dim=max_dim, low=low, max_steps=max_steps)
+            fp = build_fused_plan(engine.plan, max_dim=max_dim, low=low, max_steps=max_steps, variant=variant)
         except ValueError:
             continue
         need = len(fp.groups) + 1
@@ -77,8 +77,8 @@ def tune(engine, params_dev, candidates=CANDIDATES, repeats=1, save=True):
             torch.cuda.synchronize(engine.device)
             times.append(a.elapsed_time(b) / 1000.0)
         t = min(times[1:]) if len(times) > 1 else times[0]
-        report.append({"max_dim": max_dim, "low": low, "max_steps": max_steps, "groups": len(fp.groups),
-                       "seconds": t})
+        report.append({"max_dim": max_dim, "low": low, "max_steps": max_steps, "variant": variant,
+                       "groups": len(fp.groups), "seconds": t})
         if best is None or t < best[0]:
             best = (t, cand, fp)
     engine.fplan = best[2]
@@ -87,10 +87,11 @@ def tune(engine, params_dev, candidates=CANDIDATES, repeats=1, save=True):
     if save:
         data = _load()
         data[f"{fingerprint(engine.plan)}|{torch.cuda.get_device_name(engine.device)}"] = {
-            "max_dim": best[1][0], "low": best[1][1], "max_steps": best[1][2], "seconds": best[0]}
+            "max_dim": best[1][0], "low": best[1][1], "max_steps": best[1][2], "variant": best[1][3],
+            "seconds": best[0]}
         try:
             CACHE.write_text(json.dumps(data, indent=1) + "\n")
         except OSError:
             pass
-    return {"best": {"max_dim": best[1][0], "low": best[1][1], "max_steps": best[1][2], "seconds": best[0]},
-            "candidates": report}
+    return {"best": {"max_dim": best[1][0], "low": best[1][1], "max_steps": best[1][2], "variant": best[1][3],
+                     "seconds": best[0]}, "candidates": report}

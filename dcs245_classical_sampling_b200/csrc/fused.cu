@@ -86,56 +86,81 @@ __device__ __forceinline__ void run_step(float2* __restrict__ sh, int T, const F
     const float2 fp = f2(f0.x + f1.x, f0.y + f1.y), fm = f2(f0.x - f1.x, f0.y - f1.y);
     const float2 f1a = f2(gKa * f1.x, gKa * f1.y);  // f1 (-1)^sKa
     const uint32_t tK = st.tK, tKa = st.tKa, tpiv = st.tpiv;
+    // Orbits of one step are disjoint, so UNR orbits are loaded into registers before any of
+    // them is stored: the shared-memory loads overlap instead of waiting behind the stores.
+    constexpr int UNR = (KIND == DCS_KIND_SHRINK4) ? 1 : (KIND == DCS_KIND_GROW || KIND == DCS_KIND_DIAG ||
+                                                         KIND == DCS_KIND_FIXED) ? 4 : 2;
+    constexpr int NIN = (KIND == DCS_KIND_SHRINK4) ? 4 : (KIND == DCS_KIND_GROW || KIND == DCS_KIND_DIAG ||
+                                                         KIND == DCS_KIND_FIXED) ? 1 : 2;
     uint32_t tu = 0;  // spread(256 k), advanced by a masked increment over mhi
-#pragma unroll 4
-    for (int k = 0; k < niter; ++k) {
-        const uint32_t t = tp | tu;
-        const int sc = hs ^ (__popc(tu & tbeta) & 1);
-        tu = ((tu | ~mhi) + 1u) & mhi;
-        const float2 x = sh[t];
-        if constexpr (KIND == DCS_KIND_GROW) {
-            sh[t] = fmul(f0, x);
-            sh[t ^ tpiv] = negif(fmul(f1, x), sc);
-        } else if constexpr (KIND == DCS_KIND_MIX) {
-            // o0 = f0 x + s_c f1 (-1)^sKa b ;  o1 = f0 b + s_c f1 x
-            const uint32_t td = t ^ tKa;
-            const float2 b = sh[td];
-            sh[t] = fmadd(f0, x, negif(fmul(f1a, b), sc));
-            sh[td] = fmadd(f0, b, negif(fmul(f1, x), sc));
-        } else if constexpr (KIND == DCS_KIND_DIAG) {
-            sh[t] = fmul(sc ? fm : fp, x);
-        } else if constexpr (KIND == DCS_KIND_REPLACE) {
-            // o0 = f0 (x + b) ;  o1 = s_c f1 (x + (-1)^sK b)
-            const uint32_t td = t ^ tK;
-            const float2 b = sh[td];
-            sh[t] = fmul(f0, f2(x.x + b.x, x.y + b.y));
-            sh[td] = negif(fmul(f1, f2(fmaf(gK, b.x, x.x), fmaf(gK, b.y, x.y))), sc);
-        } else if constexpr (KIND == DCS_KIND_FIXED) {
-            sh[t] = y ? negif(fmul(f1, x), sc) : fmul(f0, x);
-        } else if constexpr (KIND == DCS_KIND_FIXED_SHRINK) {
-            const uint32_t td = t ^ tK;
-            const float2 b = sh[td];
-            sh[t] = y ? negif(fmul(f1, f2(fmaf(gK, b.x, x.x), fmaf(gK, b.y, x.y))), sc)
-                      : fmul(f0, f2(x.x + b.x, x.y + b.y));
-        } else if constexpr (KIND == DCS_KIND_SHRINK4) {
-            // o0 = f0 (x + b) + s_d f1 (g + (-1)^sK h) ;  o1 = f0 (g + h) + s_c f1 (x + (-1)^sK b)
-            const uint32_t t1 = t ^ tK, td = t ^ tKa, td1 = td ^ tK;
-            const float2 b = sh[t1], g = sh[td], h = sh[td1];
-            const int sd = sc ^ st.sKa;
-            sh[t] = fmadd(f0, f2(x.x + b.x, x.y + b.y),
-                          negif(fmul(f1, f2(fmaf(gK, h.x, g.x), fmaf(gK, h.y, g.y))), sd));
-            sh[td] = fmadd(f0, f2(g.x + h.x, g.y + h.y),
-                           negif(fmul(f1, f2(fmaf(gK, b.x, x.x), fmaf(gK, b.y, x.y))), sc));
-        } else {  // DCS_KIND_SHRINK2: f0 (x + b) + s_c f1 (x + (-1)^sK b)
-            const uint32_t td = t ^ tK;
-            const float2 b = sh[td];
-            sh[t] = fmadd(f0, f2(x.x + b.x, x.y + b.y),
-                          negif(fmul(f1, f2(fmaf(gK, b.x, x.x), fmaf(gK, b.y, x.y))), sc));
+    for (int k0 = 0; k0 < niter; k0 += UNR) {
+        uint32_t t[UNR];
+        int sc[UNR];
+        float2 v[UNR][NIN];
+#pragma unroll
+        for (int u = 0; u < UNR; ++u) {
+            t[u] = tp | tu;
+            sc[u] = hs ^ (__popc(tu & tbeta) & 1);
+            tu = ((tu | ~mhi) + 1u) & mhi;
+        }
+#pragma unroll
+        for (int u = 0; u < UNR; ++u) {
+            if (k0 + u < niter) {
+                v[u][0] = sh[t[u]];
+                if constexpr (KIND == DCS_KIND_MIX) v[u][1] = sh[t[u] ^ tKa];
+                if constexpr (NIN >= 2 && KIND != DCS_KIND_MIX) v[u][1] = sh[t[u] ^ tK];
+                if constexpr (NIN == 4) {
+                    v[u][2] = sh[t[u] ^ tKa];
+                    v[u][3] = sh[t[u] ^ tKa ^ tK];
+                }
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < UNR; ++u) {
+            if (k0 + u >= niter) break;
+            const uint32_t tt = t[u];
+            const int s_ = sc[u];
+            const float2 x = v[u][0];
+            if constexpr (KIND == DCS_KIND_GROW) {
+                sh[tt] = fmul(f0, x);
+                sh[tt ^ tpiv] = negif(fmul(f1, x), s_);
+            } else if constexpr (KIND == DCS_KIND_MIX) {
+                // o0 = f0 x + s_c f1 (-1)^sKa b ;  o1 = f0 b + s_c f1 x
+                const float2 b = v[u][1];
+                sh[tt] = fmadd(f0, x, negif(fmul(f1a, b), s_));
+                sh[tt ^ tKa] = fmadd(f0, b, negif(fmul(f1, x), s_));
+            } else if constexpr (KIND == DCS_KIND_DIAG) {
+                sh[tt] = fmul(s_ ? fm : fp, x);
+            } else if constexpr (KIND == DCS_KIND_REPLACE) {
+                // o0 = f0 (x + b) ;  o1 = s_c f1 (x + (-1)^sK b)
+                const float2 b = v[u][1];
+                sh[tt] = fmul(f0, f2(x.x + b.x, x.y + b.y));
+                sh[tt ^ tK] = negif(fmul(f1, f2(fmaf(gK, b.x, x.x), fmaf(gK, b.y, x.y))), s_);
+            } else if constexpr (KIND == DCS_KIND_FIXED) {
+                sh[tt] = y ? negif(fmul(f1, x), s_) : fmul(f0, x);
+            } else if constexpr (KIND == DCS_KIND_FIXED_SHRINK) {
+                const float2 b = v[u][1];
+                sh[tt] = y ? negif(fmul(f1, f2(fmaf(gK, b.x, x.x), fmaf(gK, b.y, x.y))), s_)
+                           : fmul(f0, f2(x.x + b.x, x.y + b.y));
+            } else if constexpr (KIND == DCS_KIND_SHRINK4) {
+                // o0 = f0 (x + b) + s_d f1 (g + (-1)^sK h) ;  o1 = f0 (g + h) + s_c f1 (x + (-1)^sK b)
+                const float2 b = v[u][1], g = v[u][2], h = v[u][3];
+                const int sd = s_ ^ st.sKa;
+                sh[tt] = fmadd(f0, f2(x.x + b.x, x.y + b.y),
+                               negif(fmul(f1, f2(fmaf(gK, h.x, g.x), fmaf(gK, h.y, g.y))), sd));
+                sh[tt ^ tKa] = fmadd(f0, f2(g.x + h.x, g.y + h.y),
+                                     negif(fmul(f1, f2(fmaf(gK, b.x, x.x), fmaf(gK, b.y, x.y))), s_));
+            } else {  // DCS_KIND_SHRINK2: f0 (x + b) + s_c f1 (x + (-1)^sK b)
+                const float2 b = v[u][1];
+                sh[tt] = fmadd(f0, f2(x.x + b.x, x.y + b.y),
+                               negif(fmul(f1, f2(fmaf(gK, b.x, x.x), fmaf(gK, b.y, x.y))), s_));
+            }
         }
     }
 }
 
-__global__ void __launch_bounds__(kThreads)
+template <int MINB>
+__global__ void __launch_bounds__(kThreads, MINB)
 k_fused(float2* __restrict__ E, const __grid_constant__ FusedArgs A, const dcs_param* __restrict__ params,
         unsigned long long* __restrict__ maxbits, dcs_scale* __restrict__ scale) {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -176,15 +201,22 @@ k_fused(float2* __restrict__ E, const __grid_constant__ FusedArgs A, const dcs_p
     for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const uint64_t base = deposit(tile, A.coset_runs, A.ncoset_runs);
         // load (only entries active before the group; the rest are written before being read)
-        for (int t = threadIdx.x; t < T; t += kThreads) {
-            const uint64_t a = base ^ hi_tab[t >> low] ^ ((uint64_t)t & lowmask);
-            float2 v = f2(0.f, 0.f);
-            if (!(a & in_inactive)) {
-                v = E[a];
-                v.x *= sc;
-                v.y *= sc;
+        for (int t0 = threadIdx.x; t0 < T; t0 += 4 * kThreads) {
+            float2 v[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int t = t0 + u * kThreads;
+                v[u] = f2(0.f, 0.f);
+                if (t < T) {
+                    const uint64_t a = base ^ hi_tab[t >> low] ^ ((uint64_t)t & lowmask);
+                    if (!(a & in_inactive)) v[u] = E[a];
+                }
             }
-            sh[t] = v;
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int t = t0 + u * kThreads;
+                if (t < T) sh[t] = f2(v[u].x * sc, v[u].y * sc);
+            }
         }
         __syncthreads();
         for (int s = 0; s < A.count; ++s) {
@@ -282,17 +314,26 @@ extern "C" int dcs_fused_groups(void* table, const dcs_step* steps, int nsteps, 
         const size_t smem = sizeof(float2) * ((size_t)1 << g.tile_dim) +
                             sizeof(uint64_t) * ((size_t)1 << (g.tile_dim - g.low_bits));
         if (!max_smem_set[dev]) {
-            cudaError_t e = cudaFuncSetAttribute(k_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
+            cudaError_t e = cudaFuncSetAttribute(k_fused<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
+            if (e == cudaSuccess)
+                e = cudaFuncSetAttribute(k_fused<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
             if (e != cudaSuccess) return dcs_host::check_cuda(e, "k_fused smem attribute");
             max_smem_set[dev] = 1;
         }
         const uint64_t ntiles = 1ull << g.coset_m;
         int per_sm = (int)((220 * 1024) / (smem + 2048));
         if (per_sm < 1) per_sm = 1;
-        if (per_sm > 8) per_sm = 8;
+        const int reg_cap = g.variant == 1 ? 2 : 3;
+        if (per_sm > reg_cap) per_sm = reg_cap;
         uint64_t grid = (uint64_t)sms * per_sm;
         if (grid > ntiles) grid = ntiles;
-        k_fused<<<(unsigned)grid, kThreads, smem, st>>>((float2*)table, A, params, (unsigned long long*)maxbits, scale);
+        // variant 0: at least 3 CTAs per SM (register cap 80); variant 1: 2 CTAs per SM (more registers)
+        if (g.variant == 1)
+            k_fused<2><<<(unsigned)grid, kThreads, smem, st>>>((float2*)table, A, params, (unsigned long long*)maxbits,
+                                                              scale);
+        else
+            k_fused<3><<<(unsigned)grid, kThreads, smem, st>>>((float2*)table, A, params, (unsigned long long*)maxbits,
+                                                              scale);
         DCS_CHECK_LAUNCH("k_fused launch");
     }
     return DCS_OK;

@@ -216,7 +216,7 @@ class InplaceConditionalBlockGPU:
             from .fused import build_fused_plan
             cfg = cached(plan, torch.cuda.get_device_name(self.device)) or {}
             self.fused_config = {"max_dim": cfg.get("max_dim", 13), "low": cfg.get("low", 4),
-                                 "max_steps": cfg.get("max_steps", 24)}
+                                 "max_steps": cfg.get("max_steps", 24), "variant": cfg.get("variant", 0)}
             self.fplan = build_fused_plan(plan, **self.fused_config)
             self.items = 1
         self.table = torch.empty(self.items * table_entries, dtype=tdtype, device=self.device)
@@ -258,7 +258,7 @@ class InplaceConditionalBlockGPU:
         _, items = self.params.items(x)
         prm = torch.from_numpy(items[0][1].view(np.int64).copy()).to(self.device)
         rep = at.tune(self, prm, **({"candidates": candidates} if candidates else {}))
-        self.fused_config = {k: rep["best"][k] for k in ("max_dim", "low", "max_steps")}
+        self.fused_config = {k: rep["best"][k] for k in ("max_dim", "low", "max_steps", "variant")}
         self.scale = torch.zeros(self.items * _lib.SCALE_DTYPE.itemsize // 8, dtype=torch.int64,
                                  device=self.device)
         return rep

@@ -120,7 +120,7 @@ def group_steps(steps, max_dim=13, low=4, max_steps=MAX_GROUP_STEPS, max_extra=1
     return spans
 
 
-def build_fused_plan(plan, max_dim=13, low=4, max_steps=MAX_GROUP_STEPS, max_extra=1, spans=None):
+def build_fused_plan(plan, max_dim=13, low=4, max_steps=MAX_GROUP_STEPS, max_extra=1, spans=None, variant=0):
     steps = plan.steps
     if spans is None:
         spans = group_steps(steps, max_dim, low, max_steps, max_extra)
@@ -179,6 +179,7 @@ def build_fused_plan(plan, max_dim=13, low=4, max_steps=MAX_GROUP_STEPS, max_ext
         g["first"], g["count"], g["tile_dim"], g["low_bits"] = first, count, dim, l
         g["coset_m"], g["ncoset_runs"], g["step_tile_off"] = bin(cmask).count("1"), len(runs), first
         g["out_mask"] = slot_mask(steps[first + count - 1].active_out)
+        g["variant"] = variant
         for i, b in enumerate(basis):
             g["basis"][i] = b
         for r, (src, dst, ln) in enumerate(runs):

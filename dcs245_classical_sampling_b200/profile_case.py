@@ -32,6 +32,7 @@ def main():
     ap.add_argument("--iters", type=int, default=3)
     ap.add_argument("--max-dim", type=int, default=13)
     ap.add_argument("--low", type=int, default=4)
+    ap.add_argument("--variant", type=int, default=0)
     a = ap.parse_args()
     lib = _lib.load()
     w = build_workload(a.workload)
@@ -55,7 +56,7 @@ def main():
     stream = torch.cuda.current_stream(dev)
     sub = P.BlockPlan(**{**bp.__dict__, "steps": steps})
     if a.mode == "fused":
-        fp = build_fused_plan(sub, max_dim=a.max_dim, low=a.low)
+        fp = build_fused_plan(sub, max_dim=a.max_dim, low=a.low, variant=a.variant)
         nmax = len(fp.groups)
     else:
         dsteps = device_steps(steps)

@@ -111,7 +111,7 @@ typedef struct dcs_group {
     int32_t tile_dim, low_bits;
     int32_t coset_m, ncoset_runs;
     int32_t step_tile_off; /* index into the per-step tile-mask table */
-    int32_t pad;
+    int32_t variant;       /* kernel variant: 0 = 3 CTAs per SM, 1 = 2 CTAs per SM */
     uint64_t out_mask;     /* active_out after the last step (for the max) */
     uint64_t basis[16];    /* tile basis (slot masks) */
     uint32_t coset_runs[DCS_MAX_RUNS];
