@@ -5,9 +5,10 @@
 // active before the group (128-byte rows of 2^low contiguous entries), applies every step of
 // the group in shared memory with the same orbit formulas as the per-step kernel
 // (reference: source/kernel_opt/inplace_gpu.py:29-58), and stores the entries that are
-// active after the group.  The power-of-two renormalisation is applied once per pass (on
-// load) from the previous pass's max; the pass's own max is reduced per CTA and published
-// with one atomicMax.
+// active after the group.  The power-of-two renormalisation is applied once per pass (at the
+// store; the steps are linear) from the previous pass's max; the pass's own max is reduced per
+// CTA and published with one atomicMax.  Tile loads are cp.async copies, zero-filled for
+// entries that are inactive before the group.
 #include <string.h>
 
 #include "common.cuh"
@@ -64,30 +65,29 @@ __device__ __forceinline__ uint32_t spread(uint32_t o, const uint8_t* ins, int n
     return o;
 }
 
-// Per-step constants, computed once per launch into shared memory.
-struct StepConst {
-    float2 f0, f1, f1a, fp, fm;  // f1a = (-1)^sKa f1, fp/fm = f0 +- f1
-    float gK;                    // (-1)^sK
-    int y, ov;
-};
-
 // One vertex step over every active orbit representative of the tile.  Representatives are the
 // tile indices with zero bits at ins[]: the role slots (so the index is the reference's entry c)
 // and the tile bits of slots inactive at this step (so every orbit touched is active).  The
-// index o = tid + 256 k is spread as spread(tid) | spread(256 k): the first part (with its sign
-// parity in bit 31) comes from a per-launch table; the second is the same for every thread and
-// walks the tile bits in mhi in increasing order with ((v | ~mhi) + 1) & mhi.
+// index o = tid + 256 k is spread as spread(tid) | spread(256 k): the first part is fixed per
+// thread and step; the second is the same for every thread and walks the tile bits in mhi in
+// increasing order with ((v | ~mhi) + 1) & mhi.
 template <int KIND>
-__device__ __forceinline__ void run_step(float2* __restrict__ sh, int nrep, uint32_t tpw, const FusedStep& st,
-                                         const StepConst& c, int cs) {
+__device__ __forceinline__ void run_step(float2* __restrict__ sh, int T, const FusedStep& st, float2 f0, float2 f1,
+                                         int cs, int y) {
+    const int nins = st.nins;
+    const int nrep = T >> nins;  // a power of two
     if ((int)threadIdx.x >= nrep) return;
-    const uint32_t tp = tpw & 0x7fffffffu;
-    const int hs = (int)(tpw >> 31) ^ cs;
-    const uint32_t tbeta = st.tbeta, mhi = st.mhi;
+    const uint32_t tbeta = st.tbeta;
+    const uint32_t tp = spread(threadIdx.x, st.ins, nins);
+    const int hs = (__popc(tp & tbeta) & 1) ^ cs;
+    const uint32_t mhi = st.mhi;
     const int niter = nrep > kThreads ? nrep >> kThreadLog : 1;
-    const float2 f0 = c.f0, f1 = c.f1;
+    // partner-sign factors of this step, (-1)^sK and (-1)^sKa, and f0 +- f1 for the diagonal kinds
+    const float gK = st.sK ? -1.f : 1.f, gKa = st.sKa ? -1.f : 1.f;
+    const float2 fp = f2(f0.x + f1.x, f0.y + f1.y), fm = f2(f0.x - f1.x, f0.y - f1.y);
+    const float2 f1a = f2(gKa * f1.x, gKa * f1.y);  // f1 (-1)^sKa
     const uint32_t tK = st.tK, tKa = st.tKa, tpiv = st.tpiv;
-    uint32_t tu = 0;
+    uint32_t tu = 0;  // spread(256 k), advanced by a masked increment over mhi
 #pragma unroll 4
     for (int k = 0; k < niter; ++k) {
         const uint32_t t = tp | tu;
@@ -101,37 +101,37 @@ __device__ __forceinline__ void run_step(float2* __restrict__ sh, int nrep, uint
             // o0 = f0 x + s_c f1 (-1)^sKa b ;  o1 = f0 b + s_c f1 x
             const uint32_t td = t ^ tKa;
             const float2 b = sh[td];
-            sh[t] = fmadd(f0, x, negif(fmul(c.f1a, b), sc));
+            sh[t] = fmadd(f0, x, negif(fmul(f1a, b), sc));
             sh[td] = fmadd(f0, b, negif(fmul(f1, x), sc));
         } else if constexpr (KIND == DCS_KIND_DIAG) {
-            sh[t] = fmul(sc ? c.fm : c.fp, x);
+            sh[t] = fmul(sc ? fm : fp, x);
         } else if constexpr (KIND == DCS_KIND_REPLACE) {
             // o0 = f0 (x + b) ;  o1 = s_c f1 (x + (-1)^sK b)
             const uint32_t td = t ^ tK;
             const float2 b = sh[td];
             sh[t] = fmul(f0, f2(x.x + b.x, x.y + b.y));
-            sh[td] = negif(fmul(f1, f2(fmaf(c.gK, b.x, x.x), fmaf(c.gK, b.y, x.y))), sc);
+            sh[td] = negif(fmul(f1, f2(fmaf(gK, b.x, x.x), fmaf(gK, b.y, x.y))), sc);
         } else if constexpr (KIND == DCS_KIND_FIXED) {
-            sh[t] = c.y ? negif(fmul(f1, x), sc) : fmul(f0, x);
+            sh[t] = y ? negif(fmul(f1, x), sc) : fmul(f0, x);
         } else if constexpr (KIND == DCS_KIND_FIXED_SHRINK) {
             const uint32_t td = t ^ tK;
             const float2 b = sh[td];
-            sh[t] = c.y ? negif(fmul(f1, f2(fmaf(c.gK, b.x, x.x), fmaf(c.gK, b.y, x.y))), sc)
-                        : fmul(f0, f2(x.x + b.x, x.y + b.y));
+            sh[t] = y ? negif(fmul(f1, f2(fmaf(gK, b.x, x.x), fmaf(gK, b.y, x.y))), sc)
+                      : fmul(f0, f2(x.x + b.x, x.y + b.y));
         } else if constexpr (KIND == DCS_KIND_SHRINK4) {
             // o0 = f0 (x + b) + s_d f1 (g + (-1)^sK h) ;  o1 = f0 (g + h) + s_c f1 (x + (-1)^sK b)
             const uint32_t t1 = t ^ tK, td = t ^ tKa, td1 = td ^ tK;
             const float2 b = sh[t1], g = sh[td], h = sh[td1];
             const int sd = sc ^ st.sKa;
             sh[t] = fmadd(f0, f2(x.x + b.x, x.y + b.y),
-                          negif(fmul(f1, f2(fmaf(c.gK, h.x, g.x), fmaf(c.gK, h.y, g.y))), sd));
+                          negif(fmul(f1, f2(fmaf(gK, h.x, g.x), fmaf(gK, h.y, g.y))), sd));
             sh[td] = fmadd(f0, f2(g.x + h.x, g.y + h.y),
-                           negif(fmul(f1, f2(fmaf(c.gK, b.x, x.x), fmaf(c.gK, b.y, x.y))), sc));
+                           negif(fmul(f1, f2(fmaf(gK, b.x, x.x), fmaf(gK, b.y, x.y))), sc));
         } else {  // DCS_KIND_SHRINK2: f0 (x + b) + s_c f1 (x + (-1)^sK b)
             const uint32_t td = t ^ tK;
             const float2 b = sh[td];
             sh[t] = fmadd(f0, f2(x.x + b.x, x.y + b.y),
-                          negif(fmul(f1, f2(fmaf(c.gK, b.x, x.x), fmaf(c.gK, b.y, x.y))), sc));
+                          negif(fmul(f1, f2(fmaf(gK, b.x, x.x), fmaf(gK, b.y, x.y))), sc));
         }
     }
 }
@@ -144,11 +144,10 @@ k_fused(float2* __restrict__ E, const __grid_constant__ FusedArgs A, const dcs_p
     const int T = 1 << A.tile_dim;
     const int low = A.low_bits;
     const int nhi = 1 << (A.tile_dim - low);
-    // shared memory: tile | hi_tab | tp_tab[count][kThreads] | step constants
     float2* sh = reinterpret_cast<float2*>(smem);
     uint64_t* hi_tab = reinterpret_cast<uint64_t*>(smem + sizeof(float2) * (size_t)T);
-    uint32_t* tp_tab = reinterpret_cast<uint32_t*>(hi_tab + nhi);
-    StepConst* sc_tab = reinterpret_cast<StepConst*>(tp_tab + A.count * kThreads);
+    __shared__ float4 fw[kMaxSteps];
+    __shared__ int ovy[kMaxSteps];
 
     const double m2prev = (double)__uint_as_float((uint32_t)maxbits[A.group]);
     const int e = scale_exponent(m2prev);
@@ -160,24 +159,9 @@ k_fused(float2* __restrict__ E, const __grid_constant__ FusedArgs A, const dcs_p
         else if (m2prev == 0.0) scale->flags |= 2u;
     }
     if (threadIdx.x < A.count) {
-        const FusedStep& st = A.st[threadIdx.x];
-        const dcs_param p = params[st.pidx];
-        StepConst c;
-        c.f0 = f2((float)p.f0r, (float)p.f0i);
-        c.f1 = f2((float)p.f1r, (float)p.f1i);
-        const float gKa = st.sKa ? -1.f : 1.f;
-        c.f1a = f2(gKa * c.f1.x, gKa * c.f1.y);
-        c.fp = f2(c.f0.x + c.f1.x, c.f0.y + c.f1.y);
-        c.fm = f2(c.f0.x - c.f1.x, c.f0.y - c.f1.y);
-        c.gK = st.sK ? -1.f : 1.f;
-        c.y = p.y & 1;
-        c.ov = p.ov & 1;
-        sc_tab[threadIdx.x] = c;
-    }
-    for (int s = 0; s < A.count; ++s) {
-        const FusedStep& st = A.st[s];
-        const uint32_t tp = spread(threadIdx.x, st.ins, st.nins);
-        tp_tab[s * kThreads + threadIdx.x] = tp | ((uint32_t)(__popc(tp & st.tbeta) & 1) << 31);
+        const dcs_param p = params[A.st[threadIdx.x].pidx];
+        fw[threadIdx.x] = make_float4((float)p.f0r, (float)p.f0i, (float)p.f1r, (float)p.f1i);
+        ovy[threadIdx.x] = (p.ov & 1) | ((p.y & 1) << 1);
     }
     for (int h = threadIdx.x; h < nhi; h += blockDim.x) {
         uint64_t a = 0;
@@ -193,36 +177,34 @@ k_fused(float2* __restrict__ E, const __grid_constant__ FusedArgs A, const dcs_p
     float lm = 0.f;
     for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const uint64_t base = deposit(tile, A.coset_runs, A.ncoset_runs);
-        // load (only entries active before the group; the rest are written before being read)
+        // load (only entries active before the group; the rest are written before being read):
+        // asynchronous 8-byte copies, zero-filled for inactive entries, all in flight at once
         for (int t = threadIdx.x; t < T; t += kThreads) {
             const uint64_t a = base ^ hi_tab[t >> low] ^ ((uint64_t)t & lowmask);
-            float2 v = f2(0.f, 0.f);
-            if (!(a & in_inactive)) {
-                v = E[a];
-                v.x *= sc;
-                v.y *= sc;
-            }
-            sh[t] = v;
+            const bool act = !(a & in_inactive);
+            const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&sh[t]);
+            const float2* src = act ? E + a : E;
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(dst), "l"(src), "r"(act ? 8 : 0)
+                         : "memory");
         }
+        asm volatile("cp.async.wait_all;\n" ::: "memory");
         __syncthreads();
         for (int s = 0; s < A.count; ++s) {
             const FusedStep& st = A.st[s];
-            const StepConst& c = sc_tab[s];
-            if (!(base & st.cskip)) {
-                // tile-constant part of the sign: parity(base & beta) ^ ov
-                const int cs = (__popcll(base & st.beta) & 1) ^ c.ov;
-                const int nrep = T >> st.nins;
-                const uint32_t tpw = tp_tab[s * kThreads + threadIdx.x];
-                switch (st.kind) {
-                    case DCS_KIND_GROW: run_step<DCS_KIND_GROW>(sh, nrep, tpw, st, c, cs); break;
-                    case DCS_KIND_MIX: run_step<DCS_KIND_MIX>(sh, nrep, tpw, st, c, cs); break;
-                    case DCS_KIND_DIAG: run_step<DCS_KIND_DIAG>(sh, nrep, tpw, st, c, cs); break;
-                    case DCS_KIND_REPLACE: run_step<DCS_KIND_REPLACE>(sh, nrep, tpw, st, c, cs); break;
-                    case DCS_KIND_FIXED: run_step<DCS_KIND_FIXED>(sh, nrep, tpw, st, c, cs); break;
-                    case DCS_KIND_FIXED_SHRINK: run_step<DCS_KIND_FIXED_SHRINK>(sh, nrep, tpw, st, c, cs); break;
-                    case DCS_KIND_SHRINK4: run_step<DCS_KIND_SHRINK4>(sh, nrep, tpw, st, c, cs); break;
-                    default: run_step<DCS_KIND_SHRINK2>(sh, nrep, tpw, st, c, cs); break;
-                }
+            const float4 w = fw[s];
+            const float2 f0 = f2(w.x, w.y), f1 = f2(w.z, w.w);
+            const int y = ovy[s] >> 1;
+            // tile-constant part of the sign: parity(base & beta) ^ ov
+            const int cs = (__popcll(base & st.beta) & 1) ^ (ovy[s] & 1);
+            if (!(base & st.cskip)) switch (st.kind) {
+                case DCS_KIND_GROW: run_step<DCS_KIND_GROW>(sh, T, st, f0, f1, cs, y); break;
+                case DCS_KIND_MIX: run_step<DCS_KIND_MIX>(sh, T, st, f0, f1, cs, y); break;
+                case DCS_KIND_DIAG: run_step<DCS_KIND_DIAG>(sh, T, st, f0, f1, cs, y); break;
+                case DCS_KIND_REPLACE: run_step<DCS_KIND_REPLACE>(sh, T, st, f0, f1, cs, y); break;
+                case DCS_KIND_FIXED: run_step<DCS_KIND_FIXED>(sh, T, st, f0, f1, cs, y); break;
+                case DCS_KIND_FIXED_SHRINK: run_step<DCS_KIND_FIXED_SHRINK>(sh, T, st, f0, f1, cs, y); break;
+                case DCS_KIND_SHRINK4: run_step<DCS_KIND_SHRINK4>(sh, T, st, f0, f1, cs, y); break;
+                default: run_step<DCS_KIND_SHRINK2>(sh, T, st, f0, f1, cs, y); break;
             }
             __syncthreads();
         }
@@ -230,7 +212,7 @@ k_fused(float2* __restrict__ E, const __grid_constant__ FusedArgs A, const dcs_p
         for (int t = threadIdx.x; t < T; t += kThreads) {
             const uint64_t a = base ^ hi_tab[t >> low] ^ ((uint64_t)t & lowmask);
             if (a & out_inactive) continue;
-            const float2 v = sh[t];
+            const float2 v = f2(sh[t].x * sc, sh[t].y * sc);  // the pass's 2^-e (exact; the steps are linear)
             lm = fmaxf(lm, v.x * v.x + v.y * v.y);
             E[a] = v;
         }
@@ -300,8 +282,7 @@ extern "C" int dcs_fused_groups(void* table, const dcs_step* steps, int nsteps, 
             }
         }
         const size_t smem = sizeof(float2) * ((size_t)1 << g.tile_dim) +
-                            sizeof(uint64_t) * ((size_t)1 << (g.tile_dim - g.low_bits)) +
-                            sizeof(uint32_t) * (size_t)g.count * kThreads + sizeof(StepConst) * (size_t)g.count;
+                            sizeof(uint64_t) * ((size_t)1 << (g.tile_dim - g.low_bits));
         if (!max_smem_set[dev]) {
             cudaError_t e = cudaFuncSetAttribute(k_fused<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
             if (e == cudaSuccess)
