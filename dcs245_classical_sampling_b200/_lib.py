@@ -62,6 +62,7 @@ SIGNATURES = {
     "dcs_block_tail": (_I, [_P, _I, _P, _P, _I, _P]),
     "dcs_draw_scratch_bytes": (ctypes.c_size_t, [_I, _I]),
     "dcs_draw": (_I, [_P, _I, _I, _P, _P, _P, _P]),
+    "dcs_draw_static": (_I, [_P, _I, _P, _P, _P]),
     "dcs_overlap": (_I, [_P, _P, _U64, _P, _P, _P]),
 }
 

@@ -18,6 +18,8 @@
 //   5. the 53-bit grid total-variation diagnostic of the reference.
 #include <string.h>
 
+#include <mutex>
+
 #include "common.cuh"
 
 namespace {
@@ -426,5 +428,82 @@ extern "C" int dcs_overlap(const double* ref, const double* ap, uint64_t len, do
     DCS_CHECK_LAUNCH("k_overlap");
     k_overlap_final<<<1, 32, 0, s>>>((const dd*)scratch, parts, out);
     DCS_CHECK_LAUNCH("k_overlap_final");
+    return DCS_OK;
+}
+
+// ---------------------------------------------------------------- draw without allocation
+//
+// For callers that cannot allocate device memory at the point where they draw: code that runs
+// while a CUDA stream is being captured (cudaMalloc cannot be captured), host runtimes that
+// hand the library only the buffers they own and forbid allocation in their sampling loop, and
+// latency-sensitive loops where an allocation would synchronise the device.  The scratch lives
+// in a file-scope device array of fixed size, so this entry point allocates nothing.
+//
+// Limit: one block of up to 2^20 amplitudes per call (DCS_DRAW_STATIC_MAX_K); every GPU that
+// loads the library holds the array (about 8.1 MiB) until the process exits.
+namespace {
+constexpr size_t kStaticDrawBytes = ((size_t)1 << DCS_DRAW_STATIC_MAX_K) * sizeof(double) +
+                                    (((size_t)1 << DCS_DRAW_STATIC_MAX_K) / kChunk) * (sizeof(dd) + sizeof(double)) +
+                                    sizeof(BlockState) + 4096;
+static __device__ __align__(256) unsigned char g_draw_scratch[kStaticDrawBytes];
+
+// the device address of g_draw_scratch, looked up once per device with that device current
+std::mutex g_static_mutex;
+void* g_static_ptr[64] = {nullptr};
+}  // namespace
+
+extern "C" int dcs_draw_static(const double* blocks, int k, const double* uniform, dcs_draw_result* result,
+                               void* stream) {
+    if (!blocks || !uniform || !result || k < 0 || k > 30) {
+        dcs_host::set_error("dcs_draw_static: invalid arguments");
+        return DCS_E_ARG;
+    }
+    const Layout L = layout(k, 1);
+    if (k > DCS_DRAW_STATIC_MAX_K || L.bytes > kStaticDrawBytes) {
+        dcs_host::set_error("dcs_draw_static: block of 2^%d amplitudes exceeds the static maximum of 2^%d", k,
+                            DCS_DRAW_STATIC_MAX_K);
+        return DCS_E_ARG;
+    }
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return dcs_host::check_cuda(e, "dcs_draw_static: cudaGetDevice");
+    if (dev < 0 || dev >= 64) {
+        dcs_host::set_error("dcs_draw_static: device index %d out of range", dev);
+        return DCS_E_ARG;
+    }
+    void* scratch = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_static_mutex);
+        if (!g_static_ptr[dev]) {
+            void* p = nullptr;
+            e = cudaGetSymbolAddress(&p, g_draw_scratch);
+            if (e != cudaSuccess) return dcs_host::check_cuda(e, "dcs_draw_static: cudaGetSymbolAddress");
+            g_static_ptr[dev] = p;
+        }
+        scratch = g_static_ptr[dev];
+    }
+    char* base = (char*)scratch;
+    double* w = (double*)(base + L.w);
+    dd* cs = (dd*)(base + L.chunk_sum);
+    BlockState* st = (BlockState*)(base + L.state);
+    double* part = (double*)(base + L.tv_part);
+    const uint64_t n = 1ull << k;
+    const int nch = (int)(n >= (uint64_t)kChunk ? n / kChunk : 1);
+    cudaStream_t s = (cudaStream_t)stream;
+    // the array keeps the previous call's contents: the per-block state must start at zero
+    e = cudaMemsetAsync(st, 0, sizeof(BlockState), s);
+    if (e != cudaSuccess) return dcs_host::check_cuda(e, "dcs_draw_static memset");
+    k_weights<<<dim3(nch, 1), kThreads, 0, s>>>((const double2*)blocks, k, w, cs, st);
+    DCS_CHECK_LAUNCH("k_weights");
+    k_scan_locate<<<1, 1, 0, s>>>(cs, nch, uniform, st, result);
+    DCS_CHECK_LAUNCH("k_scan_locate");
+    k_locate_elem<<<1, kThreads, 0, s>>>(w, k, cs, nch, st, result);
+    DCS_CHECK_LAUNCH("k_locate_elem");
+    k_sequential<<<1, 32, 0, s>>>(w, k, st, result, 1);
+    DCS_CHECK_LAUNCH("k_sequential");
+    k_tv<<<dim3(nch, 1), kThreads, 0, s>>>(w, k, cs, nch, st, result, part);
+    DCS_CHECK_LAUNCH("k_tv");
+    k_tv_final<<<1, 32, 0, s>>>(part, nch, st, result, 1);
+    DCS_CHECK_LAUNCH("k_tv_final");
     return DCS_OK;
 }

@@ -219,6 +219,20 @@ size_t dcs_draw_scratch_bytes(int k, int nblocks);
 int dcs_draw(const double *blocks, int k, int nblocks, const double *uniforms, void *scratch,
              dcs_draw_result *results, void *stream);
 
+/* Draw that allocates nothing (no counterpart in the reference; this library's addition).
+ * For callers that cannot allocate device memory where they sample: code running while a
+ * stream is captured, host runtimes that lend the library only their own buffers, loops where
+ * an allocation would synchronise the device.  Same computation and result as dcs_draw for
+ * one block, with the scratch in a fixed device array inside the library (about 8.1 MiB per
+ * GPU that loads the library, held until the process exits).  Limit: one block of at most
+ * 2^DCS_DRAW_STATIC_MAX_K amplitudes per call; larger blocks are rejected with DCS_E_ARG.
+ * The first call on each device looks the array up (cudaGetSymbolAddress) with that device
+ * current; make that first call before any stream capture.  All calls share the array:
+ * calls that overlap on the GPU (other streams, other threads) race and must be serialised
+ * by the caller.  blocks, uniform (1 double) and result are device memory. */
+#define DCS_DRAW_STATIC_MAX_K 20
+int dcs_draw_static(const double *blocks, int k, const double *uniform, dcs_draw_result *result, void *stream);
+
 /* Audit sums of two complex128 vectors (compensated FP64): out[0] = <ref,ref>,
  * out[1] = <ap,ap>, out[2] + i out[3] = <ref,ap> = sum conj(ref) ap.  scratch: 16 KiB of
  * device memory; out: 4 doubles of device memory.  Reference quantity:
