@@ -48,6 +48,11 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--seed", type=int, default=24520)
     ap.add_argument("--tune", action="store_true", help="autotune the fused tile shape before timing")
+    ap.add_argument("--serve", action="store_true", help="run the serving mix (32q/48q/64q) instead")
+    ap.add_argument("--serve-seconds", type=float, default=20.0, help="arrival window of the serving run")
+    ap.add_argument("--serve-rate", type=float, default=1.0, help="Poisson request rate (1/s)")
+    ap.add_argument("--serve-max-samples", type=int, default=64)
+    ap.add_argument("--hbm-budget-gib", type=float, default=170.0)
     return ap.parse_args()
 
 
@@ -420,10 +425,66 @@ def kernel_roofline(eng, prep, out, stream):
             "launch_ms": [round(a.elapsed_time(b), 3) for a, b, _ in evs]}
 
 
+def serve_arm(args):
+    """Serving mix: Poisson requests against three circuits, continuous batching, p50/p99."""
+    import torch
+    from dcs245_classical_sampling_b200.serve import CircuitRunner, Server, latency_stats, poisson_requests
+    from dcs245_classical_sampling_b200.workloads import build_workload
+    rank, world, local = dist_init()
+    torch.cuda.set_device(local)
+    mix = {"ring32_d37_t79_k14": 50, "ring48_d55_t177_k17": 30, "ring64_d73_t314_k20": 20}
+    budget = args.hbm_budget_gib * 2 ** 30
+    t0 = time.perf_counter()
+    runners = {}
+    big = CircuitRunner("ring64_d73_t314_k20", build_workload("ring64_d73_t314_k20"), key=args.seed + 64,
+                        max_samples=1, device=local)
+    runners[big.name] = big
+    left = budget - big.table_bytes()
+    for name, share in (("ring48_d55_t177_k17", 0.8), ("ring32_d37_t79_k14", 0.2)):
+        runners[name] = CircuitRunner(name, build_workload(name), key=args.seed + len(runners), max_samples=64,
+                                      device=local, hbm_budget=left * share)
+    setup = time.perf_counter() - t0
+    # warm every runner once
+    from dcs245_classical_sampling_b200.serve import Request
+    Server(runners).run([Request(10 ** 6 + i, c, 1, 0.0) for i, c in enumerate(runners)], realtime=False)
+    reqs = poisson_requests(args.serve_rate, args.serve_seconds, mix, seed=args.seed,
+                            max_samples=args.serve_max_samples)
+    clocks = ClockSampler(local)
+    clocks.start()
+    ta = time.perf_counter()
+    done = Server(runners).run(reqs, realtime=True)
+    span = time.perf_counter() - ta
+    clk = clocks.stop()
+    per = {}
+    for r in done:
+        d = per.setdefault(r.circuit, {"requests": 0, "samples": 0, "lat_ms": []})
+        d["requests"] += 1
+        d["samples"] += r.nsamples
+        d["lat_ms"].append((r.finish - r.arrival) * 1e3)
+    for d in per.values():
+        lat = d.pop("lat_ms")
+        d["p50_ms"], d["p99_ms"] = float(np.percentile(lat, 50)), float(np.percentile(lat, 99))
+    tot = sum(r.nsamples for r in done)
+    ties = sum(int(rec["tie"]) for r in done for rec, _ in r.records.values())
+    bad = sum(int(rec["status"] != 0) for r in done for rec, _ in r.records.values())
+    line = {"metric": "serving mix: samples/s and request p50/p99 ms (32q 2^14, 48q 2^17, 64q 2^20; 50/30/20)",
+            "value": tot / span, "unit": "samples/s", "n_gpus": 1, "higher_is_better": True,
+            "latency": latency_stats(done), "per_circuit": per, "requests": len(done), "samples": tot,
+            "span_s": span, "arrival_window_s": args.serve_seconds, "rate_hz": args.serve_rate,
+            "hbm_budget_gib": args.hbm_budget_gib,
+            "slots": {c: {"samples_per_launch": r.max_samples, "table_items": r.engine.items,
+                          "table_gib": r.table_bytes() / 2 ** 30, "mode": r.mode} for c, r in runners.items()},
+            "ties": ties, "failed_draws": bad, "setup_s": setup, "clocks": clk,
+            "data": "synthetic (seeded ring circuits, Philox4x32-10 prefixes and uniforms on the device)"}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         reference_arm(args)
+    elif args.serve:
+        serve_arm(args)
     else:
         gpu_arm(args)
 

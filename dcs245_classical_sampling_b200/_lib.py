@@ -64,6 +64,9 @@ SIGNATURES = {
     "dcs_draw": (_I, [_P, _I, _I, _P, _P, _P, _P]),
     "dcs_draw_static": (_I, [_P, _I, _P, _P, _P]),
     "dcs_overlap": (_I, [_P, _P, _U64, _P, _P, _P]),
+    "dcs_philox_prefixes": (_I, [_P, _P, _I, _U64, _P, _I, _P, _P, _P]),
+    "dcs_philox4x32_10_host": (None, [_P, ctypes.c_uint32, ctypes.c_uint32]),
+    "dcs_build_items": (_I, [_P, _P, _P, _P, _P, _P, _P, _P, _I, _I, _I, _P, _I, _P, _P, _P, _P]),
 }
 
 

@@ -233,6 +233,29 @@ int dcs_draw(const double *blocks, int k, int nblocks, const double *uniforms, v
 #define DCS_DRAW_STATIC_MAX_K 20
 int dcs_draw_static(const double *blocks, int k, const double *uniform, dcs_draw_result *result, void *stream);
 
+/* Serving: prefixes and uniforms from Philox4x32-10 on the device (no reference counterpart:
+ * the reference draws them on the host with NumPy PCG64, sampling_protocol.py:14-41).
+ * Sample i uses counter (req[i], idx[i], 0, 0) and key (low, high 32 bits of `key`); output
+ * words 0-1 give the closed bits (bit j -> qubit closed[j], nclosed <= 64) as a qubit mask in
+ * xbits[i], words 2-3 give uniforms[i] = (w3:w2 >> 11) * 2^-53.  All pointers device. */
+int dcs_philox_prefixes(const uint32_t *req, const uint32_t *idx, int count, uint64_t key, const int32_t *closed,
+                        int nclosed, uint64_t *xbits, double *uniforms, void *stream);
+/* The same Philox4x32-10 bijection on the host (ctr is updated in place), for checking. */
+void dcs_philox4x32_10_host(uint32_t ctr[4], uint32_t key0, uint32_t key1);
+
+/* Serving: per-(sample, slice) contraction parameters built on the device from prefix bits —
+ * the reference's host bookkeeping (conditional_block_gpu.py:136-157, inplace_gpu.py:111-114).
+ * Static per-circuit tables (device): fsel (8 doubles per step: f for x bit 0, f for x bit 1),
+ * xq (data qubit selecting the row, -1 for references), fixidx (index among fixed steps or -1),
+ * flip (nslices x nsteps bytes), F (nfixed x ceil(nsteps/32) words: later-neighbour masks of
+ * fixed steps), tail (nfixed terminal-offset xors), coef (2 doubles per slice), freeflip (per
+ * slice).  Output item i = sample * nslices + slice: params[i * nsteps + j], coefs[2i..2i+1],
+ * xors[i]. */
+int dcs_build_items(const double *fsel, const int32_t *xq, const int32_t *fixidx, const uint8_t *flip,
+                    const uint32_t *F, const uint64_t *tail, const double *coef, const uint64_t *freeflip,
+                    int nsteps, int nfixed, int nslices, const uint64_t *xbits, int nsamples, dcs_param *params,
+                    double *coefs, uint64_t *xors, void *stream);
+
 /* Audit sums of two complex128 vectors (compensated FP64): out[0] = <ref,ref>,
  * out[1] = <ap,ap>, out[2] + i out[3] = <ref,ap> = sum conj(ref) ap.  scratch: 16 KiB of
  * device memory; out: 4 doubles of device memory.  Reference quantity:
