@@ -174,15 +174,19 @@ class InplaceConditionalBlockGPU:
         self._alloc = False
 
     # ------------------------------------------------------------------ allocation
-    def alloc(self, dtype=np.complex64, device=0, fp64_kernel_path=None, mode="device", items=None,
+    def alloc(self, dtype=np.complex64, device=0, fp64_kernel_path=None, mode=None, items=None,
               hbm_budget=None):
         """Allocate device buffers (conditional_block_inplace_gpu.py:18-34).
 
         dtype: complex64 (FP32 arithmetic) or complex128 (FP64 arithmetic).
+        mode: "plain", "device" or "fused" (default: fused for complex64 tables of 2^26 entries
+        and more, device otherwise).
         items: concurrent work items (slices) per launch; default = as many slices as fit
         in the HBM budget (default 85% of free device memory)."""
         if np.dtype(dtype) not in (np.dtype(np.complex64), np.dtype(np.complex128)):
             raise ValueError(dtype)
+        if mode is None:  # fused passes pay off once the tables are far larger than a tile
+            mode = "fused" if np.dtype(dtype) == np.dtype(np.complex64) and self.plan.maxslots >= 26 else "device"
         if mode not in ("plain", "device", "fused"):
             raise ValueError(mode)
         if mode == "fused" and np.dtype(dtype) != np.dtype(np.complex64):
