@@ -31,6 +31,10 @@ REPO = Path(__file__).resolve().parent
 sys.path.insert(0, str(REPO))
 
 METRIC = "samples/s (64q, 2^20 block) served vs plain at c_y≥0.9999; p50/p99 ms"
+# DRAM traffic / algorithmic bytes of one k_fused launch, measured by ncu on a 2^27-universe group
+# of the same plan (profiles/k_fused_ring64_prefix_group23.md): full-size launches cannot be
+# captured with all counters, and the traffic of a group scales with the entries it touches.
+FUSED_TRAFFIC_RATIO = 0.9635
 FALLBACK_HBM = 6650.0
 
 
@@ -361,7 +365,10 @@ def gpu_arm(args):
                         "d2h_bytes_per_step": d2h},
                 "gpu_launches": launches,
                 "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
-                             "traffic": None, "kernel": dom["kernel"],
+                             "traffic": (FUSED_TRAFFIC_RATIO * dom["alg_bytes_per_launch"]
+                                         if dom["kernel"] == "k_fused" else None),
+                             "traffic_note": "ncu dram bytes of a 2^27-universe k_fused launch scaled by entries",
+                             "kernel": dom["kernel"],
                              "peak_source": f"{how} (MEASURED_PEAKS.json hbm_gbs)" if how == "measured" else
                              "fallback 6650 GB/s", "launches": dom["launches"],
                              "alg_bytes_per_launch": dom["alg_bytes_per_launch"],
