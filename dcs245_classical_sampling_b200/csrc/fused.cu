@@ -32,6 +32,7 @@ struct FusedStep {
 
 struct FusedArgs {
     int32_t count, tile_dim, low_bits, coset_m, ncoset_runs, group;
+    int32_t pair_in, pair_out;  // slot 0 (tile bit 0) active before / after the group
     uint64_t in_mask_first, out_mask_last;
     uint64_t basis[16];
     uint32_t coset_runs[DCS_MAX_RUNS];
@@ -71,67 +72,76 @@ __device__ __forceinline__ uint32_t spread(uint32_t o, const uint8_t* ins, int n
 // index o = tid + 256 k is spread as spread(tid) | spread(256 k): the first part is fixed per
 // thread and step; the second is the same for every thread and walks the tile bits in mhi in
 // increasing order with ((v | ~mhi) + 1) & mhi.
+// Shared-memory accessors by byte offset (offset = 8 * tile index).
+__device__ __forceinline__ float2 ldsh(const unsigned char* base, uint32_t off) {
+    return *reinterpret_cast<const float2*>(base + off);
+}
+__device__ __forceinline__ void stsh(unsigned char* base, uint32_t off, float2 v) {
+    *reinterpret_cast<float2*>(base + off) = v;
+}
+
 template <int KIND>
-__device__ __forceinline__ void run_step(float2* __restrict__ sh, int T, const FusedStep& st, float2 f0, float2 f1,
-                                         int cs, int y) {
+__device__ __forceinline__ void run_step(unsigned char* __restrict__ shb, int T, const FusedStep& st, float2 f0,
+                                         float2 f1, int cs, int y) {
     const int nins = st.nins;
     const int nrep = T >> nins;  // a power of two
     if ((int)threadIdx.x >= nrep) return;
-    const uint32_t tbeta = st.tbeta;
-    const uint32_t tp = spread(threadIdx.x, st.ins, nins);
-    const int hs = (__popc(tp & tbeta) & 1) ^ cs;
-    const uint32_t mhi = st.mhi;
+    // tile indices are handled as byte offsets (index << 3) throughout
+    const uint32_t tbeta3 = st.tbeta << 3;
+    const uint32_t tp = spread(threadIdx.x, st.ins, nins) << 3;
+    const int hs = (__popc(tp & tbeta3) & 1) ^ cs;
+    const uint32_t mhi3 = st.mhi << 3;
     const int niter = nrep > kThreads ? nrep >> kThreadLog : 1;
     // partner-sign factors of this step, (-1)^sK and (-1)^sKa, and f0 +- f1 for the diagonal kinds
     const float gK = st.sK ? -1.f : 1.f, gKa = st.sKa ? -1.f : 1.f;
     const float2 fp = f2(f0.x + f1.x, f0.y + f1.y), fm = f2(f0.x - f1.x, f0.y - f1.y);
     const float2 f1a = f2(gKa * f1.x, gKa * f1.y);  // f1 (-1)^sKa
-    const uint32_t tK = st.tK, tKa = st.tKa, tpiv = st.tpiv;
-    uint32_t tu = 0;  // spread(256 k), advanced by a masked increment over mhi
+    const uint32_t tK = st.tK << 3, tKa = st.tKa << 3, tpiv = st.tpiv << 3;
+    uint32_t tu = 0;  // spread(256 k) << 3, advanced by a masked increment over mhi << 3
 #pragma unroll 4
     for (int k = 0; k < niter; ++k) {
         const uint32_t t = tp | tu;
-        const int sc = hs ^ (__popc(tu & tbeta) & 1);
-        tu = ((tu | ~mhi) + 1u) & mhi;
-        const float2 x = sh[t];
+        const int sc = hs ^ (__popc(tu & tbeta3) & 1);
+        tu = ((tu | ~mhi3) + 1u) & mhi3;
+        const float2 x = ldsh(shb, t);
         if constexpr (KIND == DCS_KIND_GROW) {
-            sh[t] = fmul(f0, x);
-            sh[t ^ tpiv] = negif(fmul(f1, x), sc);
+            stsh(shb, t, fmul(f0, x));
+            stsh(shb, t ^ tpiv, negif(fmul(f1, x), sc));
         } else if constexpr (KIND == DCS_KIND_MIX) {
             // o0 = f0 x + s_c f1 (-1)^sKa b ;  o1 = f0 b + s_c f1 x
             const uint32_t td = t ^ tKa;
-            const float2 b = sh[td];
-            sh[t] = fmadd(f0, x, negif(fmul(f1a, b), sc));
-            sh[td] = fmadd(f0, b, negif(fmul(f1, x), sc));
+            const float2 b = ldsh(shb, td);
+            stsh(shb, t, fmadd(f0, x, negif(fmul(f1a, b), sc)));
+            stsh(shb, td, fmadd(f0, b, negif(fmul(f1, x), sc)));
         } else if constexpr (KIND == DCS_KIND_DIAG) {
-            sh[t] = fmul(sc ? fm : fp, x);
+            stsh(shb, t, fmul(sc ? fm : fp, x));
         } else if constexpr (KIND == DCS_KIND_REPLACE) {
             // o0 = f0 (x + b) ;  o1 = s_c f1 (x + (-1)^sK b)
             const uint32_t td = t ^ tK;
-            const float2 b = sh[td];
-            sh[t] = fmul(f0, f2(x.x + b.x, x.y + b.y));
-            sh[td] = negif(fmul(f1, f2(fmaf(gK, b.x, x.x), fmaf(gK, b.y, x.y))), sc);
+            const float2 b = ldsh(shb, td);
+            stsh(shb, t, fmul(f0, f2(x.x + b.x, x.y + b.y)));
+            stsh(shb, td, negif(fmul(f1, f2(fmaf(gK, b.x, x.x), fmaf(gK, b.y, x.y))), sc));
         } else if constexpr (KIND == DCS_KIND_FIXED) {
-            sh[t] = y ? negif(fmul(f1, x), sc) : fmul(f0, x);
+            stsh(shb, t, y ? negif(fmul(f1, x), sc) : fmul(f0, x));
         } else if constexpr (KIND == DCS_KIND_FIXED_SHRINK) {
             const uint32_t td = t ^ tK;
-            const float2 b = sh[td];
-            sh[t] = y ? negif(fmul(f1, f2(fmaf(gK, b.x, x.x), fmaf(gK, b.y, x.y))), sc)
-                      : fmul(f0, f2(x.x + b.x, x.y + b.y));
+            const float2 b = ldsh(shb, td);
+            stsh(shb, t, y ? negif(fmul(f1, f2(fmaf(gK, b.x, x.x), fmaf(gK, b.y, x.y))), sc)
+                           : fmul(f0, f2(x.x + b.x, x.y + b.y)));
         } else if constexpr (KIND == DCS_KIND_SHRINK4) {
             // o0 = f0 (x + b) + s_d f1 (g + (-1)^sK h) ;  o1 = f0 (g + h) + s_c f1 (x + (-1)^sK b)
             const uint32_t t1 = t ^ tK, td = t ^ tKa, td1 = td ^ tK;
-            const float2 b = sh[t1], g = sh[td], h = sh[td1];
+            const float2 b = ldsh(shb, t1), g = ldsh(shb, td), h = ldsh(shb, td1);
             const int sd = sc ^ st.sKa;
-            sh[t] = fmadd(f0, f2(x.x + b.x, x.y + b.y),
-                          negif(fmul(f1, f2(fmaf(gK, h.x, g.x), fmaf(gK, h.y, g.y))), sd));
-            sh[td] = fmadd(f0, f2(g.x + h.x, g.y + h.y),
-                           negif(fmul(f1, f2(fmaf(gK, b.x, x.x), fmaf(gK, b.y, x.y))), sc));
+            stsh(shb, t, fmadd(f0, f2(x.x + b.x, x.y + b.y),
+                               negif(fmul(f1, f2(fmaf(gK, h.x, g.x), fmaf(gK, h.y, g.y))), sd)));
+            stsh(shb, td, fmadd(f0, f2(g.x + h.x, g.y + h.y),
+                                negif(fmul(f1, f2(fmaf(gK, b.x, x.x), fmaf(gK, b.y, x.y))), sc)));
         } else {  // DCS_KIND_SHRINK2: f0 (x + b) + s_c f1 (x + (-1)^sK b)
             const uint32_t td = t ^ tK;
-            const float2 b = sh[td];
-            sh[t] = fmadd(f0, f2(x.x + b.x, x.y + b.y),
-                          negif(fmul(f1, f2(fmaf(gK, b.x, x.x), fmaf(gK, b.y, x.y))), sc));
+            const float2 b = ldsh(shb, td);
+            stsh(shb, t, fmadd(f0, f2(x.x + b.x, x.y + b.y),
+                               negif(fmul(f1, f2(fmaf(gK, b.x, x.x), fmaf(gK, b.y, x.y))), sc)));
         }
     }
 }
@@ -178,14 +188,27 @@ k_fused(float2* __restrict__ E, const __grid_constant__ FusedArgs A, const dcs_p
     for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const uint64_t base = deposit(tile, A.coset_runs, A.ncoset_runs);
         // load (only entries active before the group; the rest are written before being read):
-        // asynchronous 8-byte copies, zero-filled for inactive entries, all in flight at once
-        for (int t = threadIdx.x; t < T; t += kThreads) {
-            const uint64_t a = base ^ hi_tab[t >> low] ^ ((uint64_t)t & lowmask);
-            const bool act = !(a & in_inactive);
-            const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&sh[t]);
-            const float2* src = act ? E + a : E;
-            asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(dst), "l"(src), "r"(act ? 8 : 0)
-                         : "memory");
+        // asynchronous copies, zero-filled for inactive entries, all in flight at once.  When
+        // slot 0 is active before the group, entries t and t+1 (t even) share their activity
+        // and sit in one aligned 16-byte pair: one copy moves both.
+        if (A.pair_in) {
+            for (int t = 2 * threadIdx.x; t < T; t += 2 * kThreads) {
+                const uint64_t a = base ^ hi_tab[t >> low] ^ ((uint64_t)t & lowmask);
+                const bool act = !(a & in_inactive);
+                const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&sh[t]);
+                const float2* src = act ? E + a : E;
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src), "r"(act ? 16 : 0)
+                             : "memory");
+            }
+        } else {
+            for (int t = threadIdx.x; t < T; t += kThreads) {
+                const uint64_t a = base ^ hi_tab[t >> low] ^ ((uint64_t)t & lowmask);
+                const bool act = !(a & in_inactive);
+                const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&sh[t]);
+                const float2* src = act ? E + a : E;
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(dst), "l"(src), "r"(act ? 8 : 0)
+                             : "memory");
+            }
         }
         asm volatile("cp.async.wait_all;\n" ::: "memory");
         __syncthreads();
@@ -197,24 +220,35 @@ k_fused(float2* __restrict__ E, const __grid_constant__ FusedArgs A, const dcs_p
             // tile-constant part of the sign: parity(base & beta) ^ ov
             const int cs = (__popcll(base & st.beta) & 1) ^ (ovy[s] & 1);
             if (!(base & st.cskip)) switch (st.kind) {
-                case DCS_KIND_GROW: run_step<DCS_KIND_GROW>(sh, T, st, f0, f1, cs, y); break;
-                case DCS_KIND_MIX: run_step<DCS_KIND_MIX>(sh, T, st, f0, f1, cs, y); break;
-                case DCS_KIND_DIAG: run_step<DCS_KIND_DIAG>(sh, T, st, f0, f1, cs, y); break;
-                case DCS_KIND_REPLACE: run_step<DCS_KIND_REPLACE>(sh, T, st, f0, f1, cs, y); break;
-                case DCS_KIND_FIXED: run_step<DCS_KIND_FIXED>(sh, T, st, f0, f1, cs, y); break;
-                case DCS_KIND_FIXED_SHRINK: run_step<DCS_KIND_FIXED_SHRINK>(sh, T, st, f0, f1, cs, y); break;
-                case DCS_KIND_SHRINK4: run_step<DCS_KIND_SHRINK4>(sh, T, st, f0, f1, cs, y); break;
-                default: run_step<DCS_KIND_SHRINK2>(sh, T, st, f0, f1, cs, y); break;
+                case DCS_KIND_GROW: run_step<DCS_KIND_GROW>(smem, T, st, f0, f1, cs, y); break;
+                case DCS_KIND_MIX: run_step<DCS_KIND_MIX>(smem, T, st, f0, f1, cs, y); break;
+                case DCS_KIND_DIAG: run_step<DCS_KIND_DIAG>(smem, T, st, f0, f1, cs, y); break;
+                case DCS_KIND_REPLACE: run_step<DCS_KIND_REPLACE>(smem, T, st, f0, f1, cs, y); break;
+                case DCS_KIND_FIXED: run_step<DCS_KIND_FIXED>(smem, T, st, f0, f1, cs, y); break;
+                case DCS_KIND_FIXED_SHRINK: run_step<DCS_KIND_FIXED_SHRINK>(smem, T, st, f0, f1, cs, y); break;
+                case DCS_KIND_SHRINK4: run_step<DCS_KIND_SHRINK4>(smem, T, st, f0, f1, cs, y); break;
+                default: run_step<DCS_KIND_SHRINK2>(smem, T, st, f0, f1, cs, y); break;
             }
             __syncthreads();
         }
-        // store (only entries active after the group) and max
-        for (int t = threadIdx.x; t < T; t += kThreads) {
-            const uint64_t a = base ^ hi_tab[t >> low] ^ ((uint64_t)t & lowmask);
-            if (a & out_inactive) continue;
-            const float2 v = f2(sh[t].x * sc, sh[t].y * sc);  // the pass's 2^-e (exact; the steps are linear)
-            lm = fmaxf(lm, v.x * v.x + v.y * v.y);
-            E[a] = v;
+        // store (only entries active after the group) and max; pairs when slot 0 is active after
+        if (A.pair_out) {
+            for (int t = 2 * threadIdx.x; t < T; t += 2 * kThreads) {
+                const uint64_t a = base ^ hi_tab[t >> low] ^ ((uint64_t)t & lowmask);
+                if (a & out_inactive) continue;
+                const float4 q = *reinterpret_cast<const float4*>(&sh[t]);
+                const float4 v = make_float4(q.x * sc, q.y * sc, q.z * sc, q.w * sc);  // the pass's 2^-e
+                lm = fmaxf(lm, fmaxf(v.x * v.x + v.y * v.y, v.z * v.z + v.w * v.w));
+                *reinterpret_cast<float4*>(E + a) = v;
+            }
+        } else {
+            for (int t = threadIdx.x; t < T; t += kThreads) {
+                const uint64_t a = base ^ hi_tab[t >> low] ^ ((uint64_t)t & lowmask);
+                if (a & out_inactive) continue;
+                const float2 v = f2(sh[t].x * sc, sh[t].y * sc);  // the pass's 2^-e (exact; the steps are linear)
+                lm = fmaxf(lm, v.x * v.x + v.y * v.y);
+                E[a] = v;
+            }
         }
         __syncthreads();
     }
@@ -259,6 +293,8 @@ extern "C" int dcs_fused_groups(void* table, const dcs_step* steps, int nsteps, 
         A.group = gi;
         A.in_mask_first = steps[g.first].in_mask;
         A.out_mask_last = g.out_mask;
+        A.pair_in = g.low_bits >= 1 && (A.in_mask_first & 1ull);
+        A.pair_out = g.low_bits >= 1 && (A.out_mask_last & 1ull);
         for (int i = 0; i < 16; ++i) A.basis[i] = g.basis[i];
         for (int r = 0; r < DCS_MAX_RUNS; ++r) A.coset_runs[r] = g.coset_runs[r];
         for (int s = 0; s < g.count; ++s) {
