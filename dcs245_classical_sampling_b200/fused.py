@@ -152,6 +152,22 @@ def build_fused_plan(plan, max_dim=13, low=4, max_steps=MAX_GROUP_STEPS, max_ext
             basis, pivots = _reduced_basis(vecs, l)
         if len(basis) > MAX_BASIS:
             raise ValueError(f"group {gi}: {len(basis)} tile basis vectors exceed {MAX_BASIS}")
+        # order the non-low coordinates by how often a step of the group inserts a zero there
+        # (role slots and inactive slots): the least-inserted ones take the low coordinates, so
+        # the 32 lanes of a warp mostly touch consecutive entries (fewer bank conflicts)
+        group_steps_ = steps[first:first + count]
+        def inserted(pv):
+            c = 0
+            for st in group_steps_:
+                kind, omit = orbit_kind(st)
+                role = {KIND_GROW: [st.pivot], 1: [st.pivot_a], 3: [st.pivot], 5: [st.pivot], 7: [st.pivot],
+                        6: [st.pivot, st.pivot_a]}.get(kind, [])
+                if pv in role or not (slot_mask(st.active_in) >> pv) & 1:
+                    c += 1
+            return c
+        order_ = sorted(range(len(basis)), key=lambda i: (inserted(pivots[i]), i))
+        basis = [basis[i] for i in order_]
+        pivots = [pivots[i] for i in order_]
         dim = l + len(basis)
         for b in basis:
             if b & ~U:
