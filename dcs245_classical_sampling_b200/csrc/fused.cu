@@ -97,76 +97,51 @@ __device__ __forceinline__ void run_step(unsigned char* __restrict__ shb, int T,
     const float2 fp = f2(f0.x + f1.x, f0.y + f1.y), fm = f2(f0.x - f1.x, f0.y - f1.y);
     const float2 f1a = f2(gKa * f1.x, gKa * f1.y);  // f1 (-1)^sKa
     const uint32_t tK = st.tK << 3, tKa = st.tKa << 3, tpiv = st.tpiv << 3;
-    // Orbits of one step are disjoint: UNR orbits are loaded before any of them is stored, so
-    // their shared-memory loads overlap (the compiler cannot prove that on its own).
-    constexpr int NIN = (KIND == DCS_KIND_SHRINK4) ? 4 : (KIND == DCS_KIND_GROW || KIND == DCS_KIND_DIAG ||
-                                                         KIND == DCS_KIND_FIXED) ? 1 : 2;
-    constexpr int UNR = NIN == 4 ? 1 : NIN == 2 ? 2 : 4;
     uint32_t tu = 0;  // spread(256 k) << 3, advanced by a masked increment over mhi << 3
-    for (int k0 = 0; k0 < niter; k0 += UNR) {
-        uint32_t t[UNR];
-        int sc[UNR];
-        float2 v[UNR][NIN];
-#pragma unroll
-        for (int u = 0; u < UNR; ++u) {
-            t[u] = tp | tu;
-            sc[u] = hs ^ (__popc(tu & tbeta3) & 1);
-            tu = ((tu | ~mhi3) + 1u) & mhi3;
-        }
-        // niter is a power of two, so either all UNR orbits exist or niter < UNR (only u = 0 then)
-        const int nu = niter < UNR ? niter : UNR;
-#pragma unroll
-        for (int u = 0; u < UNR; ++u) {
-            if (u < nu) {
-                v[u][0] = ldsh(shb, t[u]);
-                if constexpr (KIND == DCS_KIND_MIX) v[u][1] = ldsh(shb, t[u] ^ tKa);
-                if constexpr (NIN >= 2 && KIND != DCS_KIND_MIX) v[u][1] = ldsh(shb, t[u] ^ tK);
-                if constexpr (NIN == 4) {
-                    v[u][2] = ldsh(shb, t[u] ^ tKa);
-                    v[u][3] = ldsh(shb, t[u] ^ tKa ^ tK);
-                }
-            }
-        }
-#pragma unroll
-        for (int u = 0; u < UNR; ++u) {
-            if (u >= nu) break;
-            const uint32_t tt = t[u];
-            const int s_ = sc[u];
-            const float2 x = v[u][0];
-            if constexpr (KIND == DCS_KIND_GROW) {
-                stsh(shb, tt, fmul(f0, x));
-                stsh(shb, tt ^ tpiv, negif(fmul(f1, x), s_));
-            } else if constexpr (KIND == DCS_KIND_MIX) {
-                // o0 = f0 x + s_c f1 (-1)^sKa b ;  o1 = f0 b + s_c f1 x
-                const float2 b = v[u][1];
-                stsh(shb, tt, fmadd(f0, x, negif(fmul(f1a, b), s_)));
-                stsh(shb, tt ^ tKa, fmadd(f0, b, negif(fmul(f1, x), s_)));
-            } else if constexpr (KIND == DCS_KIND_DIAG) {
-                stsh(shb, tt, fmul(s_ ? fm : fp, x));
-            } else if constexpr (KIND == DCS_KIND_REPLACE) {
-                // o0 = f0 (x + b) ;  o1 = s_c f1 (x + (-1)^sK b)
-                const float2 b = v[u][1];
-                stsh(shb, tt, fmul(f0, f2(x.x + b.x, x.y + b.y)));
-                stsh(shb, tt ^ tK, negif(fmul(f1, f2(fmaf(gK, b.x, x.x), fmaf(gK, b.y, x.y))), s_));
-            } else if constexpr (KIND == DCS_KIND_FIXED) {
-                stsh(shb, tt, y ? negif(fmul(f1, x), s_) : fmul(f0, x));
-            } else if constexpr (KIND == DCS_KIND_FIXED_SHRINK) {
-                const float2 b = v[u][1];
-                stsh(shb, tt, y ? negif(fmul(f1, f2(fmaf(gK, b.x, x.x), fmaf(gK, b.y, x.y))), s_)
-                                : fmul(f0, f2(x.x + b.x, x.y + b.y)));
-            } else if constexpr (KIND == DCS_KIND_SHRINK4) {
-                // o0 = f0 (x + b) + s_d f1 (g + (-1)^sK h) ;  o1 = f0 (g + h) + s_c f1 (x + (-1)^sK b)
-                const float2 b = v[u][1], g = v[u][2], h = v[u][3];
-                const int sd = s_ ^ st.sKa;
-                stsh(shb, tt, fmadd(f0, f2(x.x + b.x, x.y + b.y),
-                                    negif(fmul(f1, f2(fmaf(gK, h.x, g.x), fmaf(gK, h.y, g.y))), sd)));
-                stsh(shb, tt ^ tKa, fmadd(f0, f2(g.x + h.x, g.y + h.y),
-                                          negif(fmul(f1, f2(fmaf(gK, b.x, x.x), fmaf(gK, b.y, x.y))), s_)));
-            } else {  // DCS_KIND_SHRINK2: f0 (x + b) + s_c f1 (x + (-1)^sK b)
-                const float2 b = v[u][1];
-                stsh(shb, tt, fmadd(f0, f2(x.x + b.x, x.y + b.y),
-                                    negif(fmul(f1, f2(fmaf(gK, b.x, x.x), fmaf(gK, b.y, x.y))), s_)));
-            }
+#pragma unroll 4
+    for (int k = 0; k < niter; ++k) {
+        const uint32_t t = tp | tu;
+        const int sc = hs ^ (__popc(tu & tbeta3) & 1);
+        tu = ((tu | ~mhi3) + 1u) & mhi3;
+        const float2 x = ldsh(shb, t);
+        if constexpr (KIND == DCS_KIND_GROW) {
+            stsh(shb, t, fmul(f0, x));
+            stsh(shb, t ^ tpiv, negif(fmul(f1, x), sc));
+        } else if constexpr (KIND == DCS_KIND_MIX) {
+            // o0 = f0 x + s_c f1 (-1)^sKa b ;  o1 = f0 b + s_c f1 x
+            const uint32_t td = t ^ tKa;
+            const float2 b = ldsh(shb, td);
+            stsh(shb, t, fmadd(f0, x, negif(fmul(f1a, b), sc)));
+            stsh(shb, td, fmadd(f0, b, negif(fmul(f1, x), sc)));
+        } else if constexpr (KIND == DCS_KIND_DIAG) {
+            stsh(shb, t, fmul(sc ? fm : fp, x));
+        } else if constexpr (KIND == DCS_KIND_REPLACE) {
+            // o0 = f0 (x + b) ;  o1 = s_c f1 (x + (-1)^sK b)
+            const uint32_t td = t ^ tK;
+            const float2 b = ldsh(shb, td);
+            stsh(shb, t, fmul(f0, f2(x.x + b.x, x.y + b.y)));
+            stsh(shb, td, negif(fmul(f1, f2(fmaf(gK, b.x, x.x), fmaf(gK, b.y, x.y))), sc));
+        } else if constexpr (KIND == DCS_KIND_FIXED) {
+            stsh(shb, t, y ? negif(fmul(f1, x), sc) : fmul(f0, x));
+        } else if constexpr (KIND == DCS_KIND_FIXED_SHRINK) {
+            const uint32_t td = t ^ tK;
+            const float2 b = ldsh(shb, td);
+            stsh(shb, t, y ? negif(fmul(f1, f2(fmaf(gK, b.x, x.x), fmaf(gK, b.y, x.y))), sc)
+                           : fmul(f0, f2(x.x + b.x, x.y + b.y)));
+        } else if constexpr (KIND == DCS_KIND_SHRINK4) {
+            // o0 = f0 (x + b) + s_d f1 (g + (-1)^sK h) ;  o1 = f0 (g + h) + s_c f1 (x + (-1)^sK b)
+            const uint32_t t1 = t ^ tK, td = t ^ tKa, td1 = td ^ tK;
+            const float2 b = ldsh(shb, t1), g = ldsh(shb, td), h = ldsh(shb, td1);
+            const int sd = sc ^ st.sKa;
+            stsh(shb, t, fmadd(f0, f2(x.x + b.x, x.y + b.y),
+                               negif(fmul(f1, f2(fmaf(gK, h.x, g.x), fmaf(gK, h.y, g.y))), sd)));
+            stsh(shb, td, fmadd(f0, f2(g.x + h.x, g.y + h.y),
+                                negif(fmul(f1, f2(fmaf(gK, b.x, x.x), fmaf(gK, b.y, x.y))), sc)));
+        } else {  // DCS_KIND_SHRINK2: f0 (x + b) + s_c f1 (x + (-1)^sK b)
+            const uint32_t td = t ^ tK;
+            const float2 b = ldsh(shb, td);
+            stsh(shb, t, fmadd(f0, f2(x.x + b.x, x.y + b.y),
+                               negif(fmul(f1, f2(fmaf(gK, b.x, x.x), fmaf(gK, b.y, x.y))), sc)));
         }
     }
 }
