@@ -28,6 +28,11 @@ struct FusedStep {
     uint8_t sK, sKa, nins, pad;
     uint8_t ins[16];
     uint32_t mhi;
+    // pairing with the next step (see dcs_tile_step)
+    uint8_t pair, pnins, swapB, swapA;
+    uint32_t pmhi, tau1, tau2;
+    uint8_t pins[16];
+    uint8_t s1e[4], s2e[4];
 };
 
 struct FusedArgs {
@@ -146,6 +151,147 @@ __device__ __forceinline__ void run_step(unsigned char* __restrict__ shb, int T,
     }
 }
 
+// ---------------------------------------------------------------- pairs of steps
+// Step weights for the pair bodies.
+struct StepW {
+    float2 f0, f1;
+    int y;
+};
+
+constexpr bool two_entry(int k) { return k != DCS_KIND_DIAG && k != DCS_KIND_FIXED; }
+
+// One step on a two-entry orbit (c, d) with signs s_c, s_d (reference formulas).
+template <int K>
+__device__ __forceinline__ void apply2(float2& xc, float2& xd, int sc, int sd, const StepW& w) {
+    const float2 f0 = w.f0, f1 = w.f1;
+    if constexpr (K == DCS_KIND_GROW) {
+        xd = negif(fmul(f1, xc), sc);
+        xc = fmul(f0, xc);
+    } else if constexpr (K == DCS_KIND_MIX) {
+        const float2 oc = fmadd(f0, xc, negif(fmul(f1, xd), sd));
+        xd = fmadd(f0, xd, negif(fmul(f1, xc), sc));
+        xc = oc;
+    } else if constexpr (K == DCS_KIND_REPLACE) {
+        const float2 u = negif(xc, sc), v = negif(xd, sd);
+        const float2 oc = fmul(f0, f2(xc.x + xd.x, xc.y + xd.y));
+        xd = fmul(f1, f2(u.x + v.x, u.y + v.y));
+        xc = oc;
+    } else if constexpr (K == DCS_KIND_FIXED_SHRINK) {
+        if (w.y) {
+            const float2 u = negif(xc, sc), v = negif(xd, sd);
+            xc = fmul(f1, f2(u.x + v.x, u.y + v.y));
+        } else {
+            xc = fmul(f0, f2(xc.x + xd.x, xc.y + xd.y));
+        }
+    } else {  // DCS_KIND_SHRINK2: f0 (x + b) + f1 (s_c x + s_d b)
+        const float2 u = negif(xc, sc), v = negif(xd, sd);
+        xc = fmadd(f1, f2(u.x + v.x, u.y + v.y), fmul(f0, f2(xc.x + xd.x, xc.y + xd.y)));
+    }
+}
+
+// One step on a one-entry orbit with sign s.
+template <int K>
+__device__ __forceinline__ void apply1(float2& x, int s, const StepW& w) {
+    if constexpr (K == DCS_KIND_DIAG) {
+        x = fmadd(w.f0, x, negif(fmul(w.f1, x), s));
+    } else {  // DCS_KIND_FIXED
+        x = w.y ? negif(fmul(w.f1, x), s) : fmul(w.f0, x);
+    }
+}
+
+// Two consecutive steps per shared-memory round trip.  Super-orbit entries:
+// e0 = t, e1 = t ^ tau1, e2 = t ^ tau2, e3 = t ^ tau1 ^ tau2 (e1/e3 absent when step 1 has
+// one-entry orbits, e2/e3 when step 2 has).  t is zero at both steps' role coordinates, so e0
+// is entry c of both steps; step 1 acts on (e0, e1) and (e2, e3), step 2 on (e0, e2) and (e1, e3),
+// with the second pair's roles swapped when the other step's vector has the role bit set.
+template <int K1, int K2>
+__device__ __forceinline__ void run_pair(unsigned char* __restrict__ shb, int T, const FusedStep& a, const StepW& wa,
+                                         int csa, bool doa, const FusedStep& b, const StepW& wb, int csb, bool dob) {
+    constexpr bool A2 = two_entry(K1), B2 = two_entry(K2);
+    const int nrep = T >> a.pnins;
+    if ((int)threadIdx.x >= nrep) return;
+    const uint32_t ta3 = a.tbeta << 3, tb3 = b.tbeta << 3;
+    const uint32_t tp = spread(threadIdx.x, a.pins, a.pnins) << 3;
+    const int hsa = (__popc(tp & ta3) & 1) ^ csa, hsb = (__popc(tp & tb3) & 1) ^ csb;
+    const uint32_t mhi3 = a.pmhi << 3, tau1 = a.tau1 << 3, tau2 = a.tau2 << 3;
+    const int niter = nrep > kThreads ? nrep >> kThreadLog : 1;
+    const int a1 = a.s1e[1], a2 = a.s1e[2], a3 = a.s1e[3], b1 = a.s2e[1], b2 = a.s2e[2], b3 = a.s2e[3];
+    const bool swB = a.swapB, swA = a.swapA;
+    uint32_t tu = 0;
+#pragma unroll 2
+    for (int k = 0; k < niter; ++k) {
+        const uint32_t t0 = tp | tu;
+        const int sa = hsa ^ (__popc(tu & ta3) & 1), sb = hsb ^ (__popc(tu & tb3) & 1);
+        tu = ((tu | ~mhi3) + 1u) & mhi3;
+        const uint32_t t1 = t0 ^ tau1, t2 = t0 ^ tau2, t3 = t1 ^ tau2;
+        float2 e0 = ldsh(shb, t0), e1, e2, e3;
+        if constexpr (A2) e1 = ldsh(shb, t1);
+        if constexpr (B2) e2 = ldsh(shb, t2);
+        if constexpr (A2 && B2) e3 = ldsh(shb, t3);
+        if (doa) {
+            if constexpr (A2) {
+                apply2<K1>(e0, e1, sa, sa ^ a1, wa);
+                if constexpr (B2) {
+                    if (swB) apply2<K1>(e3, e2, sa ^ a3, sa ^ a2, wa);
+                    else apply2<K1>(e2, e3, sa ^ a2, sa ^ a3, wa);
+                }
+            } else {
+                apply1<K1>(e0, sa, wa);
+                if constexpr (B2) apply1<K1>(e2, sa ^ a2, wa);
+            }
+        }
+        if (dob) {
+            if constexpr (B2) {
+                apply2<K2>(e0, e2, sb, sb ^ b2, wb);
+                if constexpr (A2) {
+                    if (swA) apply2<K2>(e3, e1, sb ^ b3, sb ^ b1, wb);
+                    else apply2<K2>(e1, e3, sb ^ b1, sb ^ b3, wb);
+                }
+            } else {
+                apply1<K2>(e0, sb, wb);
+                if constexpr (A2) apply1<K2>(e1, sb ^ b1, wb);
+            }
+        }
+        stsh(shb, t0, e0);
+        if constexpr (A2) stsh(shb, t1, e1);
+        if constexpr (B2) stsh(shb, t2, e2);
+        if constexpr (A2 && B2) stsh(shb, t3, e3);
+    }
+}
+
+template <int K1>
+__device__ __forceinline__ void dispatch_pair2(int k2, unsigned char* shb, int T, const FusedStep& a,
+                                               const StepW& wa, int csa, bool doa, const FusedStep& b,
+                                               const StepW& wb, int csb, bool dob) {
+    switch (k2) {
+        case DCS_KIND_GROW: run_pair<K1, DCS_KIND_GROW>(shb, T, a, wa, csa, doa, b, wb, csb, dob); break;
+        case DCS_KIND_MIX: run_pair<K1, DCS_KIND_MIX>(shb, T, a, wa, csa, doa, b, wb, csb, dob); break;
+        case DCS_KIND_DIAG: run_pair<K1, DCS_KIND_DIAG>(shb, T, a, wa, csa, doa, b, wb, csb, dob); break;
+        case DCS_KIND_REPLACE: run_pair<K1, DCS_KIND_REPLACE>(shb, T, a, wa, csa, doa, b, wb, csb, dob); break;
+        case DCS_KIND_FIXED: run_pair<K1, DCS_KIND_FIXED>(shb, T, a, wa, csa, doa, b, wb, csb, dob); break;
+        case DCS_KIND_FIXED_SHRINK:
+            run_pair<K1, DCS_KIND_FIXED_SHRINK>(shb, T, a, wa, csa, doa, b, wb, csb, dob);
+            break;
+        default: run_pair<K1, DCS_KIND_SHRINK2>(shb, T, a, wa, csa, doa, b, wb, csb, dob); break;
+    }
+}
+
+__device__ __forceinline__ void dispatch_pair(int k1, int k2, unsigned char* shb, int T, const FusedStep& a,
+                                              const StepW& wa, int csa, bool doa, const FusedStep& b,
+                                              const StepW& wb, int csb, bool dob) {
+    switch (k1) {
+        case DCS_KIND_GROW: dispatch_pair2<DCS_KIND_GROW>(k2, shb, T, a, wa, csa, doa, b, wb, csb, dob); break;
+        case DCS_KIND_MIX: dispatch_pair2<DCS_KIND_MIX>(k2, shb, T, a, wa, csa, doa, b, wb, csb, dob); break;
+        case DCS_KIND_DIAG: dispatch_pair2<DCS_KIND_DIAG>(k2, shb, T, a, wa, csa, doa, b, wb, csb, dob); break;
+        case DCS_KIND_REPLACE: dispatch_pair2<DCS_KIND_REPLACE>(k2, shb, T, a, wa, csa, doa, b, wb, csb, dob); break;
+        case DCS_KIND_FIXED: dispatch_pair2<DCS_KIND_FIXED>(k2, shb, T, a, wa, csa, doa, b, wb, csb, dob); break;
+        case DCS_KIND_FIXED_SHRINK:
+            dispatch_pair2<DCS_KIND_FIXED_SHRINK>(k2, shb, T, a, wa, csa, doa, b, wb, csb, dob);
+            break;
+        default: dispatch_pair2<DCS_KIND_SHRINK2>(k2, shb, T, a, wa, csa, doa, b, wb, csb, dob); break;
+    }
+}
+
 template <int MINB>
 __global__ void __launch_bounds__(kThreads, MINB)
 k_fused(float2* __restrict__ E, const __grid_constant__ FusedArgs A, const dcs_param* __restrict__ params,
@@ -212,13 +358,24 @@ k_fused(float2* __restrict__ E, const __grid_constant__ FusedArgs A, const dcs_p
         }
         asm volatile("cp.async.wait_all;\n" ::: "memory");
         __syncthreads();
-        for (int s = 0; s < A.count; ++s) {
+        for (int s = 0; s < A.count;) {
             const FusedStep& st = A.st[s];
             const float4 w = fw[s];
             const float2 f0 = f2(w.x, w.y), f1 = f2(w.z, w.w);
             const int y = ovy[s] >> 1;
             // tile-constant part of the sign: parity(base & beta) ^ ov
             const int cs = (__popcll(base & st.beta) & 1) ^ (ovy[s] & 1);
+            if (st.pair && s + 1 < A.count) {
+                const FusedStep& st2 = A.st[s + 1];
+                const float4 w2 = fw[s + 1];
+                const StepW wa{f0, f1, y}, wb{f2(w2.x, w2.y), f2(w2.z, w2.w), ovy[s + 1] >> 1};
+                const int cs2 = (__popcll(base & st2.beta) & 1) ^ (ovy[s + 1] & 1);
+                dispatch_pair(st.kind, st2.kind, smem, T, st, wa, cs, !(base & st.cskip), st2, wb, cs2,
+                              !(base & st2.cskip));
+                __syncthreads();
+                s += 2;
+                continue;
+            }
             if (!(base & st.cskip)) switch (st.kind) {
                 case DCS_KIND_GROW: run_step<DCS_KIND_GROW>(smem, T, st, f0, f1, cs, y); break;
                 case DCS_KIND_MIX: run_step<DCS_KIND_MIX>(smem, T, st, f0, f1, cs, y); break;
@@ -230,6 +387,7 @@ k_fused(float2* __restrict__ E, const __grid_constant__ FusedArgs A, const dcs_p
                 default: run_step<DCS_KIND_SHRINK2>(smem, T, st, f0, f1, cs, y); break;
             }
             __syncthreads();
+            ++s;
         }
         // store (only entries active after the group) and max; pairs when slot 0 is active after
         if (A.pair_out) {
@@ -305,12 +463,24 @@ extern "C" int dcs_fused_groups(void* table, const dcs_step* steps, int nsteps, 
             f.cskip = ts.cskip;
             f.tK = ts.tK; f.tKa = ts.tKa; f.tpiv = ts.tpiv; f.tbeta = ts.tbeta;
             f.sK = ts.sK; f.sKa = ts.sKa; f.nins = ts.nins; f.mhi = ts.mhi;
+            f.pair = ts.pair && s + 1 < g.count && d.kind != DCS_KIND_SHRINK4 &&
+                     steps[g.first + s + 1].kind != DCS_KIND_SHRINK4;
+            f.pnins = ts.pnins; f.swapB = ts.swapB; f.swapA = ts.swapA;
+            f.pmhi = ts.pmhi; f.tau1 = ts.tau1; f.tau2 = ts.tau2;
+            for (int i = 0; i < 4; ++i) { f.s1e[i] = ts.s1e[i]; f.s2e[i] = ts.s2e[i]; }
             f.kind = d.kind;
             f.pidx = g.first + s;
             bool bad = f.nins > 16 || f.nins > g.tile_dim || (f.tK | f.tKa | f.tpiv | f.tbeta) >> g.tile_dim;
             for (int i = 0; i < f.nins && !bad; ++i) {
                 f.ins[i] = ts.ins[i];
                 bad = ts.ins[i] >= g.tile_dim || (i && ts.ins[i] <= ts.ins[i - 1]);
+            }
+            if (f.pair) {
+                bad = bad || f.pnins > 16 || f.pnins > g.tile_dim || (f.tau1 | f.tau2) >> g.tile_dim;
+                for (int i = 0; i < f.pnins && !bad; ++i) {
+                    f.pins[i] = ts.pins[i];
+                    bad = ts.pins[i] >= g.tile_dim || (i && ts.pins[i] <= ts.pins[i - 1]);
+                }
             }
             if (bad) {
                 dcs_host::set_error("dcs_fused_groups: malformed tile step %d", g.first + s);

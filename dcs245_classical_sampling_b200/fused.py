@@ -120,7 +120,81 @@ def group_steps(steps, max_dim=13, low=4, max_steps=MAX_GROUP_STEPS, max_extra=1
     return spans
 
 
-def build_fused_plan(plan, max_dim=13, low=4, max_steps=MAX_GROUP_STEPS, max_extra=1, spans=None, variant=0):
+PAIR_KINDS = (0, 1, 2, 3, 4, 5, 7)  # every kind but the four-entry shrink
+
+
+def _tau(kind, ts):
+    """Tile-coordinate orbit vector of a step (0 for one-entry kinds)."""
+    if kind == KIND_GROW:
+        return int(ts["tpiv"])
+    if kind == 1:
+        return int(ts["tKa"])
+    if kind in (3, 5, 7):
+        return int(ts["tK"])
+    return 0
+
+
+def _role_slot(st, kind):
+    if kind == KIND_GROW:
+        return st.pivot
+    if kind == 1:
+        return st.pivot_a
+    if kind in (3, 5, 7):
+        return st.pivot
+    return None
+
+
+def _pair_steps(steps, first, count, tsteps, dim, tilepos_of, tbit, U):
+    """Mark pairs of consecutive steps that can share one shared-memory round trip."""
+    par = lambda v: bin(v).count("1") & 1
+    s = first
+    while s + 1 < first + count:
+        a, b = steps[s], steps[s + 1]
+        ka, kb = orbit_kind(a)[0], orbit_kind(b)[0]
+        ta, tb = tsteps[s], tsteps[s + 1]
+        tau1, tau2 = _tau(ka, ta), _tau(kb, tb)
+        ra, rb = _role_slot(a, ka), _role_slot(b, kb)
+        ok = ka in PAIR_KINDS and kb in PAIR_KINDS and not (tau1 and tau2 and (tau1 == tau2))
+        ok = ok and not (ra is not None and rb is not None and ra == rb)
+        if not ok:
+            s += 1
+            continue
+        # zero bits: both role slots, and slots inactive at both steps (inactive at the first
+        # step and not grown by it stay inactive at the second)
+        ins = set()
+        if ra is not None:
+            ins.add(tbit(ra))
+        if rb is not None:
+            ins.add(tbit(rb))
+        ina, inb = slot_mask(a.active_in), slot_mask(b.active_in)
+        for q in range(64):
+            if (U >> q) & 1 and not (ina >> q) & 1 and not (inb >> q) & 1 and q != ra and q != rb and tilepos_of(q):
+                ins.add(tbit(q))
+        ins = sorted(ins)
+        if len(ins) > 16 or len(ins) > dim:
+            s += 1
+            continue
+        t1, t2 = int(ta["tbeta"]), int(tb["tbeta"])
+        offs = [0, tau1, tau2, tau1 ^ tau2]
+        ta["pair"] = 1
+        ta["pnins"] = len(ins)
+        for i, bit in enumerate(ins):
+            ta["pins"][i] = bit
+        free = [bb for bb in range(dim) if bb not in ins]
+        ta["pmhi"] = sum(1 << bb for bb in free[8:])
+        ta["tau1"], ta["tau2"] = tau1, tau2
+        # roles: entry t has zero at both role coordinates; in (t^tau2, t^tau1^tau2) step 1's entry c
+        # is the one whose role coordinate is zero, i.e. the second one when tau2 has that bit
+        ta["swapB"] = (tau2 >> tbit(ra)) & 1 if ra is not None else 0
+        ta["swapA"] = (tau1 >> tbit(rb)) & 1 if rb is not None else 0
+        for j, o in enumerate(offs):
+            ta["s1e"][j] = par(o & t1)
+            ta["s2e"][j] = par(o & t2)
+        s += 2
+
+
+def build_fused_plan(plan, max_dim=13, low=4, max_steps=MAX_GROUP_STEPS, max_extra=1, spans=None, variant=0,
+                     pairs=True):
     steps = plan.steps
     if spans is None:
         spans = group_steps(steps, max_dim, low, max_steps, max_extra)
@@ -250,6 +324,9 @@ def build_fused_plan(plan, max_dim=13, low=4, max_steps=MAX_GROUP_STEPS, max_ext
             ts["mhi"] = sum(1 << b for b in free[8:])  # 256 threads: index bits >= 8
             ts["rb1"] = max(st.pivot_a if kind == 1 else st.pivot, 0)  # role slot(s), for checking
             ts["rb2"] = max(st.pivot_a, 0) if kind == 6 else 0
+        if pairs:
+            _pair_steps(steps, first, count, tsteps, dim, tilepos_of=lambda q: (q < l or q in pivots),
+                        tbit=tbit, U=U)
         fp.universe.append(bin(U).count("1"))
         fp.tiles.append(1 << bin(cmask).count("1"))
         fp.dims.append(dim)

@@ -134,7 +134,17 @@ typedef struct dcs_tile_step {
     uint8_t pad[3];
     uint8_t ins[16];        /* inserted tile bits, ascending */
     uint32_t mhi;           /* tile bits receiving representative-index bits 8 and up (256 threads) */
-    uint32_t pad2;
+    /* pairing with the next step (one shared-memory round trip for both): super-orbit
+     * {t, t^tau1, t^tau2, t^tau1^tau2} with t zero at pins[]; step 1 acts along tau1, step 2 along
+     * tau2; swapB / swapA: the entry with zero role slot in pair (t^tau2, t^tau1^tau2) for step 1 /
+     * (t^tau1, t^tau1^tau2) for step 2 is the second one; s1e / s2e: sign parity of the offsets
+     * (0, tau1, tau2, tau1^tau2) under step 1's / step 2's tile functional. */
+    uint8_t pair;           /* 1: this step and the next run as a pair */
+    uint8_t pnins, swapB, swapA;
+    uint32_t pmhi;
+    uint32_t tau1, tau2;
+    uint8_t pins[16];
+    uint8_t s1e[4], s2e[4];
 } dcs_tile_step;
 
 /* Result of one draw (device-side struct; the host copies it back). */

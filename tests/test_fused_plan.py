@@ -54,10 +54,15 @@ def emulate(bp, fp, params):
         A = bases[:, None] ^ taddr[None, :]
         inm = P.slot_mask(steps[first].active_in)
         sh = np.where((A & np.uint64(~inm & (2**64 - 1))) == 0, E[A.astype(np.int64)] * sc, 0)
-        for s in range(first, first + count):
+        s = first
+        while s < first + count:
             st = steps[s]
             kind, _ = P.orbit_kind(st)
             ts = fp.tile_steps[s]
+            if int(ts["pair"]) and s + 1 < first + count:
+                sh = _emulate_pair(bp, fp, params, s, bases, A, sh, dim, low)
+                s += 2
+                continue
             pr = params[s]
             f0, f1 = complex(pr["f0r"], pr["f0i"]), complex(pr["f1r"], pr["f1i"])
             ov, y = int(pr["ov"]), int(pr["y"])
@@ -116,12 +121,124 @@ def emulate(bp, fp, params):
             else:
                 td = tj ^ tK; b = sh[ti, td].copy()
                 sh[ti, tj] = (f0 + f1 * sgn(sc)) * x + (f0 + f1 * sgn(sc ^ sK)) * b
+            s += 1
         outm = P.slot_mask(steps[first + count - 1].active_out)
         keep = (A & np.uint64(~outm & (2**64 - 1))) == 0
         E[A[keep].astype(np.int64)] = sh[keep]
         m2 = float(np.max(np.abs(sh[keep]) ** 2)) if keep.any() else 0.0
     term = _deposit(np.arange(1 << len(bp.terminal_slots), dtype=np.uint64), P.slot_mask(bp.terminal_slots))
     return E[term.astype(np.int64)], ls
+
+
+def _par_arr(v, mask):
+    y = v & np.uint64(mask)
+    par = np.zeros_like(y)
+    while np.any(y):
+        par ^= y & np.uint64(1)
+        y >>= np.uint64(1)
+    return par.astype(np.int64)
+
+
+def _apply2(kind, xc, xd, sc, sd, f0, f1, y):
+    sg = lambda b: np.where(b, -1.0, 1.0)
+    if kind == P.KIND_GROW:
+        return f0 * xc, f1 * xc * sg(sc)
+    if kind == P.KIND_MIX:
+        return f0 * xc + f1 * sg(sd) * xd, f0 * xd + f1 * sg(sc) * xc
+    if kind == P.KIND_REPLACE:
+        return f0 * (xc + xd), f1 * (sg(sc) * xc + sg(sd) * xd)
+    if kind == P.KIND_FIXED_SHRINK:
+        return (f1 * (sg(sc) * xc + sg(sd) * xd) if y else f0 * (xc + xd)), xd
+    return (f0 + f1 * sg(sc)) * xc + (f0 + f1 * sg(sd)) * xd, xd  # shrink2
+
+
+def _apply1(kind, x, s, f0, f1, y):
+    sg = np.where(s, -1.0, 1.0)
+    if kind == P.KIND_DIAG:
+        return (f0 + f1 * sg) * x
+    return f1 * sg * x if y else f0 * x
+
+
+def _emulate_pair(bp, fp, params, s, bases, A, sh, dim, low):
+    """Mirror of csrc/fused.cu run_pair: two steps per round trip over super-orbits."""
+    a, b = bp.steps[s], bp.steps[s + 1]
+    ka, kb = P.orbit_kind(a)[0], P.orbit_kind(b)[0]
+    ta = fp.tile_steps[s]
+    pa, pb = params[s], params[s + 1]
+    fa0, fa1 = complex(pa["f0r"], pa["f0i"]), complex(pa["f1r"], pa["f1i"])
+    fb0, fb1 = complex(pb["f0r"], pb["f0i"]), complex(pb["f1r"], pb["f1i"])
+    two = lambda k: k not in (P.KIND_DIAG, P.KIND_FIXED)
+    A2, B2 = two(ka), two(kb)
+    nins = int(ta["pnins"])
+    o = np.arange((1 << dim) >> nins, dtype=np.int64)
+    for rho in [int(v) for v in ta["pins"][:nins]]:
+        o = ((o >> rho) << (rho + 1)) | (o & ((1 << rho) - 1))
+    tau1, tau2 = int(ta["tau1"]), int(ta["tau2"])
+    R = np.arange(len(bases))[:, None]
+    t0 = np.broadcast_to(o, (len(bases), len(o)))
+    t1, t2 = t0 ^ tau1, t0 ^ tau2
+    t3 = t1 ^ tau2
+    a0 = A[R, t0]
+    # invariants: e0 is entry c of both steps
+    for st, kk in ((a, ka), (b, kb)):
+        role = {P.KIND_GROW: st.pivot, P.KIND_MIX: st.pivot_a}.get(kk, st.pivot if kk in (3, 5, 7) else None)
+        if role is not None:
+            assert not ((a0 >> np.uint64(role)) & np.uint64(1)).any()
+    cs_a = np.array([bin(int(bb) & a.beta).count("1") & 1 for bb in bases], np.int64)[:, None] ^ int(pa["ov"])
+    cs_b = np.array([bin(int(bb) & b.beta).count("1") & 1 for bb in bases], np.int64)[:, None] ^ int(pb["ov"])
+    tba, tbb = int(fp.tile_steps[s]["tbeta"]), int(fp.tile_steps[s + 1]["tbeta"])
+    sa = _par_arr(t0.astype(np.uint64), tba) ^ cs_a
+    sb = _par_arr(t0.astype(np.uint64), tbb) ^ cs_b
+    s1e = [int(v) for v in ta["s1e"]]
+    s2e = [int(v) for v in ta["s2e"]]
+    # partner signs against the physical parity
+    for tt, j in ((t1, 1), (t2, 2), (t3, 3)):
+        aa = A[R, tt]
+        np.testing.assert_array_equal(sa ^ s1e[j], _neg(aa.reshape(-1), a.beta, int(pa["ov"])).reshape(aa.shape))
+        np.testing.assert_array_equal(sb ^ s2e[j], _neg(aa.reshape(-1), b.beta, int(pb["ov"])).reshape(aa.shape))
+    live_a = ((bases & np.uint64(int(ta["cskip"]))) == 0)[:, None]
+    live_b = ((bases & np.uint64(int(fp.tile_steps[s + 1]["cskip"]))) == 0)[:, None]
+    e0 = sh[R, t0].copy()
+    e1 = sh[R, t1].copy() if A2 else None
+    e2 = sh[R, t2].copy() if B2 else None
+    e3 = sh[R, t3].copy() if (A2 and B2) else None
+    def sel(live, new, old):
+        return np.where(live, new, old)
+    if A2:
+        n0, n1 = _apply2(ka, e0, e1, sa, sa ^ s1e[1], fa0, fa1, int(pa["y"]))
+        e0, e1 = sel(live_a, n0, e0), sel(live_a, n1, e1)
+        if B2:
+            if int(ta["swapB"]):
+                n3, n2 = _apply2(ka, e3, e2, sa ^ s1e[3], sa ^ s1e[2], fa0, fa1, int(pa["y"]))
+            else:
+                n2, n3 = _apply2(ka, e2, e3, sa ^ s1e[2], sa ^ s1e[3], fa0, fa1, int(pa["y"]))
+            e2, e3 = sel(live_a, n2, e2), sel(live_a, n3, e3)
+    else:
+        e0 = sel(live_a, _apply1(ka, e0, sa, fa0, fa1, int(pa["y"])), e0)
+        if B2:
+            e2 = sel(live_a, _apply1(ka, e2, sa ^ s1e[2], fa0, fa1, int(pa["y"])), e2)
+    if B2:
+        n0, n2 = _apply2(kb, e0, e2, sb, sb ^ s2e[2], fb0, fb1, int(pb["y"]))
+        e0, e2 = sel(live_b, n0, e0), sel(live_b, n2, e2)
+        if A2:
+            if int(ta["swapA"]):
+                n3, n1 = _apply2(kb, e3, e1, sb ^ s2e[3], sb ^ s2e[1], fb0, fb1, int(pb["y"]))
+            else:
+                n1, n3 = _apply2(kb, e1, e3, sb ^ s2e[1], sb ^ s2e[3], fb0, fb1, int(pb["y"]))
+            e1, e3 = sel(live_b, n1, e1), sel(live_b, n3, e3)
+    else:
+        e0 = sel(live_b, _apply1(kb, e0, sb, fb0, fb1, int(pb["y"])), e0)
+        if A2:
+            e1 = sel(live_b, _apply1(kb, e1, sb ^ s2e[1], fb0, fb1, int(pb["y"])), e1)
+    sh = sh.copy()
+    sh[R, t0] = e0
+    if A2:
+        sh[R, t1] = e1
+    if B2:
+        sh[R, t2] = e2
+    if A2 and B2:
+        sh[R, t3] = e3
+    return sh
 
 
 @pytest.mark.parametrize("name,dims", [("c1", [(13, 4), (6, 2), (4, 0)]), ("small", [(13, 4), (8, 3), (6, 2)]),
@@ -144,6 +261,7 @@ def test_fused_emulation_matches_oracle(golden, name, dims):
         for max_dim, low in dims:
             fp = build_fused_plan(bp, max_dim=max_dim, low=low)
             assert sum(c for _, c in fp.spans) == len(bp.steps)
+            assert int(fp.tile_steps["pair"].sum()) > 0
             got, gls = emulate(bp, fp, params)
             if not np.any(want):
                 assert not np.any(got)  # the slice's table vanished: the reference skips it
