@@ -35,7 +35,8 @@ TILE_STEP_DTYPE = np.dtype([("cskip", "<u8"), ("tK", "<u4"), ("tKa", "<u4"), ("t
                             ("sK", "<u1"), ("sKa", "<u1"), ("nins", "<u1"), ("rb1", "<u1"), ("rb2", "<u1"),
                             ("pad", "<u1", (3,)), ("ins", "<u1", (16,)), ("mhi", "<u4"), ("pair", "<u1"),
                             ("pnins", "<u1"), ("swapB", "<u1"), ("swapA", "<u1"), ("pmhi", "<u4"), ("tau1", "<u4"),
-                            ("tau2", "<u4"), ("pins", "<u1", (16,)), ("s1e", "<u1", (4,)), ("s2e", "<u1", (4,))])
+                            ("tau2", "<u4"), ("pins", "<u1", (16,)), ("s1e", "<u1", (4,)), ("s2e", "<u1", (4,)),
+                            ("pad3", "<u4")])
 DRAW_DTYPE = np.dtype([
     ("index", "<i8"), ("tie", "<i4"), ("status", "<i4"), ("total_cdf", "<f8"), ("total_exact", "<f8"),
     ("selected_weight", "<f8"), ("cdf_lower", "<f8"), ("cdf_upper", "<f8"), ("cdf_lower_exact", "<f8"),

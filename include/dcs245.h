@@ -145,6 +145,7 @@ typedef struct dcs_tile_step {
     uint32_t tau1, tau2;
     uint8_t pins[16];
     uint8_t s1e[4], s2e[4];
+    uint32_t pad3;          /* explicit tail padding (8-byte alignment) */
 } dcs_tile_step;
 
 /* Result of one draw (device-side struct; the host copies it back). */
