@@ -16,8 +16,9 @@ import numpy as np
 from . import _lib
 
 CACHE = Path(__file__).resolve().parent / "autotune_cache.json"
-CANDIDATES = [(13, 4, 24, 0), (13, 4, 24, 1), (12, 4, 24, 0), (12, 4, 24, 1), (13, 3, 24, 0), (13, 5, 24, 0),
-              (13, 4, 12, 0), (14, 4, 24, 1)]
+# (max tile dim, contiguous low bits, max steps per group, kernel variant, step pairs)
+CANDIDATES = [(13, 4, 24, 0, False), (13, 4, 24, 1, False), (12, 4, 24, 0, False), (13, 3, 24, 0, False),
+              (13, 3, 24, 0, True), (13, 5, 24, 0, False), (13, 4, 12, 0, False), (14, 4, 24, 1, False)]
 
 
 def fingerprint(plan):
@@ -51,9 +52,10 @@ def tune(engine, params_dev, candidates=CANDIDATES, repeats=1, save=True):
     report = []
     best = None
     for cand in candidates:
-        max_dim, low, max_steps, variant = cand
+        max_dim, low, max_steps, variant, pairs = cand
         try:
-            fp = build_fused_plan(engine.plan, max_dim=max_dim, low=low, max_steps=max_steps, variant=variant)
+            fp = build_fused_plan(engine.plan, max_dim=max_dim, low=low, max_steps=max_steps, variant=variant,
+                                  pairs=pairs)
         except ValueError:
             continue
         need = len(fp.groups) + 1
@@ -78,7 +80,7 @@ def tune(engine, params_dev, candidates=CANDIDATES, repeats=1, save=True):
             times.append(a.elapsed_time(b) / 1000.0)
         t = min(times[1:]) if len(times) > 1 else times[0]
         report.append({"max_dim": max_dim, "low": low, "max_steps": max_steps, "variant": variant,
-                       "groups": len(fp.groups), "seconds": t})
+                       "pairs": pairs, "groups": len(fp.groups), "seconds": t})
         if best is None or t < best[0]:
             best = (t, cand, fp)
     engine.fplan = best[2]
@@ -88,10 +90,10 @@ def tune(engine, params_dev, candidates=CANDIDATES, repeats=1, save=True):
         data = _load()
         data[f"{fingerprint(engine.plan)}|{torch.cuda.get_device_name(engine.device)}"] = {
             "max_dim": best[1][0], "low": best[1][1], "max_steps": best[1][2], "variant": best[1][3],
-            "seconds": best[0]}
+            "pairs": best[1][4], "seconds": best[0]}
         try:
             CACHE.write_text(json.dumps(data, indent=1) + "\n")
         except OSError:
             pass
     return {"best": {"max_dim": best[1][0], "low": best[1][1], "max_steps": best[1][2], "variant": best[1][3],
-                     "seconds": best[0]}, "candidates": report}
+                     "pairs": best[1][4], "seconds": best[0]}, "candidates": report}

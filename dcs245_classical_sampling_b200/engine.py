@@ -220,7 +220,8 @@ class InplaceConditionalBlockGPU:
             from .fused import build_fused_plan
             cfg = cached(plan, torch.cuda.get_device_name(self.device)) or {}
             self.fused_config = {"max_dim": cfg.get("max_dim", 13), "low": cfg.get("low", 4),
-                                 "max_steps": cfg.get("max_steps", 24), "variant": cfg.get("variant", 0)}
+                                 "max_steps": cfg.get("max_steps", 24), "variant": cfg.get("variant", 0),
+                                 "pairs": cfg.get("pairs", False)}
             self.fplan = build_fused_plan(plan, **self.fused_config)
             self.items = 1
         self.table = torch.empty(self.items * table_entries, dtype=tdtype, device=self.device)
@@ -253,6 +254,15 @@ class InplaceConditionalBlockGPU:
     def _nmax(self):
         return len(self.fplan.groups) if self.mode == "fused" else self.nsteps
 
+    def set_fused_config(self, **cfg):
+        """Rebuild the fused plan with another tile shape (max_dim, low, max_steps, variant, pairs)."""
+        from .fused import build_fused_plan
+        if self.mode != "fused":
+            raise ValueError("set_fused_config needs mode='fused'")
+        self.fused_config = {**self.fused_config, **cfg}
+        self.fplan = build_fused_plan(self.plan, **self.fused_config)
+        self.maxbits = torch.zeros(self.items * (len(self.fplan.groups) + 1), dtype=torch.int64, device=self.device)
+
     def autotune(self, x_bits=None, candidates=None):
         """Time the fused tile-shape candidates on this engine's table and keep the fastest."""
         from . import autotune as at
@@ -262,7 +272,7 @@ class InplaceConditionalBlockGPU:
         _, items = self.params.items(x)
         prm = torch.from_numpy(items[0][1].view(np.int64).copy()).to(self.device)
         rep = at.tune(self, prm, **({"candidates": candidates} if candidates else {}))
-        self.fused_config = {k: rep["best"][k] for k in ("max_dim", "low", "max_steps", "variant")}
+        self.fused_config = {k: rep["best"][k] for k in ("max_dim", "low", "max_steps", "variant", "pairs")}
         self.scale = torch.zeros(self.items * _lib.SCALE_DTYPE.itemsize // 8, dtype=torch.int64,
                                  device=self.device)
         return rep

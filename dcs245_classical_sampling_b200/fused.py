@@ -194,7 +194,7 @@ def _pair_steps(steps, first, count, tsteps, dim, tilepos_of, tbit, U):
 
 
 def build_fused_plan(plan, max_dim=13, low=4, max_steps=MAX_GROUP_STEPS, max_extra=1, spans=None, variant=0,
-                     pairs=True):
+                     pairs=False):
     steps = plan.steps
     if spans is None:
         spans = group_steps(steps, max_dim, low, max_steps, max_extra)

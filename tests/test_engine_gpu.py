@@ -51,6 +51,18 @@ def test_complex64_block_matches_reference(golden, name, mode):
         assert meta["prefix_dtype"] == "complex64"
 
 
+@pytest.mark.parametrize("name", CASES)
+def test_fused_step_pairs_match_reference(golden, name):
+    """The fused kernel with two steps per shared-memory round trip (autotuner option)."""
+    case, arrays = golden(name)
+    eng = _engine(case, arrays, np.complex64, mode="fused")
+    eng.set_fused_config(pairs=True)
+    assert int(eng.fplan.tile_steps["pair"].sum()) > 0
+    for rec in case["protocol"]["records"]:
+        v, _ = eng.block(_x(rec))
+        assert rel_l2(v.cpu().numpy(), arrays[f"block_{rec['sample_id']}"]) < 1e-5
+
+
 def test_one_item_at_a_time_equals_batched_slices(golden):
     case, arrays = golden("small")
     a = _engine(case, arrays, np.complex128, items=1)

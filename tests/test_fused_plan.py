@@ -258,10 +258,10 @@ def test_fused_emulation_matches_oracle(golden, name, dims):
         want, wls, off = block_ref.execute(oe.steps, f, yfix, oe.fut, oe.maxslots)
         freeflip = sum(int(flips[q]) << j for j, q in enumerate(oe.open_red))
         assert xor == (off >> oe.stop) ^ freeflip
-        for max_dim, low in dims:
-            fp = build_fused_plan(bp, max_dim=max_dim, low=low)
+        for (max_dim, low), pairs in [(d, pr) for d in dims for pr in (False, True)]:
+            fp = build_fused_plan(bp, max_dim=max_dim, low=low, pairs=pairs)
             assert sum(c for _, c in fp.spans) == len(bp.steps)
-            assert int(fp.tile_steps["pair"].sum()) > 0
+            assert (int(fp.tile_steps["pair"].sum()) > 0) == pairs
             got, gls = emulate(bp, fp, params)
             if not np.any(want):
                 assert not np.any(got)  # the slice's table vanished: the reference skips it
