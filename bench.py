@@ -447,10 +447,8 @@ def kernel_roofline(eng, prep, out, stream):
             a = torch.cuda.Event(enable_timing=True)
             b = torch.cuda.Event(enable_timing=True)
             a.record(stream)
-            _lib.check(lib.dcs_fused_groups(_lib.ptr(eng.table), f.dsteps.ctypes.data, len(f.dsteps),
-                                            f.groups.ctypes.data, len(f.groups), f.tile_steps.ctypes.data,
-                                            params_ptr, g, 1, _lib.ptr(eng.maxbits), _lib.ptr(eng.scale),
-                                            stream.cuda_stream))
+            _lib.check(f.launch(lib, _lib.ptr(eng.table), params_ptr, g, 1, _lib.ptr(eng.maxbits),
+                                _lib.ptr(eng.scale), stream.cuda_stream))
             b.record(stream)
             first, count = f.spans[g]
             alg = ((1 << len(plan.steps[first].active_in)) + (1 << len(plan.steps[first + count - 1].active_out))) * 8

@@ -33,16 +33,19 @@ GROUP_DTYPE = np.dtype([
 ])
 TILE_STEP_DTYPE = np.dtype([("cskip", "<u8"), ("tK", "<u4"), ("tKa", "<u4"), ("tpiv", "<u4"), ("tbeta", "<u4"),
                             ("sK", "<u1"), ("sKa", "<u1"), ("nins", "<u1"), ("rb1", "<u1"), ("rb2", "<u1"),
-                            ("pad", "<u1", (3,)), ("ins", "<u1", (16,)), ("mhi", "<u4"), ("pair", "<u1"),
+                            ("rk1", "<u1"), ("rk2", "<u1"), ("rmix", "<u1"), ("ins", "<u1", (16,)), ("mhi", "<u4"),
+                            ("pair", "<u1"),
                             ("pnins", "<u1"), ("swapB", "<u1"), ("swapA", "<u1"), ("pmhi", "<u4"), ("tau1", "<u4"),
                             ("tau2", "<u4"), ("pins", "<u1", (16,)), ("s1e", "<u1", (4,)), ("s2e", "<u1", (4,)),
-                            ("pad3", "<u4")])
+                            ("ptab", "<u2"), ("run_len", "<u1"), ("rdead", "<u1")])
+TILE_RUN_DTYPE = np.dtype([("nins", "<u1"), ("count", "<u1"), ("r", "<u1"), ("pad", "<u1"), ("ins", "<u1", (16,)),
+                           ("mhi", "<u4"), ("off", "<u2", (16,))])
 DRAW_DTYPE = np.dtype([
     ("index", "<i8"), ("tie", "<i4"), ("status", "<i4"), ("total_cdf", "<f8"), ("total_exact", "<f8"),
     ("selected_weight", "<f8"), ("cdf_lower", "<f8"), ("cdf_upper", "<f8"), ("cdf_lower_exact", "<f8"),
     ("cdf_upper_exact", "<f8"), ("uniform", "<f8"), ("tv53", "<f8"),
 ])
-STRUCTS = [STEP_DTYPE, PARAM_DTYPE, SCALE_DTYPE, GROUP_DTYPE, TILE_STEP_DTYPE, DRAW_DTYPE]
+STRUCTS = [STEP_DTYPE, PARAM_DTYPE, SCALE_DTYPE, GROUP_DTYPE, TILE_STEP_DTYPE, DRAW_DTYPE, TILE_RUN_DTYPE]
 
 _P = ctypes.c_void_p
 _I = ctypes.c_int
@@ -60,6 +63,7 @@ SIGNATURES = {
     "dcs_slice_steps": (_I, [_I, _P, _P, _P, _I, _I, _I, _P, _P, _P]),
     "dcs_slice_steps_batched": (_I, [_I, _P, _U64, _P, _P, _U64, _I, _I, _I, _P, _P, _I, _P]),
     "dcs_fused_groups": (_I, [_P, _P, _I, _P, _I, _P, _P, _I, _I, _P, _P, _P]),
+    "dcs_fused_runs": (_I, [_P, _P, _I, _P, _I, _P, _P, _P, _I, _I, _P, _P, _P]),
     "dcs_accumulate_batched": (_I, [_I, _P, _U64, _I, _P, _I, _P, _P, _P, _P, _I, _D, _P, _P, _U64, _P, _I, _I,
                                     _P]),
     "dcs_block_tail": (_I, [_P, _I, _P, _P, _I, _P]),

@@ -16,9 +16,12 @@ import numpy as np
 from . import _lib
 
 CACHE = Path(__file__).resolve().parent / "autotune_cache.json"
-# (max tile dim, contiguous low bits, max steps per group, kernel variant, step pairs)
-CANDIDATES = [(13, 4, 24, 0, False), (13, 4, 24, 1, False), (12, 4, 24, 0, False), (13, 3, 24, 0, False),
-              (13, 3, 24, 0, True), (13, 5, 24, 0, False), (13, 4, 12, 0, False), (14, 4, 24, 1, False)]
+# (max tile dim, contiguous low bits, max steps per group, kernel variant, step pairs); variant
+# bit 0 = two CTAs per SM, bit 1 = paired tile layout with packed FP32x2 arithmetic, bit 2 =
+# register runs (bit 3: of local dimension 4, else 3)
+CANDIDATES = [(13, 3, 24, 0, True), (13, 3, 24, 12, False), (13, 4, 24, 12, False), (13, 3, 24, 6, False),
+              (13, 4, 24, 6, False), (13, 3, 24, 7, False), (13, 3, 24, 15, False), (13, 5, 24, 6, False),
+              (12, 3, 24, 6, False), (13, 3, 12, 6, False)]
 
 
 def fingerprint(plan):
@@ -71,10 +74,8 @@ def tune(engine, params_dev, candidates=CANDIDATES, repeats=1, save=True):
             a = torch.cuda.Event(enable_timing=True)
             b = torch.cuda.Event(enable_timing=True)
             a.record(stream)
-            _lib.check(lib.dcs_fused_groups(_lib.ptr(engine.table), fp.dsteps.ctypes.data, len(fp.dsteps),
-                                            fp.groups.ctypes.data, len(fp.groups), fp.tile_steps.ctypes.data,
-                                            _lib.ptr(params_dev), 0, len(fp.groups), _lib.ptr(mb),
-                                            _lib.ptr(engine.scale), stream.cuda_stream))
+            _lib.check(fp.launch(lib, _lib.ptr(engine.table), _lib.ptr(params_dev), 0, len(fp.groups), _lib.ptr(mb),
+                                 _lib.ptr(engine.scale), stream.cuda_stream))
             b.record(stream)
             torch.cuda.synchronize(engine.device)
             times.append(a.elapsed_time(b) / 1000.0)

@@ -16,7 +16,7 @@ REPO = PKG.parent
 CSRC = PKG / "csrc"
 INCLUDE = REPO / "include"
 LIB = PKG / "libdcs245.so"
-SOURCES = ["abi.cu", "step.cu", "fused.cu", "block.cu", "draw.cu", "serve.cu"]
+SOURCES = ["abi.cu", "step.cu", "fused.cu", "runs.cu", "block.cu", "draw.cu", "serve.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

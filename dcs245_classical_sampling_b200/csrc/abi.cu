@@ -54,6 +54,7 @@ extern "C" size_t dcs_struct_size(int which) {
         case 3: return sizeof(dcs_group);
         case 4: return sizeof(dcs_tile_step);
         case 5: return sizeof(dcs_draw_result);
+        case 6: return sizeof(dcs_tile_run);
     }
     return 0;
 }

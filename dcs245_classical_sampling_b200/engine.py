@@ -338,10 +338,8 @@ class InplaceConditionalBlockGPU:
         nm = self._nmax() + 1
         if self.mode == "fused":
             f = self.fplan
-            _lib.check(lib.dcs_fused_groups(_lib.ptr(self.table), f.dsteps.ctypes.data, len(f.dsteps),
-                                            f.groups.ctypes.data, len(f.groups), f.tile_steps.ctypes.data,
-                                            params_ptr, 0, len(f.groups), _lib.ptr(self.maxbits),
-                                            _lib.ptr(self.scale), st))
+            _lib.check(f.launch(lib, _lib.ptr(self.table), params_ptr, 0, len(f.groups), _lib.ptr(self.maxbits),
+                                _lib.ptr(self.scale), st))
             return
         if self.mode == "plain":
             mb = self.maxbits.view(self.items, nm)

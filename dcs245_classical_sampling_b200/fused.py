@@ -84,10 +84,21 @@ class FusedPlan:
     groups: np.ndarray
     tile_steps: np.ndarray
     dsteps: np.ndarray
+    tile_runs: np.ndarray = None
     spans: list = field(default_factory=list)      # (first, count) per group
     universe: list = field(default_factory=list)   # |U| per group
     tiles: list = field(default_factory=list)      # tile count per group
     dims: list = field(default_factory=list)
+
+    def launch(self, lib, table, params, g0, ng, maxbits, scale, stream):
+        """Run groups [g0, g0 + ng) (device pointers as ints); returns the library status."""
+        if self.tile_runs is not None:
+            return lib.dcs_fused_runs(table, self.dsteps.ctypes.data, len(self.dsteps), self.groups.ctypes.data,
+                                      len(self.groups), self.tile_steps.ctypes.data, self.tile_runs.ctypes.data,
+                                      params, g0, ng, maxbits, scale, stream)
+        return lib.dcs_fused_groups(table, self.dsteps.ctypes.data, len(self.dsteps), self.groups.ctypes.data,
+                                    len(self.groups), self.tile_steps.ctypes.data, params, g0, ng, maxbits, scale,
+                                    stream)
 
     def algorithmic_bytes(self, plan, elem=8):
         tot = 0
@@ -193,6 +204,131 @@ def _pair_steps(steps, first, count, tsteps, dim, tilepos_of, tbit, U):
         s += 2
 
 
+def _rank(vecs):
+    piv = {}
+    for v in vecs:
+        while v:
+            t = v.bit_length() - 1
+            if t in piv:
+                v ^= piv[t]
+            else:
+                piv[t] = v
+                break
+    return len(piv)
+
+
+def _run_vectors(st, kind, ts, tbit):
+    """(vector, role coordinate) pairs of a step in tile coordinates, and the shrink4 mixing bits.
+
+    A four-entry shrink gets the reduced pair (b1, b2) of span{K, Ka} with b1 one at K's role and
+    zero at Ka's, b2 the other way round; K = b1 (+ b2 if rmix bit 0), Ka = b2 (+ b1 if bit 1)."""
+    if kind == KIND_GROW:
+        return [(int(ts["tpiv"]), tbit(st.pivot))], 0
+    if kind == 1:
+        return [(int(ts["tKa"]), tbit(st.pivot_a))], 0
+    if kind in (3, 5, 7):
+        return [(int(ts["tK"]), tbit(st.pivot))], 0
+    if kind == 6:
+        tK, tKa = int(ts["tK"]), int(ts["tKa"])
+        p, pa = tbit(st.pivot), tbit(st.pivot_a)
+        a, b = (tK >> pa) & 1, (tKa >> p) & 1
+        if a and b:
+            return None, 0
+        return [(tK ^ tKa if a else tK, p), (tKa ^ tK if b else tKa, pa)], a | (b << 1)
+    return [], 0
+
+
+def _plan_runs(steps, first, count, tsteps, truns, dim, R, tbit, slot_of):
+    """Split a group's steps into register runs of local dimension R; False if a step does not fit."""
+    vr = []
+    for s in range(first, first + count):
+        kind, _ = orbit_kind(steps[s])
+        v, mix = _run_vectors(steps[s], kind, tsteps[s], tbit)
+        if v is None:
+            return False
+        vr.append((v, mix))
+    runs = []
+    s = first
+    while s < first + count:
+        basis, n, locs = [], 0, []
+        while s + n < first + count and n < 255:
+            if int(tsteps[s + n]["cskip"]) != int(tsteps[s]["cskip"]):
+                break
+            nb = list(basis)
+            loc = []
+            ok = True
+            for v, p in vr[s + n - first][0]:
+                idx = next((i for i, (bv, _) in enumerate(nb) if bv == v), None)
+                if idx is None:
+                    nb.append((v, p))
+                    loc.append(len(nb) - 1)
+                elif nb[idx][1] != p:
+                    ok = False
+                else:
+                    loc.append(idx)
+            ok = ok and len(nb) <= R and _rank([v for v, _ in nb]) == len(nb) and len({p for _, p in nb}) == len(nb)
+            # no basis vector touches another's role coordinate (the representatives of every
+            # step are then the local indices with a zero at the step's own local bit)
+            ok = ok and all(not (vb >> pa) & 1 for ia, (_, pa) in enumerate(nb) for ib, (vb, _) in enumerate(nb)
+                            if ia != ib)
+            if not ok:
+                break
+            basis = nb
+            locs.append(loc)
+            n += 1
+        if n == 0:
+            return False
+        runs.append((s, n, basis, locs))
+        s += n
+    for s0, n, basis, locs in runs:
+        roles = {p for _, p in basis}
+        support = 0
+        for v, _ in basis:
+            support |= v
+        active = slot_mask(steps[s0].active_in)
+        inactive = [q for q in range(dim) if not (active >> slot_of(q)) & 1 and q not in roles
+                    and not (support >> q) & 1]
+        # pad to R dimensions with unit vectors of active coordinates outside the run's support,
+        # the highest first (the low coordinates stay with the threads of a warp)
+        for q in reversed(range(dim)):
+            if len(basis) >= R:
+                break
+            if q not in roles and q not in inactive and not (support >> q) & 1:
+                basis.append((1 << q, q))
+                roles.add(q)
+        if len(basis) < R:
+            return False
+        ins = sorted(roles | set(inactive))
+        if len(ins) > 16:
+            return False
+        tr = truns[s0]
+        tr["nins"], tr["count"], tr["r"] = len(ins), n, R
+        for i, b in enumerate(ins):
+            tr["ins"][i] = b
+        free = [b for b in range(dim) if b not in ins]
+        tr["mhi"] = sum(1 << b for b in free[8:])
+        offs = []
+        for j in range(1 << R):
+            o = 0
+            for k in range(R):
+                if (j >> k) & 1:
+                    o ^= basis[k][0]
+            offs.append(o)
+            tr["off"][j] = o
+        for i in range(n):
+            ts = tsteps[s0 + i]
+            act = slot_mask(steps[s0 + i].active_in)
+            ts["rdead"] = sum(1 << k for k, (_, p) in enumerate(basis)
+                              if k not in locs[i] and not (act >> slot_of(p)) & 1)
+            loc = locs[i] + [0, 0]
+            ts["rk1"], ts["rk2"] = loc[0], loc[1]
+            ts["rmix"] = vr[s0 + i - first][1]
+            tb = int(ts["tbeta"])
+            ts["ptab"] = sum((bin(o & tb).count("1") & 1) << j for j, o in enumerate(offs))
+            ts["run_len"] = n if i == 0 else 0
+    return True
+
+
 def build_fused_plan(plan, max_dim=13, low=4, max_steps=MAX_GROUP_STEPS, max_extra=1, spans=None, variant=0,
                      pairs=False):
     steps = plan.steps
@@ -200,7 +336,8 @@ def build_fused_plan(plan, max_dim=13, low=4, max_steps=MAX_GROUP_STEPS, max_ext
         spans = group_steps(steps, max_dim, low, max_steps, max_extra)
     groups = np.zeros(len(spans), dtype=_lib.GROUP_DTYPE)
     tsteps = np.zeros(len(steps), dtype=_lib.TILE_STEP_DTYPE)
-    fp = FusedPlan(groups=groups, tile_steps=tsteps, dsteps=device_steps(steps), spans=list(spans))
+    truns = np.zeros(len(steps), dtype=_lib.TILE_RUN_DTYPE) if variant & 4 else None
+    fp = FusedPlan(groups=groups, tile_steps=tsteps, dsteps=device_steps(steps), spans=list(spans), tile_runs=truns)
     for gi, (first, count) in enumerate(spans):
         U = 0
         vecs = []
@@ -324,7 +461,12 @@ def build_fused_plan(plan, max_dim=13, low=4, max_steps=MAX_GROUP_STEPS, max_ext
             ts["mhi"] = sum(1 << b for b in free[8:])  # 256 threads: index bits >= 8
             ts["rb1"] = max(st.pivot_a if kind == 1 else st.pivot, 0)  # role slot(s), for checking
             ts["rb2"] = max(st.pivot_a, 0) if kind == 6 else 0
-        if pairs:
+        if variant & 4:
+            R = 4 if variant & 8 else 3
+            slot_of = lambda q: q if q < l else pivots[q - l]
+            if not _plan_runs(steps, first, count, tsteps, truns, dim, R, tbit, slot_of):
+                g["variant"] = variant & ~12  # this group keeps the one-step-per-round-trip kernel
+        elif pairs:
             _pair_steps(steps, first, count, tsteps, dim, tilepos_of=lambda q: (q < l or q in pivots),
                         tbit=tbit, U=U)
         fp.universe.append(bin(U).count("1"))

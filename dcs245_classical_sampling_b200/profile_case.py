@@ -33,6 +33,7 @@ def main():
     ap.add_argument("--max-dim", type=int, default=13)
     ap.add_argument("--low", type=int, default=4)
     ap.add_argument("--variant", type=int, default=0)
+    ap.add_argument("--pairs", action="store_true", help="two steps per shared-memory round trip")
     a = ap.parse_args()
     lib = _lib.load()
     w = build_workload(a.workload)
@@ -56,7 +57,7 @@ def main():
     stream = torch.cuda.current_stream(dev)
     sub = P.BlockPlan(**{**bp.__dict__, "steps": steps})
     if a.mode == "fused":
-        fp = build_fused_plan(sub, max_dim=a.max_dim, low=a.low, variant=a.variant)
+        fp = build_fused_plan(sub, max_dim=a.max_dim, low=a.low, variant=a.variant, pairs=a.pairs)
         nmax = len(fp.groups)
     else:
         dsteps = device_steps(steps)
@@ -76,10 +77,8 @@ def main():
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
             if a.mode == "fused":
-                _lib.check(lib.dcs_fused_groups(_lib.ptr(table), fp.dsteps.ctypes.data, len(fp.dsteps),
-                                                fp.groups.ctypes.data, len(fp.groups), fp.tile_steps.ctypes.data,
-                                                _lib.ptr(params), g, 1, _lib.ptr(maxbits), _lib.ptr(scale),
-                                                stream.cuda_stream))
+                _lib.check(fp.launch(lib, _lib.ptr(table), _lib.ptr(params), g, 1, _lib.ptr(maxbits),
+                                     _lib.ptr(scale), stream.cuda_stream))
                 first, count = fp.spans[g]
                 alg = ((1 << len(steps[first].active_in)) + (1 << len(steps[first + count - 1].active_out))) * 8
             else:

@@ -111,7 +111,9 @@ typedef struct dcs_group {
     int32_t tile_dim, low_bits;
     int32_t coset_m, ncoset_runs;
     int32_t step_tile_off; /* index into the per-step tile-mask table */
-    int32_t variant;       /* kernel variant: 0 = 3 CTAs per SM, 1 = 2 CTAs per SM */
+    int32_t variant;       /* kernel variant bits: 1 = 2 CTAs per SM (else 3); 2 = paired tile layout with
+                              packed FP32x2 arithmetic; 4 = register runs (dcs_fused_runs); 8 = runs of
+                              local dimension 4 (else 3) */
     uint64_t out_mask;     /* active_out after the last step (for the max) */
     uint64_t basis[16];    /* tile basis (slot masks) */
     uint32_t coset_runs[DCS_MAX_RUNS];
@@ -131,7 +133,10 @@ typedef struct dcs_tile_step {
     uint8_t sK, sKa;        /* parity(tK & tbeta), parity(tKa & tbeta) */
     uint8_t nins;           /* number of inserted zero bits (<= 16) */
     uint8_t rb1, rb2;       /* physical role slots (for checking) */
-    uint8_t pad[3];
+    /* register runs (group variant bit 4): local bit of the step's orbit vector (shrink4: of K's
+     * reduced vector) and of Ka's reduced vector; rmix bit 0: K = local rk1 + rk2, bit 1: Ka =
+     * local rk1 + rk2 */
+    uint8_t rk1, rk2, rmix;
     uint8_t ins[16];        /* inserted tile bits, ascending */
     uint32_t mhi;           /* tile bits receiving representative-index bits 8 and up (256 threads) */
     /* pairing with the next step (one shared-memory round trip for both): super-orbit
@@ -145,8 +150,26 @@ typedef struct dcs_tile_step {
     uint32_t tau1, tau2;
     uint8_t pins[16];
     uint8_t s1e[4], s2e[4];
-    uint32_t pad3;          /* explicit tail padding (8-byte alignment) */
+    uint16_t ptab;          /* register runs: bit j = parity(local offset j & tbeta) */
+    uint8_t run_len;        /* register runs: steps in the run that starts here (0 inside a run) */
+    uint8_t rdead;          /* register runs: local bits whose role slot is inactive at this step (entries
+                               with such a bit set are skipped) */
 } dcs_tile_step;
+
+/* A register run: consecutive steps of a group whose orbit vectors span a space V of dimension
+ * r (3 or 4) with one role coordinate per basis vector, and no basis vector touching another's
+ * role coordinate.  The tile splits into cosets t0 + V with t0 zero at ins[] (the role
+ * coordinates and the coordinates inactive through the run); a thread holds one coset in
+ * registers (entry j at tile index t0 ^ off[j]) and applies every step of the run to it. */
+typedef struct dcs_tile_run {
+    uint8_t nins;           /* zero bits of the coset representatives t0, ascending in ins[] */
+    uint8_t count;          /* steps in the run */
+    uint8_t r;              /* local dimension */
+    uint8_t pad;
+    uint8_t ins[16];
+    uint32_t mhi;           /* tile bits receiving representative-index bits 8 and up (256 threads) */
+    uint16_t off[16];       /* tile offsets of the 2^r local entries */
+} dcs_tile_run;
 
 /* Result of one draw (device-side struct; the host copies it back). */
 typedef struct dcs_draw_result {
@@ -168,7 +191,8 @@ const char *dcs_last_error(void);
 /* Number of SMs of the current device (for grid sizing); negative on error. */
 int dcs_sm_count(void);
 /* sizeof of the ABI structs, so that bindings can check their layouts:
- * 0 dcs_step, 1 dcs_param, 2 dcs_scale, 3 dcs_group, 4 dcs_tile_step, 5 dcs_draw_result. */
+ * 0 dcs_step, 1 dcs_param, 2 dcs_scale, 3 dcs_group, 4 dcs_tile_step, 5 dcs_draw_result,
+ * 6 dcs_tile_run. */
 size_t dcs_struct_size(int which);
 
 /* Reference-compatible single step (kernel `inplace_step`, inplace_gpu.py:20-63): the same
@@ -200,6 +224,13 @@ int dcs_slice_steps_batched(int dtype, void *table, uint64_t table_stride, const
 int dcs_fused_groups(void *table, const dcs_step *steps, int nsteps, const dcs_group *groups, int ngroups,
                      const dcs_tile_step *tile_steps, const dcs_param *params, int g0, int ng,
                      uint64_t *maxbits, dcs_scale *scale, void *stream);
+
+/* The same passes, with register runs for the groups whose variant has bit 4: tile_runs[i] is
+ * the run that starts at step i (tile_steps[i].run_len > 0); other groups run as in
+ * dcs_fused_groups. */
+int dcs_fused_runs(void *table, const dcs_step *steps, int nsteps, const dcs_group *groups, int ngroups,
+                   const dcs_tile_step *tile_steps, const dcs_tile_run *tile_runs, const dcs_param *params,
+                   int g0, int ng, uint64_t *maxbits, dcs_scale *scale, void *stream);
 
 /* Terminal gather + syndrome scatter + coherent slice accumulation into complex128 blocks.
  * For output block b, items item_begin[b] .. item_begin[b+1]-1 (slices, in slice order) add

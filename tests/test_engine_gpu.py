@@ -63,6 +63,21 @@ def test_fused_step_pairs_match_reference(golden, name):
         assert rel_l2(v.cpu().numpy(), arrays[f"block_{rec['sample_id']}"]) < 1e-5
 
 
+@pytest.mark.parametrize("name", ["c1", "small", "c2"])
+@pytest.mark.parametrize("variant", [2, 3, 4, 12, 13, 6, 7, 15])
+def test_fused_kernel_variants_match_reference(golden, name, variant):
+    """Paired layout with packed FP32x2 arithmetic (2, 3), register runs of local dimension 3 or
+    4 (4, 12, 13) and packed register runs (6, 7, 15): every autotuner variant against the
+    reference blocks."""
+    case, arrays = golden(name)
+    eng = _engine(case, arrays, np.complex64, mode="fused")
+    eng.set_fused_config(variant=variant, pairs=False, max_dim=13, low=4)
+    assert (eng.fplan.groups["variant"] == variant).any()
+    for rec in case["protocol"]["records"]:
+        v, _ = eng.block(_x(rec))
+        assert rel_l2(v.cpu().numpy(), arrays[f"block_{rec['sample_id']}"]) < 1e-5
+
+
 def test_one_item_at_a_time_equals_batched_slices(golden):
     case, arrays = golden("small")
     a = _engine(case, arrays, np.complex128, items=1)

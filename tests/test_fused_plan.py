@@ -31,7 +31,8 @@ def _neg(a, beta, ov):
     return (par.astype(np.int64) ^ ov).astype(bool)
 
 
-def emulate(bp, fp, params):
+def emulate(bp, fp, params, packed=False):
+    """packed=True follows the paired-layout kernel: packed steps where tile bit 0 is free."""
     steps = bp.steps
     E = np.zeros(1 << bp.maxslots, np.complex128)
     E[0] = 1
@@ -56,10 +57,19 @@ def emulate(bp, fp, params):
         sh = np.where((A & np.uint64(~inm & (2**64 - 1))) == 0, E[A.astype(np.int64)] * sc, 0)
         s = first
         while s < first + count:
+            if int(g["variant"]) & 4:
+                sh = _emulate_run(bp, fp, params, s, bases, sh, dim, packed=bool(int(g["variant"]) & 2))
+                s += int(fp.tile_steps[s]["run_len"])
+                continue
             st = steps[s]
             kind, _ = P.orbit_kind(st)
             ts = fp.tile_steps[s]
-            if int(ts["pair"]) and s + 1 < first + count:
+            if packed:
+                if _packable(ts, kind, dim):
+                    sh = _emulate_packed(st, kind, ts, params[s], bases, A, sh, dim)
+                    s += 1
+                    continue
+            elif int(ts["pair"]) and s + 1 < first + count:
                 sh = _emulate_pair(bp, fp, params, s, bases, A, sh, dim, low)
                 s += 2
                 continue
@@ -241,6 +251,202 @@ def _emulate_pair(bp, fp, params, s, bases, A, sh, dim, low):
     return sh
 
 
+def _emulate_run(bp, fp, params, s0, bases, sh, dim, packed=False):
+    """Mirror of csrc/fused.cu register runs: cosets t0 + V held in registers."""
+    tr = fp.tile_runs[s0]
+    n, R, nins = int(tr["count"]), int(tr["r"]), int(tr["nins"])
+    assert n >= 1 and int(fp.tile_steps[s0]["run_len"]) == n
+    ins = [int(v) for v in tr["ins"][:nins]]
+    nb = (1 << dim) >> nins
+    threads = min(nb, 256)
+    o = np.arange(threads, dtype=np.int64)
+    for rho in ins:
+        o = ((o >> rho) << (rho + 1)) | (o & ((1 << rho) - 1))
+    mhi = int(tr["mhi"])
+    niter = nb >> 8 if nb > 256 else 1
+    tus, tu = [], 0
+    for _ in range(niter):
+        tus.append(tu)
+        tu = ((tu | (~mhi & 0xFFFFFFFF)) + 1) & mhi
+    t0 = (o[:, None] | np.array(tus, dtype=np.int64)[None, :]).reshape(-1)
+    off = np.array([int(v) for v in tr["off"][:1 << R]], dtype=np.int64)
+    idx = t0[:, None] ^ off[None, :]                      # base, local entry
+    # the cosets are disjoint and cover the tile minus the run's inactive coordinates
+    assert len(np.unique(idx)) == idx.size
+    if packed and nins < dim and (nins == 0 or ins[0] != 0):
+        # paired layout: coset pairs (t0, t0 | 1) from spread(tid << 1) and the walk over mhi
+        # without its lowest bit; local entry j of lane L sits at ((t0 ^ off_j) & ~1) + (L ^ off_j & 1)
+        nb2 = nb >> 1
+        o2 = np.arange(min(nb2, 256), dtype=np.int64) << 1
+        for rho in ins:
+            o2 = ((o2 >> rho) << (rho + 1)) | (o2 & ((1 << rho) - 1))
+        m2 = mhi & (mhi - 1)
+        tus2, tu = [], 0
+        for _ in range(nb2 >> 8 if nb2 > 256 else 1):
+            tus2.append(tu)
+            tu = ((tu | (~m2 & 0xFFFFFFFF)) + 1) & m2
+        tp2 = (o2[:, None] | np.array(tus2, dtype=np.int64)[None, :]).reshape(-1)
+        assert not (tp2 & 1).any()
+        assert np.array_equal(np.sort(np.concatenate([tp2, tp2 | 1])), np.sort(t0))
+        for L in (0, 1):
+            pos = ((tp2[:, None] ^ off[None, :]) & ~1) + (L ^ (off[None, :] & 1))
+            assert np.array_equal(pos, (tp2[:, None] | L) ^ off[None, :])
+    live = ((bases & np.uint64(int(fp.tile_steps[s0]["cskip"]))) == 0)[:, None, None]
+    v = sh[:, idx].copy()                                 # tile, base, local
+    for s in range(s0, s0 + n):
+        st = bp.steps[s]
+        kind, _ = P.orbit_kind(st)
+        ts = fp.tile_steps[s]
+        assert int(ts["cskip"]) == int(fp.tile_steps[s0]["cskip"])
+        pr = params[s]
+        f0, f1 = complex(pr["f0r"], pr["f0i"]), complex(pr["f1r"], pr["f1i"])
+        y = int(pr["y"])
+        gK, gKa = (-1.0 if int(ts["sK"]) else 1.0), (-1.0 if int(ts["sKa"]) else 1.0)
+        tb, ptab = int(ts["tbeta"]), int(ts["ptab"])
+        cs = np.array([bin(int(bb) & st.beta).count("1") & 1 for bb in bases], np.int64)[:, None] ^ int(pr["ov"])
+        s0b = np.array([bin(int(q) & tb).count("1") & 1 for q in t0], np.int64)[None, :] ^ cs  # tile, base
+        sg = lambda j: np.where(s0b ^ ((ptab >> j) & 1), -1.0, 1.0)
+        k1, k2, mix = int(ts["rk1"]), int(ts["rk2"]), int(ts["rmix"])
+        dead = int(ts["rdead"])
+        e = 1 << k1
+        new = v.copy()
+        for j in range(1 << R):
+            if j & dead:
+                continue  # a removed or not yet grown slot: the kernel skips these entries
+            x = v[:, :, j]
+            if kind in (P.KIND_DIAG, P.KIND_FIXED):
+                if kind == P.KIND_DIAG:
+                    new[:, :, j] = (f0 + sg(j) * f1) * x
+                else:
+                    new[:, :, j] = sg(j) * f1 * x if y else f0 * x
+                continue
+            if kind == P.KIND_SHRINK4:
+                if j & (e | (1 << k2)):
+                    continue
+                mK = e | ((1 << k2) if mix & 1 else 0)
+                mKa = (1 << k2) | (e if mix & 2 else 0)
+                b, g_, h = v[:, :, j ^ mK], v[:, :, j ^ mKa], v[:, :, j ^ mK ^ mKa]
+                new[:, :, j] = f0 * (x + b) + sg(j) * gKa * f1 * (g_ + gK * h)
+                new[:, :, j ^ mKa] = f0 * (g_ + h) + sg(j) * f1 * (x + gK * b)
+                continue
+            if j & e:
+                continue
+            d = j | e
+            b = v[:, :, d]
+            if kind == P.KIND_GROW:
+                new[:, :, j], new[:, :, d] = f0 * x, sg(j) * f1 * x
+            elif kind == P.KIND_MIX:
+                new[:, :, j] = f0 * x + sg(j) * gKa * f1 * b
+                new[:, :, d] = f0 * b + sg(j) * f1 * x
+            elif kind == P.KIND_REPLACE:
+                new[:, :, j], new[:, :, d] = f0 * (x + b), sg(j) * f1 * (x + gK * b)
+            elif kind == P.KIND_FIXED_SHRINK:
+                new[:, :, j] = sg(j) * f1 * (x + gK * b) if y else f0 * (x + b)
+            else:
+                new[:, :, j] = f0 * (x + b) + sg(j) * f1 * (x + gK * b)
+        v = np.where(live, new, v)
+    out = sh.copy()
+    out[:, idx] = v
+    return out
+
+
+def _packable(ts, kind, dim):
+    nins = int(ts["nins"])
+    return nins < dim and (nins == 0 or int(ts["ins"][0]) != 0) and not (kind == P.KIND_GROW and int(ts["tpiv"]) & 1)
+
+
+def _emulate_packed(st, kind, ts, pr, bases, A, sh, dim):
+    """Mirror of csrc/fused.cu run_packed: representative pairs (t, t + 1) in two lanes."""
+    nins = int(ts["nins"])
+    ins = [int(v) for v in ts["ins"][:nins]]
+    nrep = (1 << dim) >> (nins + 1)
+    threads = min(nrep, 256)
+    o = np.arange(threads, dtype=np.int64) << 1
+    for rho in ins:
+        o = ((o >> rho) << (rho + 1)) | (o & ((1 << rho) - 1))
+    tp = o
+    mhi = int(ts["mhi"]) & (int(ts["mhi"]) - 1)
+    niter = nrep >> 8 if nrep > 256 else 1
+    tus, tu = [], 0
+    for _ in range(niter):
+        tus.append(tu)
+        tu = ((tu | (~mhi & 0xFFFFFFFF)) + 1) & mhi
+    tus = np.array(tus, dtype=np.int64)
+    t = (tp[:, None] | tus[None, :]).reshape(-1)
+    # the pairs cover every representative (zero at the inserted bits) exactly once
+    insmask = sum(1 << b for b in ins)
+    reps = np.flatnonzero((np.arange(1 << dim) & insmask) == 0)
+    assert np.array_equal(np.sort(np.concatenate([t, t + 1])), reps)
+    assert not (t & 1).any()
+    tb = int(ts["tbeta"])
+    f0, f1 = complex(pr["f0r"], pr["f0i"]), complex(pr["f1r"], pr["f1i"])
+    y = int(pr["y"])
+    gK, gKa = (-1.0 if int(ts["sK"]) else 1.0), (-1.0 if int(ts["sKa"]) else 1.0)
+    R = np.arange(len(bases))[:, None]
+    live = ((bases & np.uint64(int(ts["cskip"]))) == 0)[:, None]
+    cs = np.array([bin(int(bb) & st.beta).count("1") & 1 for bb in bases], np.int64)[:, None] ^ int(pr["ov"])
+    # lane signs as the kernel forms them: parity over tp, then over tu, lane 1 flipped by tbeta bit 0
+    par = lambda v: np.array([bin(int(q) & tb).count("1") & 1 for q in v], np.int64)
+    s0 = (np.repeat(par(tp), niter)[None, :] ^ np.tile(par(tus), threads)[None, :]) ^ cs
+    S = np.stack([np.where(s0, -1.0, 1.0), np.where(s0 ^ (tb & 1), -1.0, 1.0)])  # lane, tile, rep
+
+    def load(off, sw):
+        base = t ^ off
+        lo, hi = sh[R, base], sh[R, base + 1]
+        return np.stack([hi, lo]) if sw else np.stack([lo, hi])
+
+    def store(out, off, sw, val):
+        base = t ^ off
+        v = val[::-1] if sw else val
+        out[R, base] = np.where(live, v[0], out[R, base])
+        out[R, base + 1] = np.where(live, v[1], out[R, base + 1])
+
+    tK, tKa, tpiv = int(ts["tK"]), int(ts["tKa"]), int(ts["tpiv"])
+    x = load(0, False)
+    out = sh.copy()
+    touched = [t >> 1]
+    if kind == P.KIND_GROW:
+        store(out, 0, False, f0 * x)
+        store(out, tpiv & ~1, False, S * (f1 * x))
+        touched.append((t ^ (tpiv & ~1)) >> 1)
+    elif kind == P.KIND_MIX:
+        sw = tKa & 1
+        bs = S * load(tKa & ~1, sw)
+        store(out, 0, False, f0 * x + gKa * f1 * bs)
+        store(out, tKa & ~1, sw, S * (f0 * bs + f1 * x))
+        touched.append((t ^ (tKa & ~1)) >> 1)
+    elif kind == P.KIND_DIAG:
+        store(out, 0, False, (f0 + S * f1) * x)
+    elif kind == P.KIND_REPLACE:
+        sw = tK & 1
+        b = load(tK & ~1, sw)
+        store(out, 0, False, f0 * (x + b))
+        store(out, tK & ~1, sw, S * (f1 * (x + gK * b)))
+        touched.append((t ^ (tK & ~1)) >> 1)
+    elif kind == P.KIND_FIXED:
+        store(out, 0, False, S * (f1 * x) if y else f0 * x)
+    elif kind == P.KIND_FIXED_SHRINK:
+        b = load(tK & ~1, tK & 1)
+        store(out, 0, False, S * (f1 * (x + gK * b)) if y else f0 * (x + b))
+        touched.append((t ^ (tK & ~1)) >> 1)
+    elif kind == P.KIND_SHRINK4:
+        sw1, sw2 = tK & 1, tKa & 1
+        b, g = load(tK & ~1, sw1), load(tKa & ~1, sw2)
+        h = load((tK ^ tKa) & ~1, sw1 ^ sw2)
+        Sd = S * gKa
+        store(out, 0, False, f0 * (x + b) + Sd * (f1 * (g + gK * h)))
+        store(out, tKa & ~1, sw2, f0 * (g + h) + S * (f1 * (x + gK * b)))
+        touched += [(t ^ (tK & ~1)) >> 1, (t ^ (tKa & ~1)) >> 1, (t ^ ((tK ^ tKa) & ~1)) >> 1]
+    else:
+        b = load(tK & ~1, tK & 1)
+        store(out, 0, False, f0 * (x + b) + S * (f1 * (x + gK * b)))
+        touched.append((t ^ (tK & ~1)) >> 1)
+    # the 16-byte pairs a step touches are disjoint between representative pairs
+    allp = np.concatenate(touched)
+    assert len(np.unique(allp)) == len(allp)
+    return out
+
+
 @pytest.mark.parametrize("name,dims", [("c1", [(13, 4), (6, 2), (4, 0)]), ("small", [(13, 4), (8, 3), (6, 2)]),
                                        ("c2", [(13, 4)])])
 def test_fused_emulation_matches_oracle(golden, name, dims):
@@ -258,11 +464,13 @@ def test_fused_emulation_matches_oracle(golden, name, dims):
         want, wls, off = block_ref.execute(oe.steps, f, yfix, oe.fut, oe.maxslots)
         freeflip = sum(int(flips[q]) << j for j, q in enumerate(oe.open_red))
         assert xor == (off >> oe.stop) ^ freeflip
-        for (max_dim, low), pairs in [(d, pr) for d in dims for pr in (False, True)]:
-            fp = build_fused_plan(bp, max_dim=max_dim, low=low, pairs=pairs)
+        for (max_dim, low), mode in [(d, m) for d in dims
+                                     for m in ("plain", "pairs", "packed", "runs3", "runs4", "pruns3")]:
+            variant = {"runs3": 4, "runs4": 12, "pruns3": 6}.get(mode, 0)
+            fp = build_fused_plan(bp, max_dim=max_dim, low=low, pairs=mode == "pairs", variant=variant)
             assert sum(c for _, c in fp.spans) == len(bp.steps)
-            assert (int(fp.tile_steps["pair"].sum()) > 0) == pairs
-            got, gls = emulate(bp, fp, params)
+            assert (int(fp.tile_steps["pair"].sum()) > 0) == (mode == "pairs")
+            got, gls = emulate(bp, fp, params, packed=mode == "packed")
             if not np.any(want):
                 assert not np.any(got)  # the slice's table vanished: the reference skips it
             else:
