@@ -16,7 +16,8 @@ REPO = PKG.parent
 CSRC = PKG / "csrc"
 INCLUDE = REPO / "include"
 LIB = PKG / "libdcs245.so"
-SOURCES = ["abi.cu", "step.cu", "fused.cu", "runs.cu", "block.cu", "draw.cu", "serve.cu"]
+SOURCES = ["abi.cu", "step.cu", "fused.cu", "runs.cu", "runs_r4.cu", "runs_packed.cu", "block.cu", "draw.cu",
+           "serve.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -28,22 +29,38 @@ def nvcc_path():
 
 
 def build(verbose=False, ptxas_info=False, force=False):
+    """Compile every source to an object (in parallel: the register-run kernels take minutes)
+    and link the shared library."""
+    from concurrent.futures import ThreadPoolExecutor
     srcs = [CSRC / s for s in SOURCES if (CSRC / s).exists()]
     deps = srcs + list(CSRC.glob("*.cuh")) + [INCLUDE / "dcs245.h"]
     if not force and LIB.exists() and all(LIB.stat().st_mtime >= d.stat().st_mtime for d in deps):
         return LIB
-    cmd = [nvcc_path(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
-           "-Xcompiler", "-fvisibility=hidden", "--expt-relaxed-constexpr",
-           f"-I{INCLUDE}", f"-I{CSRC}", "-o", str(LIB) + ".tmp", *map(str, srcs)]
+    objdir = PKG / "_build"
+    objdir.mkdir(exist_ok=True)
+    flags = [*ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
+             "--expt-relaxed-constexpr", f"-I{INCLUDE}", f"-I{CSRC}"]
     if ptxas_info:
-        cmd.insert(1, "-Xptxas=-v")
-    if verbose:
-        print(" ".join(cmd), flush=True)
+        flags.append("-Xptxas=-v")
+
+    def compile_one(src):
+        obj = objdir / (src.stem + ".o")
+        cmd = [nvcc_path(), *flags, "-c", str(src), "-o", str(obj)]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        return obj, subprocess.run(cmd, capture_output=True, text=True)
+
+    with ThreadPoolExecutor(max_workers=len(srcs)) as ex:
+        results = list(ex.map(compile_one, srcs))
+    for obj, r in results:
+        if r.returncode != 0:
+            raise RuntimeError(f"nvcc failed on {obj.stem}.cu:\n" + r.stdout + r.stderr)
+        if verbose or ptxas_info:
+            print(r.stdout + r.stderr)
+    cmd = [nvcc_path(), *ARCH, "-shared", "-o", str(LIB) + ".tmp", *[str(o) for o, _ in results]]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
-        raise RuntimeError("nvcc failed:\n" + r.stdout + r.stderr)
-    if verbose or ptxas_info:
-        print(r.stdout + r.stderr)
+        raise RuntimeError("nvcc link failed:\n" + r.stdout + r.stderr)
     os.replace(str(LIB) + ".tmp", LIB)
     return LIB
 
