@@ -59,6 +59,8 @@ def parse():
     ap.add_argument("--serve-rate", type=float, default=1.0, help="Poisson request rate (1/s)")
     ap.add_argument("--serve-max-samples", type=int, default=64)
     ap.add_argument("--hbm-budget-gib", type=float, default=170.0)
+    ap.add_argument("--graphs", action="store_true",
+                    help="serving: replay each runner's batch as a CUDA graph (captured per batch size)")
     return ap.parse_args()
 
 
@@ -492,7 +494,9 @@ def serve_arm(args):
     left = budget - big.table_bytes()
     for name, share in (("ring48_d55_t177_k17", 0.8), ("ring32_d37_t79_k14", 0.2)):
         runners[name] = CircuitRunner(name, build_workload(name), key=args.seed + len(runners), max_samples=64,
-                                      device=local, hbm_budget=left * share)
+                                      device=local, hbm_budget=left * share, graphs=args.graphs)
+    for r in runners.values():  # every batch size captured before the arrivals start
+        r.precapture(range(1, r.max_samples + 1))
     setup = time.perf_counter() - t0
     # warm every runner once
     from dcs245_classical_sampling_b200.serve import Request
@@ -524,7 +528,7 @@ def serve_arm(args):
             "hbm_budget_gib": args.hbm_budget_gib,
             "slots": {c: {"samples_per_launch": r.max_samples, "table_items": r.engine.items,
                           "table_gib": r.table_bytes() / 2 ** 30, "mode": r.mode} for c, r in runners.items()},
-            "ties": ties, "failed_draws": bad, "setup_s": setup, "clocks": clk,
+            "ties": ties, "failed_draws": bad, "cuda_graphs": bool(args.graphs), "setup_s": setup, "clocks": clk,
             "data": "synthetic (seeded ring circuits, Philox4x32-10 prefixes and uniforms on the device)"}
     print(json.dumps(line), flush=True)
 

@@ -110,8 +110,12 @@ class Batch:
 class CircuitRunner:
     """One circuit: engine, stream, device tables, in-flight batch buffers."""
 
-    def __init__(self, name, workload, key, max_samples, device=0, mode=None, hbm_budget=None):
+    def __init__(self, name, workload, key, max_samples, device=0, mode=None, hbm_budget=None, graphs=False):
+        """graphs=True: the device work of a batch (prefixes, parameters, contraction, accumulation,
+        tail, draw) is captured once per batch size as a CUDA graph and replayed."""
         self.name, self.key = name, int(key)
+        self.graphs = bool(graphs)
+        self._graph = {}
         w = workload
         self.device = torch.device("cuda", device)
         self.engine = InplaceConditionalBlockGPU(w["graph"], w["unitaries"], w["n"], w["order"],
@@ -162,39 +166,72 @@ class CircuitRunner:
             begins.extend(bl)
         return chunks, begins
 
+    def _device_work(self, n, chunks):
+        """Every device step of a batch of n samples after the id upload, on self.stream, with
+        fixed buffers only (so that it can be captured as a CUDA graph)."""
+        eng, lib = self.engine, self.lib
+        st = self.stream.cuda_stream
+        _lib.check(lib.dcs_philox_prefixes(_lib.ptr(self.d_ids), _lib.ptr(self.d_ids) + 4 * n, n, self.key,
+                                           _lib.ptr(self.dc.closed), int(self.dc.closed.numel()),
+                                           _lib.ptr(self.d_x), _lib.ptr(self.d_u), st))
+        self.dc.build(lib, self.d_x, n, self.d_params, self.d_coefs, self.d_xors, st)
+        out = self.d_out[:n]
+        out.zero_()
+        entry = _lib.PARAM_DTYPE.itemsize
+        nm = eng._nmax() + 1
+        for c0, cn, b0, nb, boff in chunks:
+            eng._reset_items(cn)
+            eng._run_steps(_lib.ptr(self.d_params) + c0 * eng.nsteps * entry, cn)
+            _lib.check(lib.dcs_accumulate_batched(
+                eng.dcode, _lib.ptr(eng.table), eng.table_stride, eng.plan.terminal_rank,
+                eng.term_runs.ctypes.data, eng.term_nruns, eng.tbasis.ctypes.data,
+                _lib.ptr(self.d_xors) + 8 * c0, _lib.ptr(self.d_coefs) + 16 * c0,
+                _lib.ptr(self.d_begin) + 4 * boff, nb, eng.params.shift, _lib.ptr(eng.scale),
+                _lib.ptr(eng.maxbits[nm - 1:]), nm, _lib.ptr(out[b0:b0 + nb]), self.k, cn, st))
+        _lib.check(lib.dcs_block_tail(_lib.ptr(out), self.k, eng.adj_hi.ctypes.data, eng.u_open.ctypes.data, n, st))
+        _lib.check(lib.dcs_draw(_lib.ptr(out), self.k, n, _lib.ptr(self.d_u), _lib.ptr(self.d_scratch),
+                                _lib.ptr(self.d_res), st))
+
+    def _replay(self, n, chunks):
+        g = self._graph.get(n)
+        if g is None:
+            # one direct run first (kernel attributes, allocator), then the capture
+            self._device_work(n, chunks)
+            self.stream.synchronize()
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g, stream=self.stream):
+                self._device_work(n, chunks)
+            self._graph[n] = g
+        g.replay()
+
+    def precapture(self, sizes):
+        """Capture the batch graphs of the given batch sizes ahead of serving (graphs=True)."""
+        if not self.graphs:
+            return
+        with torch.cuda.stream(self.stream):
+            for n in sizes:
+                if n in self._graph or not 0 < n <= self.max_samples:
+                    continue
+                chunks, begins = self._chunks(n)
+                self.d_begin[:len(begins)].copy_(torch.tensor(begins, dtype=torch.int32), non_blocking=False)
+                self.d_ids[:2 * n].zero_()
+                self._replay(n, chunks)
+        self.stream.synchronize()
+
     def launch(self, samples):
         """Enqueue one batch (list of (request id, sample index)); returns a Batch."""
         n = len(samples)
         assert 0 < n <= self.max_samples
-        eng, lib, L = self.engine, self.lib, self.dc.nslices
         chunks, begins = self._chunks(n)
         with torch.cuda.stream(self.stream):
-            st = self.stream.cuda_stream
             ids = torch.tensor([s[0] for s in samples] + [s[1] for s in samples] + begins,
                                dtype=torch.int32).pin_memory()
             self.d_begin[:len(begins)].copy_(ids[2 * n:], non_blocking=True)
             self.d_ids[:2 * n].copy_(ids[:2 * n], non_blocking=True)
-            _lib.check(lib.dcs_philox_prefixes(_lib.ptr(self.d_ids), _lib.ptr(self.d_ids) + 4 * n, n, self.key,
-                                               _lib.ptr(self.dc.closed), int(self.dc.closed.numel()),
-                                               _lib.ptr(self.d_x), _lib.ptr(self.d_u), st))
-            self.dc.build(lib, self.d_x, n, self.d_params, self.d_coefs, self.d_xors, st)
-            out = self.d_out[:n]
-            out.zero_()
-            entry = _lib.PARAM_DTYPE.itemsize
-            nm = eng._nmax() + 1
-            for c0, cn, b0, nb, boff in chunks:
-                eng._reset_items(cn)
-                eng._run_steps(_lib.ptr(self.d_params) + c0 * eng.nsteps * entry, cn)
-                _lib.check(lib.dcs_accumulate_batched(
-                    eng.dcode, _lib.ptr(eng.table), eng.table_stride, eng.plan.terminal_rank,
-                    eng.term_runs.ctypes.data, eng.term_nruns, eng.tbasis.ctypes.data,
-                    _lib.ptr(self.d_xors) + 8 * c0, _lib.ptr(self.d_coefs) + 16 * c0,
-                    _lib.ptr(self.d_begin) + 4 * boff, nb, eng.params.shift, _lib.ptr(eng.scale),
-                    _lib.ptr(eng.maxbits[nm - 1:]), nm, _lib.ptr(out[b0:b0 + nb]), self.k, cn, st))
-            _lib.check(lib.dcs_block_tail(_lib.ptr(out), self.k, eng.adj_hi.ctypes.data, eng.u_open.ctypes.data, n,
-                                          st))
-            _lib.check(lib.dcs_draw(_lib.ptr(out), self.k, n, _lib.ptr(self.d_u), _lib.ptr(self.d_scratch),
-                                    _lib.ptr(self.d_res), st))
+            if self.graphs:
+                self._replay(n, chunks)
+            else:
+                self._device_work(n, chunks)
             host = torch.empty(n * _lib.DRAW_DTYPE.itemsize, dtype=torch.uint8).pin_memory()
             host.copy_(self.d_res[:n * _lib.DRAW_DTYPE.itemsize], non_blocking=True)
             hx = torch.empty(n, dtype=torch.int64).pin_memory()
