@@ -31,10 +31,11 @@ REPO = Path(__file__).resolve().parent
 sys.path.insert(0, str(REPO))
 
 METRIC = "samples/s (64q, 2^20 block) served vs plain at c_y≥0.9999; p50/p99 ms"
-# DRAM traffic / algorithmic bytes of one k_fused launch, measured by ncu on a 2^27-universe group
-# of the same plan (profiles/k_fused_ring64_prefix_group23.md): full-size launches cannot be
-# captured with all counters, and the traffic of a group scales with the entries it touches.
-FUSED_TRAFFIC_RATIO = 0.9635
+# DRAM traffic / algorithmic bytes of one launch of the dominant kernel, measured by ncu on a
+# group of the same plan whose tables are 2^27-2^28 entries (profiles/k_runs_ring64_prefix_group21.md,
+# profiles/k_fused_ring64_prefix_group23.md): full-size launches cannot be captured with all
+# counters, and the traffic of a group scales with the entries it touches.
+TRAFFIC_RATIO = {"k_runs": 0.9823, "k_fused": 0.9635}
 FALLBACK_HBM = 6650.0
 
 
@@ -367,9 +368,10 @@ def gpu_arm(args):
                         "d2h_bytes_per_step": d2h},
                 "gpu_launches": launches,
                 "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
-                             "traffic": (FUSED_TRAFFIC_RATIO * dom["alg_bytes_per_launch"]
-                                         if dom["kernel"] == "k_fused" else None),
-                             "traffic_note": "ncu dram bytes of a 2^27-universe k_fused launch scaled by entries",
+                             "traffic": (TRAFFIC_RATIO[dom["kernel"]] * dom["alg_bytes_per_launch"]
+                                         if dom["kernel"] in TRAFFIC_RATIO else None),
+                             "traffic_note": "ncu dram bytes / algorithmic bytes of a smaller launch of the same "
+                                             "kernel and plan, times this launch's algorithmic bytes",
                              "kernel": dom["kernel"],
                              "peak_source": f"{how} (MEASURED_PEAKS.json hbm_gbs)" if how == "measured" else
                              "fallback 6650 GB/s", "launches": dom["launches"],
@@ -455,7 +457,7 @@ def kernel_roofline(eng, prep, out, stream):
             first, count = f.spans[g]
             alg = ((1 << len(plan.steps[first].active_in)) + (1 << len(plan.steps[first + count - 1].active_out))) * 8
             evs.append((a, b, alg))
-        kernel = "k_fused"
+        kernel = "k_runs" if f.tile_runs is not None and bool((f.groups["variant"] & 4).any()) else "k_fused"
     else:
         for s in range(eng.nsteps):
             a = torch.cuda.Event(enable_timing=True)
