@@ -35,7 +35,7 @@ METRIC = "samples/s (64q, 2^20 block) served vs plain at c_y≥0.9999; p50/p99 m
 # group of the same plan whose tables are 2^27-2^28 entries (profiles/k_runs_ring64_prefix_group21.md,
 # profiles/k_fused_ring64_prefix_group23.md): full-size launches cannot be captured with all
 # counters, and the traffic of a group scales with the entries it touches.
-TRAFFIC_RATIO = {"k_runs": 0.9823, "k_fused": 0.9635}
+TRAFFIC_RATIO = {"k_runs": 0.9823, "k_fused": 0.9635, "dcs_g (plan-specialised k_runs)": 0.9823}
 FALLBACK_HBM = 6650.0
 
 
@@ -55,6 +55,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--seed", type=int, default=24520)
     ap.add_argument("--tune", action="store_true", help="autotune the fused tile shape before timing")
+    ap.add_argument("--no-jit", action="store_true",
+                    help="run the library's register-run kernel instead of the plan-specialised group kernels")
     ap.add_argument("--serve", action="store_true", help="run the serving mix (32q/48q/64q) instead")
     ap.add_argument("--serve-seconds", type=float, default=20.0, help="arrival window of the serving run")
     ap.add_argument("--serve-rate", type=float, default=1.0, help="Poisson request rate (1/s)")
@@ -225,6 +227,8 @@ def gpu_arm(args):
     tune_report = None
     if args.mode == "fused" and args.tune:
         tune_report = eng.autotune()
+    if args.mode == "fused" and not args.no_jit and eng.fplan.tile_runs is not None:
+        eng.set_fused_config(jit=True)  # plan-specialised group kernels (NVRTC, cached cubins)
     setup_s = time.perf_counter() - t0
     k = eng.k
     total = args.warmup + args.steps
@@ -314,6 +318,8 @@ def gpu_arm(args):
         e2e_elapsed = float(t.item())
 
     fused_cfg = getattr(eng, "fused_config", None)
+    if fused_cfg is not None:
+        fused_cfg = {**fused_cfg, "jit": bool(getattr(eng.fplan, "jit", None))}
     eng_items = eng.items
     blocks64 = outs[args.warmup:total].clone()
     del eng, preps, outs  # release the 128 GiB table before the other engines allocate theirs
@@ -457,7 +463,8 @@ def kernel_roofline(eng, prep, out, stream):
             first, count = f.spans[g]
             alg = ((1 << len(plan.steps[first].active_in)) + (1 << len(plan.steps[first + count - 1].active_out))) * 8
             evs.append((a, b, alg))
-        kernel = "k_runs" if f.tile_runs is not None and bool((f.groups["variant"] & 4).any()) else "k_fused"
+        kernel = ("dcs_g (plan-specialised k_runs)" if f.jit is not None else "k_runs") \
+            if f.tile_runs is not None and bool((f.groups["variant"] & 4).any()) else "k_fused"
     else:
         for s in range(eng.nsteps):
             a = torch.cuda.Event(enable_timing=True)

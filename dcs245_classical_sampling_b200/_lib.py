@@ -74,6 +74,13 @@ SIGNATURES = {
     "dcs_philox_prefixes": (_I, [_P, _P, _I, _U64, _P, _I, _P, _P, _P]),
     "dcs_philox4x32_10_host": (None, [_P, ctypes.c_uint32, ctypes.c_uint32]),
     "dcs_build_items": (_I, [_P, _P, _P, _P, _P, _P, _P, _P, _I, _I, _I, _P, _I, _P, _P, _P, _P]),
+    "dcs_jit_compile": (_I, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, _I,
+                             ctypes.POINTER(_P), ctypes.POINTER(ctypes.c_size_t), ctypes.c_char_p, ctypes.c_size_t]),
+    "dcs_jit_free": (None, [_P]),
+    "dcs_jit_load": (_I, [_P, ctypes.POINTER(_P)]),
+    "dcs_jit_unload": (_I, [_P]),
+    "dcs_jit_kernel": (_I, [_P, ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(_P), ctypes.POINTER(_I)]),
+    "dcs_jit_launch": (_I, [_P, ctypes.c_uint, ctypes.c_size_t, _P, _P, _P, _P, _P]),
 }
 
 

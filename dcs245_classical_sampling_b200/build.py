@@ -16,8 +16,8 @@ REPO = PKG.parent
 CSRC = PKG / "csrc"
 INCLUDE = REPO / "include"
 LIB = PKG / "libdcs245.so"
-SOURCES = ["abi.cu", "step.cu", "fused.cu", "runs.cu", "runs_r4.cu", "runs_packed.cu", "block.cu", "draw.cu",
-           "serve.cu"]
+SOURCES = ["abi.cu", "step.cu", "fused.cu", "runs.cu", "runs_r4.cu", "runs_packed.cu", "jit.cu", "block.cu",
+           "draw.cu", "serve.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -57,7 +57,7 @@ def build(verbose=False, ptxas_info=False, force=False):
             raise RuntimeError(f"nvcc failed on {obj.stem}.cu:\n" + r.stdout + r.stderr)
         if verbose or ptxas_info:
             print(r.stdout + r.stderr)
-    cmd = [nvcc_path(), *ARCH, "-shared", "-o", str(LIB) + ".tmp", *[str(o) for o, _ in results]]
+    cmd = [nvcc_path(), *ARCH, "-shared", "-o", str(LIB) + ".tmp", *[str(o) for o, _ in results], "-lnvrtc"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError("nvcc link failed:\n" + r.stdout + r.stderr)

@@ -1,0 +1,312 @@
+// Plan-specialised register runs: the device header of the kernels that jit.py generates per
+// fused plan and compiles with NVRTC (sm_100a) at engine setup.
+//
+// The generated kernel of a group is k_runs (runs.cuh) with every plan quantity a compile-time
+// constant: tile shape, basis, coset runs, activity masks, and per run the coset
+// representatives' zero bits, the local offsets and, per step, the kind, the local bit(s), the
+// sign functional, the dead bits and the partner signs.  What stays at run time is the data of
+// the sample: the table, the step weights f0, f1, ov, y, and the renormalisation state.  There
+// is no dispatch in the step loop and every shared-memory offset of a coset is an immediate.
+//
+// Self-contained for NVRTC: no host headers.  The two structs below have the layout of
+// dcs_param and dcs_scale in include/dcs245.h (the library checks their sizes).
+#pragma once
+
+typedef unsigned int uint32_t;
+typedef unsigned long long uint64_t;
+typedef long long int64_t;
+typedef int int32_t;
+
+struct jit_param {
+    double f0r, f0i, f1r, f1i;
+    int32_t ov, y;
+};
+struct jit_scale {
+    double logscale;
+    int64_t exponent_sum;
+    uint32_t flags, pad;
+};
+
+#define JK_GROW 0
+#define JK_MIX 1
+#define JK_DIAG 2
+#define JK_REPLACE 3
+#define JK_FIXED 4
+#define JK_FIXED_SHRINK 5
+#define JK_SHRINK4 6
+#define JK_SHRINK2 7
+
+namespace jit {
+
+constexpr int kThreads = 256;
+constexpr uint32_t kSign = 0x80000000u;
+
+__host__ __device__ constexpr int cpar(int x) { return x ? ((x & 1) ^ cpar(x >> 1)) : 0; }
+
+__device__ __forceinline__ float2 f2(float x, float y) { return make_float2(x, y); }
+__device__ __forceinline__ float2 sflip(float2 a, uint32_t m) {
+    return f2(__uint_as_float(__float_as_uint(a.x) ^ m), __uint_as_float(__float_as_uint(a.y) ^ m));
+}
+// f * x
+__device__ __forceinline__ float2 zmul(float2 f, float2 x) {
+    return f2(fmaf(f.x, x.x, -f.y * x.y), fmaf(f.x, x.y, f.y * x.x));
+}
+// acc + f * x
+__device__ __forceinline__ float2 zmadd(float2 f, float2 x, float2 acc) {
+    return f2(fmaf(f.x, x.x, fmaf(-f.y, x.y, acc.x)), fmaf(f.x, x.y, fmaf(f.y, x.x, acc.y)));
+}
+__device__ __forceinline__ float2 zadd(float2 a, float2 b) { return f2(a.x + b.x, a.y + b.y); }
+// a + (-1)^NEG b
+template <int NEG>
+__device__ __forceinline__ float2 zaddg(float2 a, float2 b) {
+    if constexpr (NEG) return f2(a.x - b.x, a.y - b.y);
+    else return f2(a.x + b.x, a.y + b.y);
+}
+
+// ---------------------------------------------------------------- orbit bodies
+// One-vector kinds along local bit K: orbits {j, j | 2^K} for j with bit K clear and no DEAD
+// bit.  Sign of representative j: (-1)^(m0 + <j, B>), so F1p / F1n = s f1 for <j, B> even /
+// odd.  SK / SKA: the partner signs (-1)^sK, (-1)^sKa.  Formulas: the per-step kernel's
+// (reference: source/kernel_opt/inplace_gpu.py:29-58).
+template <int KIND, int R, int K, int B, int DEAD, int SK, int SKA, int J = 0>
+__device__ __forceinline__ void orb1(float2 (&v)[1 << R], float2 f0, float2 F1p, float2 F1n, float2 Fap, float2 Fan,
+                                     int y) {
+    if constexpr (J < (1 << R)) {
+        if constexpr (!(J & (1 << K)) && !(J & DEAD)) {
+            constexpr int D = J | (1 << K);
+            constexpr bool N = cpar(J & B);
+            const float2 F1 = N ? F1n : F1p;
+            const float2 x = v[J], b = v[D];
+            if constexpr (KIND == JK_GROW) {
+                v[J] = zmul(f0, x);
+                v[D] = zmul(F1, x);
+            } else if constexpr (KIND == JK_MIX) {
+                v[J] = zmadd(f0, x, zmul(N ? Fan : Fap, b));
+                v[D] = zmadd(f0, b, zmul(F1, x));
+            } else if constexpr (KIND == JK_REPLACE) {
+                v[J] = zmul(f0, zadd(x, b));
+                v[D] = zmul(F1, zaddg<SK>(x, b));
+            } else if constexpr (KIND == JK_FIXED_SHRINK) {
+                v[J] = y ? zmul(F1, zaddg<SK>(x, b)) : zmul(f0, zadd(x, b));
+            } else {  // JK_SHRINK2
+                v[J] = zmadd(f0, zadd(x, b), zmul(F1, zaddg<SK>(x, b)));
+            }
+        }
+        orb1<KIND, R, K, B, DEAD, SK, SKA, J + 1>(v, f0, F1p, F1n, Fap, Fan, y);
+    }
+}
+template <int KIND, int R, int K, int B, int DEAD, int SK, int SKA>
+__device__ __forceinline__ void body1(float2 (&v)[1 << R], float4 f, int y, uint32_t m0) {
+    const float2 f0 = f2(f.x, f.y), f1 = f2(f.z, f.w);
+    const float2 F1p = sflip(f1, m0), F1n = sflip(f1, m0 ^ kSign);
+    constexpr uint32_t ka = SKA ? kSign : 0u;
+    orb1<KIND, R, K, B, DEAD, SK, SKA>(v, f0, F1p, F1n, sflip(F1p, ka), sflip(F1n, ka), y);
+}
+
+// One-entry kinds: every local entry without a DEAD bit.
+template <int R, int B, int DEAD, int J = 0>
+__device__ __forceinline__ void orb0(float2 (&v)[1 << R], float2 Fp, float2 Fn) {
+    if constexpr (J < (1 << R)) {
+        if constexpr (!(J & DEAD)) v[J] = zmul(cpar(J & B) ? Fn : Fp, v[J]);
+        orb0<R, B, DEAD, J + 1>(v, Fp, Fn);
+    }
+}
+template <int KIND, int R, int B, int DEAD>
+__device__ __forceinline__ void body0(float2 (&v)[1 << R], float4 f, int y, uint32_t m0) {
+    const float2 f0 = f2(f.x, f.y), f1 = f2(f.z, f.w);
+    const float2 F1p = sflip(f1, m0), F1n = sflip(f1, m0 ^ kSign);
+    if constexpr (KIND == JK_DIAG) {  // (f0 + s f1) x
+        orb0<R, B, DEAD>(v, zadd(f0, F1p), zadd(f0, F1n));
+    } else {  // JK_FIXED: y ? s f1 x : f0 x
+        if (y) orb0<R, B, DEAD>(v, F1p, F1n);
+        else orb0<R, 0, DEAD>(v, f0, f0);
+    }
+}
+
+// Four-entry shrink along local bits K1 (K's role) and K2 (Ka's role); MIX bit 0: K's local
+// mask also has K2, bit 1: Ka's has K1.
+//   o_c = f0 (x + b) + s_d f1 (g + gK h) ;  o_{c^Ka} = f0 (g + h) + s_c f1 (x + gK b).
+template <int R, int K1, int K2, int MIX, int B, int DEAD, int SK, int J = 0>
+__device__ __forceinline__ void orb4(float2 (&v)[1 << R], float2 f0, float2 F1p, float2 F1n, float2 Fap, float2 Fan) {
+    if constexpr (J < (1 << R)) {
+        if constexpr (!(J & ((1 << K1) | (1 << K2))) && !(J & DEAD)) {
+            constexpr int MK = (1 << K1) | ((MIX & 1) ? (1 << K2) : 0);
+            constexpr int MKA = (1 << K2) | ((MIX & 2) ? (1 << K1) : 0);
+            constexpr bool N = cpar(J & B);
+            const float2 x = v[J], b = v[J ^ MK], g = v[J ^ MKA], h = v[J ^ MK ^ MKA];
+            v[J] = zmadd(f0, zadd(x, b), zmul(N ? Fan : Fap, zaddg<SK>(g, h)));
+            v[J ^ MKA] = zmadd(f0, zadd(g, h), zmul(N ? F1n : F1p, zaddg<SK>(x, b)));
+        }
+        orb4<R, K1, K2, MIX, B, DEAD, SK, J + 1>(v, f0, F1p, F1n, Fap, Fan);
+    }
+}
+template <int R, int K1, int K2, int MIX, int B, int DEAD, int SK, int SKA>
+__device__ __forceinline__ void body4(float2 (&v)[1 << R], float4 f, int y, uint32_t m0) {
+    const float2 f0 = f2(f.x, f.y), f1 = f2(f.z, f.w);
+    const float2 F1p = sflip(f1, m0), F1n = sflip(f1, m0 ^ kSign);
+    constexpr uint32_t ka = SKA ? kSign : 0u;
+    orb4<R, K1, K2, MIX, B, DEAD, SK>(v, f0, F1p, F1n, sflip(F1p, ka), sflip(F1n, ka));
+}
+
+// ---------------------------------------------------------------- group prologue, tiles, epilogue
+__device__ __forceinline__ int scale_exponent(double m2) {
+    if (!(m2 > 0.0) || !isfinite(m2)) return 0;
+    int e;
+    frexp(sqrt(m2), &e);
+    return e;
+}
+
+// Pass scale 2^-e from the previous pass's max (block 0 records it), the group's step weights
+// into shared memory, and the table of high tile-coordinate addresses.
+template <int TD, int LOW, int COUNT, int FIRST>
+__device__ __forceinline__ float prologue(const jit_param* __restrict__ params, const uint64_t* basis,
+                                          const unsigned long long* maxbits, int group, jit_scale* scale,
+                                          float4* fw, int* ovy, uint64_t* hi_tab) {
+    const double m2prev = (double)__uint_as_float((uint32_t)maxbits[group]);
+    const int e = scale_exponent(m2prev);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        scale->logscale += (double)e * 0.69314718055994530942;
+        scale->exponent_sum += e;
+        if (!isfinite(m2prev)) scale->flags |= 1u;
+        else if (m2prev == 0.0) scale->flags |= 2u;
+    }
+    if (threadIdx.x < COUNT) {
+        const jit_param p = params[FIRST + threadIdx.x];
+        fw[threadIdx.x] = make_float4((float)p.f0r, (float)p.f0i, (float)p.f1r, (float)p.f1i);
+        ovy[threadIdx.x] = (p.ov & 1) | ((p.y & 1) << 1);
+    }
+    for (int h = threadIdx.x; h < (1 << (TD - LOW)); h += kThreads) {
+        uint64_t a = 0;
+#pragma unroll
+        for (int i = 0; i < TD - LOW; ++i)
+            if ((h >> i) & 1) a ^= basis[i];
+        hi_tab[h] = a;
+    }
+    __syncthreads();
+    return (float)ldexp(1.0, -e);
+}
+
+// Tile load: entries active before the group (as runs.cuh: 4-entry segments when slot 0 is
+// active and rows have 4 entries or more, else 16-byte pairs or single entries, zero-filled).
+template <int T, int LOW, bool PAIR_IN>
+__device__ __forceinline__ void load_tile(const float2* __restrict__ E, float2* sh, const uint64_t* hi_tab,
+                                          uint64_t base, uint64_t in_inactive) {
+    constexpr uint64_t lowmask = (1ull << LOW) - 1;
+    if constexpr (PAIR_IN && LOW >= 2) {
+        const uint32_t rot = (threadIdx.x >> 2) & 1u;
+        const uint64_t seg_inactive = in_inactive & ~3ull;
+        const bool hi_pair_active = !(in_inactive & 2ull);
+        for (int q = threadIdx.x; q < (T >> 2); q += kThreads) {
+            const int t = q << 2;
+            const uint64_t a = base ^ hi_tab[t >> LOW] ^ ((uint64_t)t & lowmask);
+            if (a & seg_inactive) continue;
+            const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&sh[t]);
+            const float2* src = E + a;
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                const uint32_t cc = c ^ rot;
+                if (cc && !hi_pair_active) continue;
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst + 16u * cc), "l"(src + 2 * cc)
+                             : "memory");
+            }
+        }
+    } else if constexpr (PAIR_IN) {
+        for (int t = 2 * threadIdx.x; t < T; t += 2 * kThreads) {
+            const uint64_t a = base ^ hi_tab[t >> LOW] ^ ((uint64_t)t & lowmask);
+            const bool act = !(a & in_inactive);
+            const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&sh[t]);
+            const float2* src = act ? E + a : E;
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src), "r"(act ? 16 : 0)
+                         : "memory");
+        }
+    } else {
+        for (int t = threadIdx.x; t < T; t += kThreads) {
+            const uint64_t a = base ^ hi_tab[t >> LOW] ^ ((uint64_t)t & lowmask);
+            const bool act = !(a & in_inactive);
+            const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&sh[t]);
+            const float2* src = act ? E + a : E;
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(dst), "l"(src), "r"(act ? 8 : 0)
+                         : "memory");
+        }
+    }
+}
+
+// Tile store of the entries active after the group, scaled by the pass's 2^-e; returns the
+// running max |x|^2.
+template <int T, int LOW, bool PAIR_OUT>
+__device__ __forceinline__ float store_tile(float2* __restrict__ E, const float2* sh, const uint64_t* hi_tab,
+                                            uint64_t base, uint64_t out_inactive, float sc, float lm) {
+    constexpr uint64_t lowmask = (1ull << LOW) - 1;
+    if constexpr (PAIR_OUT && LOW >= 2) {
+        const uint32_t rot = (threadIdx.x >> 2) & 1u;
+        const uint64_t seg_inactive = out_inactive & ~3ull;
+        const bool hi_pair_active = !(out_inactive & 2ull);
+        for (int q = threadIdx.x; q < (T >> 2); q += kThreads) {
+            const int t = q << 2;
+            const uint64_t a = base ^ hi_tab[t >> LOW] ^ ((uint64_t)t & lowmask);
+            if (a & seg_inactive) continue;
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                const uint32_t cc = c ^ rot;
+                if (cc && !hi_pair_active) continue;
+                const float4 u = *reinterpret_cast<const float4*>(&sh[t + 2 * cc]);
+                const float4 v = make_float4(u.x * sc, u.y * sc, u.z * sc, u.w * sc);
+                lm = fmaxf(lm, fmaxf(v.x * v.x + v.y * v.y, v.z * v.z + v.w * v.w));
+                *reinterpret_cast<float4*>(E + a + 2 * cc) = v;
+            }
+        }
+    } else if constexpr (PAIR_OUT) {
+        for (int t = 2 * threadIdx.x; t < T; t += 2 * kThreads) {
+            const uint64_t a = base ^ hi_tab[t >> LOW] ^ ((uint64_t)t & lowmask);
+            if (a & out_inactive) continue;
+            const float4 q = *reinterpret_cast<const float4*>(&sh[t]);
+            const float4 v = make_float4(q.x * sc, q.y * sc, q.z * sc, q.w * sc);
+            lm = fmaxf(lm, fmaxf(v.x * v.x + v.y * v.y, v.z * v.z + v.w * v.w));
+            *reinterpret_cast<float4*>(E + a) = v;
+        }
+    } else {
+        for (int t = threadIdx.x; t < T; t += kThreads) {
+            const uint64_t a = base ^ hi_tab[t >> LOW] ^ ((uint64_t)t & lowmask);
+            if (a & out_inactive) continue;
+            const float2 v = f2(sh[t].x * sc, sh[t].y * sc);
+            lm = fmaxf(lm, v.x * v.x + v.y * v.y);
+            E[a] = v;
+        }
+    }
+    return lm;
+}
+
+// Tile-constant sign parts parity(base & beta_s) ^ ov_s, one bit per step (warp 0).
+template <int COUNT>
+__device__ __forceinline__ void sign_bits(const uint64_t* beta, uint64_t base, const int* ovy, uint32_t* cs_sh) {
+    if (threadIdx.x < 32) {
+        const int s = threadIdx.x;
+        const int bit = s < COUNT ? ((__popcll(base & beta[s]) & 1) ^ (ovy[s] & 1)) : 0;
+        const uint32_t m = __ballot_sync(0xffffffffu, bit);
+        if (s == 0) *cs_sh = m;
+    }
+}
+
+__device__ __forceinline__ void block_max(float lm, unsigned long long* maxbits, int slot) {
+    __shared__ unsigned long long red[32];
+    unsigned long long v = (unsigned long long)__float_as_uint(lm);
+    for (int off = 16; off > 0; off >>= 1) {
+        const unsigned long long o = __shfl_xor_sync(0xffffffffu, v, off);
+        v = o > v ? o : v;
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        v = lane < (kThreads >> 5) ? red[lane] : 0ull;
+        for (int off = 16; off > 0; off >>= 1) {
+            const unsigned long long o = __shfl_xor_sync(0xffffffffu, v, off);
+            v = o > v ? o : v;
+        }
+        if (lane == 0 && v) atomicMax(&maxbits[slot], v);
+    }
+}
+
+__device__ __forceinline__ uint32_t ins0(uint32_t o, int p) { return ((o >> p) << (p + 1)) | (o & ((1u << p) - 1u)); }
+
+}  // namespace jit

@@ -175,14 +175,16 @@ class InplaceConditionalBlockGPU:
 
     # ------------------------------------------------------------------ allocation
     def alloc(self, dtype=np.complex64, device=0, fp64_kernel_path=None, mode=None, items=None,
-              hbm_budget=None):
+              hbm_budget=None, jit=False):
         """Allocate device buffers (conditional_block_inplace_gpu.py:18-34).
 
         dtype: complex64 (FP32 arithmetic) or complex128 (FP64 arithmetic).
         mode: "plain", "device" or "fused" (default: fused for complex64 tables of 2^26 entries
         and more, device otherwise).
         items: concurrent work items (slices) per launch; default = as many slices as fit
-        in the HBM budget (default 85% of free device memory)."""
+        in the HBM budget (default 85% of free device memory).
+        jit: in fused mode with register runs, run the groups as plan-specialised kernels
+        compiled for this plan with NVRTC (jit.py)."""
         if np.dtype(dtype) not in (np.dtype(np.complex64), np.dtype(np.complex128)):
             raise ValueError(dtype)
         if mode is None:  # fused passes pay off once the tables are far larger than a tile
@@ -222,7 +224,8 @@ class InplaceConditionalBlockGPU:
             self.fused_config = {"max_dim": cfg.get("max_dim", 13), "low": cfg.get("low", 4),
                                  "max_steps": cfg.get("max_steps", 24), "variant": cfg.get("variant", 0),
                                  "pairs": cfg.get("pairs", False)}
-            self.fplan = build_fused_plan(plan, **self.fused_config)
+            self.jit = bool(jit)
+            self.fplan = self._build_fplan()
             self.items = 1
         self.table = torch.empty(self.items * table_entries, dtype=tdtype, device=self.device)
         self.table_stride = table_entries
@@ -254,13 +257,25 @@ class InplaceConditionalBlockGPU:
     def _nmax(self):
         return len(self.fplan.groups) if self.mode == "fused" else self.nsteps
 
-    def set_fused_config(self, **cfg):
-        """Rebuild the fused plan with another tile shape (max_dim, low, max_steps, variant, pairs)."""
+    def _build_fplan(self):
+        """The fused plan of fused_config; with self.jit and register runs, its groups run as
+        plan-specialised kernels (jit.py) compiled for this plan."""
         from .fused import build_fused_plan
+        fp = build_fused_plan(self.plan, **self.fused_config)
+        if getattr(self, "jit", False) and fp.tile_runs is not None:
+            from .jit import JitPlan
+            fp.jit = JitPlan(self.plan, fp, self.lib)
+        return fp
+
+    def set_fused_config(self, jit=None, **cfg):
+        """Rebuild the fused plan with another tile shape (max_dim, low, max_steps, variant, pairs);
+        jit=True/False switches the plan-specialised group kernels on or off."""
         if self.mode != "fused":
             raise ValueError("set_fused_config needs mode='fused'")
+        if jit is not None:
+            self.jit = bool(jit)
         self.fused_config = {**self.fused_config, **cfg}
-        self.fplan = build_fused_plan(self.plan, **self.fused_config)
+        self.fplan = self._build_fplan()
         self.maxbits = torch.zeros(self.items * (len(self.fplan.groups) + 1), dtype=torch.int64, device=self.device)
 
     def autotune(self, x_bits=None, candidates=None):

@@ -85,6 +85,7 @@ class FusedPlan:
     tile_steps: np.ndarray
     dsteps: np.ndarray
     tile_runs: np.ndarray = None
+    jit: object = None  # jit.JitPlan: plan-specialised group kernels (loaded), or None
     spans: list = field(default_factory=list)      # (first, count) per group
     universe: list = field(default_factory=list)   # |U| per group
     tiles: list = field(default_factory=list)      # tile count per group
@@ -92,6 +93,12 @@ class FusedPlan:
 
     def launch(self, lib, table, params, g0, ng, maxbits, scale, stream):
         """Run groups [g0, g0 + ng) (device pointers as ints); returns the library status."""
+        if self.jit is not None:
+            return self.jit.launch(table, params, g0, ng, maxbits, scale, stream)
+        return self.launch_library(lib, table, params, g0, ng, maxbits, scale, stream)
+
+    def launch_library(self, lib, table, params, g0, ng, maxbits, scale, stream):
+        """The library kernels (register runs where the groups have them)."""
         if self.tile_runs is not None:
             return lib.dcs_fused_runs(table, self.dsteps.ctypes.data, len(self.dsteps), self.groups.ctypes.data,
                                       len(self.groups), self.tile_steps.ctypes.data, self.tile_runs.ctypes.data,

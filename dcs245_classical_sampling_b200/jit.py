@@ -1,0 +1,260 @@
+"""Plan-specialised group kernels.
+
+A fused plan with register runs (``fused.build_fused_plan(..., variant=4 or 12)``) fixes, for
+every group, the tile shape, the basis, the coset runs, the activity masks and, per run and step,
+everything the register-run kernel (``csrc/runs.cuh``) reads from its arguments and dispatches
+on at run time.  ``group_source`` writes one CUDA kernel per group with all of that as
+constants (device header ``csrc/runs_jit.cuh``): no dispatch in the step loop, compile-time
+dead masks and partner signs, immediate shared-memory offsets.  ``JitPlan`` compiles the
+kernels with NVRTC for sm_100a through the library (``dcs_jit_compile``), caches the cubin by
+source hash, loads it and launches a group exactly as ``dcs_fused_runs`` would.  Groups without
+register runs keep the library kernel.
+"""
+from __future__ import annotations
+
+import ctypes
+import hashlib
+import os
+from concurrent.futures import ThreadPoolExecutor
+from pathlib import Path
+
+import numpy as np
+
+from . import _lib
+from .plan import orbit_kind
+
+HERE = Path(__file__).resolve().parent
+HEADER = HERE / "csrc" / "runs_jit.cuh"
+CACHE_DIR = HERE / "_jit_cache"
+KERNEL_VERSION = 1  # bump when the generated code changes meaning
+
+ONE_VECTOR = (0, 1, 3, 5, 7)
+
+
+def _u64(x):
+    return f"{int(x) & 0xFFFFFFFFFFFFFFFF}ull"
+
+
+def _beff(kind, ts, R):
+    ptab = int(ts["ptab"])
+    bl = sum(((ptab >> (1 << k)) & 1) << k for k in range(R))
+    own = 0
+    if kind in ONE_VECTOR:
+        own = 1 << int(ts["rk1"])
+    elif kind == 6:
+        own = (1 << int(ts["rk1"])) | (1 << int(ts["rk2"]))
+    return bl & ~own
+
+
+def _deposit_expr(g):
+    terms = []
+    for r in range(int(g["ncoset_runs"])):
+        w = int(g["coset_runs"][r])
+        src, dst, ln = w & 255, (w >> 8) & 255, (w >> 16) & 255
+        mask = (1 << 64) - 1 if ln >= 64 else (1 << ln) - 1
+        terms.append(f"(((tile >> {src}) & {_u64(mask)}) << {dst})")
+    return " | ".join(terms) if terms else "0ull"
+
+
+def group_source(plan, fp, gi, minb=3):
+    """CUDA source of the kernel of group gi (``dcs_g<gi>``); None if the group has no runs."""
+    g = fp.groups[gi]
+    if not int(g["variant"]) & 4:
+        return None
+    R = 4 if int(g["variant"]) & 8 else 3
+    first, count = int(g["first"]), int(g["count"])
+    TD, LOW = int(g["tile_dim"]), int(g["low_bits"])
+    T = 1 << TD
+    in_mask = int(fp.dsteps[first]["in_mask"])
+    out_mask = int(g["out_mask"])
+    pair_in = LOW >= 1 and (in_mask & 1)
+    pair_out = LOW >= 1 and (out_mask & 1)
+    nb = max(1, TD - LOW)
+    basis = ", ".join(_u64(g["basis"][i]) for i in range(nb))
+    betas = ", ".join(_u64(fp.dsteps[first + s]["beta"]) for s in range(count))
+    L = []
+    L.append(f"__constant__ uint64_t g{gi}_basis[{nb}] = {{{basis}}};")
+    L.append(f"__constant__ uint64_t g{gi}_beta[{count}] = {{{betas}}};")
+    L.append(f'extern "C" __global__ void __launch_bounds__(256, {minb})')
+    L.append(f"dcs_g{gi}(float2* __restrict__ E, const jit_param* __restrict__ params, "
+             "unsigned long long* __restrict__ maxbits, jit_scale* __restrict__ scale) {")
+    L.append(f"    constexpr int TD = {TD}, LOW = {LOW}, T = 1 << TD, COUNT = {count}, FIRST = {first};")
+    L.append("    extern __shared__ __align__(16) unsigned char smem[];")
+    L.append("    float2* sh = reinterpret_cast<float2*>(smem);")
+    L.append("    uint64_t* hi_tab = reinterpret_cast<uint64_t*>(smem + sizeof(float2) * T);")
+    L.append("    __shared__ float4 fw[COUNT];")
+    L.append("    __shared__ int ovy[COUNT];")
+    L.append("    __shared__ uint32_t cs_sh;")
+    L.append(f"    const float sc = jit::prologue<TD, LOW, COUNT, FIRST>(params, g{gi}_basis, maxbits, {gi}, scale, "
+             "fw, ovy, hi_tab);")
+    L.append("    float lm = 0.f;")
+    L.append(f"    for (uint64_t tile = blockIdx.x; tile < {_u64(1 << int(g['coset_m']))}; tile += gridDim.x) {{")
+    L.append(f"        const uint64_t base = {_deposit_expr(g)};")
+    L.append(f"        jit::load_tile<T, LOW, {'true' if pair_in else 'false'}>(E, sh, hi_tab, base, "
+             f"{_u64(~in_mask)});")
+    L.append(f"        jit::sign_bits<COUNT>(g{gi}_beta, base, ovy, &cs_sh);")
+    L.append('        asm volatile("cp.async.wait_all;\\n" ::: "memory");')
+    L.append("        __syncthreads();")
+    L.append("        const uint32_t csm = cs_sh;")
+    L.append("        unsigned char* shb = smem;")
+    s = 0
+    while s < count:
+        ts0 = fp.tile_steps[first + s]
+        tr = fp.tile_runs[first + s]
+        n = int(ts0["run_len"])
+        if n < 1 or int(tr["count"]) != n or int(tr["r"]) != R:
+            raise ValueError(f"group {gi}: malformed run at step {first + s}")
+        nins = int(tr["nins"])
+        ins = [int(x) for x in tr["ins"][:nins]]
+        NB = T >> nins
+        niter = NB >> 8 if NB > 256 else 1
+        mhi3 = int(tr["mhi"]) << 3
+        offs = [int(tr["off"][j]) << 3 for j in range(1 << R)]
+        L.append(f"        // run: steps {first + s}..{first + s + n - 1}, {NB} cosets of {1 << R} entries")
+        L.append(f"        if (!(base & {_u64(ts0['cskip'])})) {{")
+        L.append(f"            if ((int)threadIdx.x < {NB}) {{")
+        L.append("                uint32_t tp = threadIdx.x;")
+        for p in ins:
+            L.append(f"                tp = jit::ins0(tp, {p});")
+        L.append("                tp <<= 3;")
+        L.append("                uint32_t tu = 0;")
+        L.append("#pragma unroll 1")
+        L.append(f"                for (int k = 0; k < {niter}; ++k) {{")
+        L.append("                    const uint32_t t0 = tp | tu;")
+        L.append(f"                    tu = ((tu | ~{mhi3}u) + 1u) & {mhi3}u;")
+        L.append(f"                    float2 v[{1 << R}];")
+        for j, o in enumerate(offs):
+            L.append(f"                    v[{j}] = *reinterpret_cast<const float2*>(shb + (t0 ^ {o}u));")
+        for i in range(n):
+            si = s + i
+            st = fp.tile_steps[first + si]
+            kind = int(fp.dsteps[first + si]["kind"])
+            B = _beff(kind, st, R)
+            dead = int(st["rdead"])
+            sk, ska = int(st["sK"]) & 1, int(st["sKa"]) & 1
+            k1, k2, mix = int(st["rk1"]), int(st["rk2"]), int(st["rmix"])
+            tb3 = (int(st["tbeta"]) << 3) & 0xFFFFFFFF
+            m0 = f"(((uint32_t)__popc(t0 & {tb3}u) ^ (csm >> {si})) & 1u) << 31"
+            args = f"(v, fw[{si}], ovy[{si}] >> 1, {m0})"
+            if kind in ONE_VECTOR:
+                call = f"jit::body1<{kind}, {R}, {k1}, {B}, {dead}, {sk}, {ska}>{args};"
+            elif kind in (2, 4):
+                call = f"jit::body0<{kind}, {R}, {B}, {dead}>{args};"
+            else:
+                call = f"jit::body4<{R}, {k1}, {k2}, {mix}, {B}, {dead}, {sk}, {ska}>{args};"
+            L.append(f"                    {call}")
+        for j, o in enumerate(offs):
+            L.append(f"                    *reinterpret_cast<float2*>(shb + (t0 ^ {o}u)) = v[{j}];")
+        L.append("                }")
+        L.append("            }")
+        L.append("        }")
+        L.append("        __syncthreads();")
+        s += n
+    L.append(f"        lm = jit::store_tile<T, LOW, {'true' if pair_out else 'false'}>(E, sh, hi_tab, base, "
+             f"{_u64(~out_mask)}, sc, lm);")
+    L.append("        __syncthreads();")
+    L.append("    }")
+    L.append(f"    jit::block_max(lm, maxbits, {gi + 1});")
+    L.append("}")
+    return "\n".join(L) + "\n"
+
+
+def plan_sources(plan, fp, minb=3, parts=8):
+    """Translation units (source strings) holding the group kernels, spread over `parts` units
+    so that NVRTC compiles them in parallel; returns [(source, [group indices])]."""
+    groups = [gi for gi in range(len(fp.groups)) if int(fp.groups[gi]["variant"]) & 4]
+    # balance by generated size
+    bodies = {gi: group_source(plan, fp, gi, minb) for gi in groups}
+    units = [([], 0) for _ in range(max(1, min(parts, len(groups))))]
+    for gi in sorted(groups, key=lambda q: -len(bodies[q])):
+        k = min(range(len(units)), key=lambda u: units[u][1])
+        units[k] = (units[k][0] + [gi], units[k][1] + len(bodies[gi]))
+    out = []
+    for gis, _ in units:
+        if not gis:
+            continue
+        src = '#include "runs_jit.cuh"\n\n' + "\n".join(bodies[gi] for gi in sorted(gis))
+        out.append((src, sorted(gis)))
+    return out
+
+
+def compile_source(lib, source, name="dcs_plan.cu"):
+    """Cubin of one translation unit (NVRTC, sm_100a), cached on disk by source hash."""
+    header = HEADER.read_text()
+    key = hashlib.sha256(f"{KERNEL_VERSION}\0{header}\0{source}".encode()).hexdigest()[:32]
+    path = CACHE_DIR / f"{key}.cubin"
+    if path.exists():
+        return path.read_bytes()
+    img = ctypes.c_void_p()
+    size = ctypes.c_size_t()
+    log = ctypes.create_string_buffer(1 << 16)
+    rc = lib.dcs_jit_compile(source.encode(), name.encode(), header.encode(), b"runs_jit.cuh", 1,
+                             ctypes.byref(img), ctypes.byref(size), log, len(log))
+    if rc != 0:
+        raise _lib.DCSError(rc, lib.dcs_last_error().decode() + "\n" + log.value.decode(errors="replace"))
+    data = ctypes.string_at(img.value, size.value)
+    lib.dcs_jit_free(img)
+    try:
+        CACHE_DIR.mkdir(exist_ok=True)
+        tmp = path.with_suffix(f".{os.getpid()}.tmp")
+        tmp.write_bytes(data)
+        os.replace(tmp, path)
+    except OSError:
+        pass
+    return data
+
+
+def compile_plan(plan, fp, lib=None, minb=3, parts=8):
+    """[(cubin, [group indices])] for a fused plan (NVRTC in parallel threads)."""
+    lib = lib or _lib.load()
+    units = plan_sources(plan, fp, minb, parts)
+    with ThreadPoolExecutor(max_workers=len(units) or 1) as ex:
+        images = list(ex.map(lambda u: compile_source(lib, u[0], f"dcs_plan_{u[1][0]}.cu"), units))
+    return [(img, gis) for img, (_, gis) in zip(images, units)]
+
+
+class JitPlan:
+    """Loaded group kernels of one fused plan (current CUDA device)."""
+
+    def __init__(self, plan, fp, lib=None, minb=3, parts=8):
+        self.lib = lib or _lib.load()
+        self.fp = fp
+        self.kernels = {}
+        self._libs = []
+        self._images = []
+        sms = self.lib.dcs_sm_count()
+        for img, gis in compile_plan(plan, fp, self.lib, minb, parts):
+            buf = ctypes.create_string_buffer(img, len(img))
+            self._images.append(buf)
+            handle = ctypes.c_void_p()
+            _lib.check(self.lib.dcs_jit_load(ctypes.cast(buf, ctypes.c_void_p), ctypes.byref(handle)))
+            self._libs.append(handle)
+            for gi in gis:
+                g = fp.groups[gi]
+                td, low = int(g["tile_dim"]), int(g["low_bits"])
+                smem = 8 * (1 << td) + 8 * (1 << (td - low))
+                k = ctypes.c_void_p()
+                per_sm = ctypes.c_int()
+                _lib.check(self.lib.dcs_jit_kernel(handle, f"dcs_g{gi}".encode(), smem, ctypes.byref(k),
+                                                   ctypes.byref(per_sm)))
+                grid = min(sms * max(1, per_sm.value), 1 << int(g["coset_m"]))
+                self.kernels[gi] = (k, grid, smem)
+
+    def launch(self, table, params, g0, ng, maxbits, scale, stream):
+        """Groups [g0, g0 + ng) on `stream` (ints: device pointers); library status."""
+        for gi in range(g0, g0 + ng):
+            kern = self.kernels.get(gi)
+            if kern is None:
+                rc = self.fp.launch_library(self.lib, table, params, gi, 1, maxbits, scale, stream)
+            else:
+                k, grid, smem = kern
+                rc = self.lib.dcs_jit_launch(k, grid, smem, table, params, maxbits, scale, stream)
+            if rc != 0:
+                return rc
+        return 0
+
+    def close(self):
+        for h in self._libs:
+            self.lib.dcs_jit_unload(h)
+        self._libs = []
+        self.kernels = {}

@@ -232,6 +232,23 @@ int dcs_fused_runs(void *table, const dcs_step *steps, int nsteps, const dcs_gro
                    const dcs_tile_step *tile_steps, const dcs_tile_run *tile_runs, const dcs_param *params,
                    int g0, int ng, uint64_t *maxbits, dcs_scale *scale, void *stream);
 
+/* Plan-specialised group kernels (no reference counterpart: the reference's kernels are fixed
+ * sources compiled once).  A fused plan with register runs is turned into one CUDA kernel per
+ * group with every plan quantity a constant (generator: jit.py, device header: runs_jit.cuh).
+ * dcs_jit_compile compiles CUDA source for sm_100a with NVRTC into a cubin image (release with
+ * dcs_jit_free); `log` receives the compiler log.  dcs_jit_load loads an image through the
+ * runtime library API.  dcs_jit_kernel looks up a kernel, allows it `smem` bytes of dynamic
+ * shared memory and returns its resident blocks per SM.  dcs_jit_launch runs it with 256
+ * threads per block on (table, params, maxbits, scale), as dcs_fused_runs runs one group. */
+int dcs_jit_compile(const char *source, const char *name, const char *header_source, const char *header_name,
+                    int lineinfo, void **image, size_t *image_size, char *log, size_t log_capacity);
+void dcs_jit_free(void *image);
+int dcs_jit_load(const void *image, void **library);
+int dcs_jit_unload(void *library);
+int dcs_jit_kernel(void *library, const char *name, size_t smem, void **kernel, int *blocks_per_sm);
+int dcs_jit_launch(void *kernel, unsigned grid, size_t smem, void *table, const dcs_param *params, uint64_t *maxbits,
+                   dcs_scale *scale, void *stream);
+
 /* Terminal gather + syndrome scatter + coherent slice accumulation into complex128 blocks.
  * For output block b, items item_begin[b] .. item_begin[b+1]-1 (slices, in slice order) add
  *   total_b[synd(i) ^ xors[it]] += env_it(i) * (coefs[2it] + i coefs[2it+1]) * exp(logscale_it - log_shift)

@@ -78,6 +78,24 @@ def test_fused_kernel_variants_match_reference(golden, name, variant):
         assert rel_l2(v.cpu().numpy(), arrays[f"block_{rec['sample_id']}"]) < 1e-5
 
 
+@pytest.mark.parametrize("name", ["c1", "small", "c2"])
+@pytest.mark.parametrize("variant", [4, 12])
+def test_plan_specialised_kernels_match_reference(golden, name, variant):
+    """Group kernels generated and compiled for the plan (jit.py) against the reference blocks,
+    and against the library's register-run kernel on the same configuration."""
+    case, arrays = golden(name)
+    eng = _engine(case, arrays, np.complex64, mode="fused")
+    eng.set_fused_config(variant=variant, pairs=False, max_dim=13, low=4, jit=False)
+    lib_blocks = [eng.block(_x(rec))[0].cpu().numpy() for rec in case["protocol"]["records"]]
+    eng.set_fused_config(jit=True)
+    assert eng.fplan.jit is not None and eng.fplan.jit.kernels
+    for rec, lb in zip(case["protocol"]["records"], lib_blocks):
+        v, _ = eng.block(_x(rec))
+        v = v.cpu().numpy()
+        assert rel_l2(v, arrays[f"block_{rec['sample_id']}"]) < 1e-5
+        assert rel_l2(v, lb) < 1e-6
+
+
 def test_one_item_at_a_time_equals_batched_slices(golden):
     case, arrays = golden("small")
     a = _engine(case, arrays, np.complex128, items=1)
