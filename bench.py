@@ -226,9 +226,9 @@ def gpu_arm(args):
     eng.alloc(np.complex64, device=local, mode=args.mode)
     tune_report = None
     if args.mode == "fused" and args.tune:
-        tune_report = eng.autotune()
-    if args.mode == "fused" and not args.no_jit and eng.fplan.tile_runs is not None:
-        eng.set_fused_config(jit=True)  # plan-specialised group kernels (NVRTC, cached cubins)
+        tune_report = eng.autotune(jit=not args.no_jit)
+    if args.mode == "fused" and eng.fplan.tile_runs is not None and eng.jit == args.no_jit:
+        eng.set_fused_config(jit=not args.no_jit)  # plan-specialised group kernels (NVRTC, cached cubins)
     setup_s = time.perf_counter() - t0
     k = eng.k
     total = args.warmup + args.steps

@@ -44,10 +44,19 @@ def cached(plan, device_name):
     return _load().get(f"{fingerprint(plan)}|{device_name}")
 
 
-def tune(engine, params_dev, candidates=CANDIDATES, repeats=1, save=True):
+# with plan-specialised group kernels (jit.py; scalar register runs, so no packed variants)
+JIT_CANDIDATES = [(13, 3, 24, 12, False), (13, 4, 24, 12, False), (13, 3, 24, 4, False), (13, 4, 24, 4, False),
+                  (13, 3, 24, 13, False), (13, 5, 24, 12, False), (12, 3, 24, 12, False), (13, 3, 16, 12, False),
+                  (14, 4, 24, 13, False)]
+
+
+def tune(engine, params_dev, candidates=None, repeats=1, save=True, jit=False):
     """Time each candidate on the engine (mode "fused", already allocated) and install the best.
 
-    params_dev: device params of one work item (nsteps dcs_param).  Returns the report."""
+    params_dev: device params of one work item (nsteps dcs_param).  jit: time the candidates
+    as plan-specialised group kernels.  Returns the report."""
+    if candidates is None:
+        candidates = JIT_CANDIDATES if jit else CANDIDATES
     import torch
     from .fused import build_fused_plan
     lib = engine.lib
@@ -61,6 +70,9 @@ def tune(engine, params_dev, candidates=CANDIDATES, repeats=1, save=True):
                                   pairs=pairs)
         except ValueError:
             continue
+        if jit and fp.tile_runs is not None:
+            from .jit import JitPlan
+            fp.jit = JitPlan(engine.plan, fp, lib)
         need = len(fp.groups) + 1
         if engine.maxbits.numel() < need:
             engine.maxbits = torch.zeros(need, dtype=torch.int64, device=engine.device)
@@ -81,9 +93,13 @@ def tune(engine, params_dev, candidates=CANDIDATES, repeats=1, save=True):
             times.append(a.elapsed_time(b) / 1000.0)
         t = min(times[1:]) if len(times) > 1 else times[0]
         report.append({"max_dim": max_dim, "low": low, "max_steps": max_steps, "variant": variant,
-                       "pairs": pairs, "groups": len(fp.groups), "seconds": t})
+                       "pairs": pairs, "jit": fp.jit is not None, "groups": len(fp.groups), "seconds": t})
         if best is None or t < best[0]:
+            if best is not None and best[2].jit is not None:
+                best[2].jit.close()
             best = (t, cand, fp)
+        elif fp.jit is not None:
+            fp.jit.close()
     engine.fplan = best[2]
     nm = len(best[2].groups) + 1
     engine.maxbits = torch.zeros(engine.items * nm, dtype=torch.int64, device=engine.device)
@@ -91,10 +107,11 @@ def tune(engine, params_dev, candidates=CANDIDATES, repeats=1, save=True):
         data = _load()
         data[f"{fingerprint(engine.plan)}|{torch.cuda.get_device_name(engine.device)}"] = {
             "max_dim": best[1][0], "low": best[1][1], "max_steps": best[1][2], "variant": best[1][3],
-            "pairs": best[1][4], "seconds": best[0]}
+            "pairs": best[1][4], "jit": best[2].jit is not None, "seconds": best[0]}
         try:
             CACHE.write_text(json.dumps(data, indent=1) + "\n")
         except OSError:
             pass
     return {"best": {"max_dim": best[1][0], "low": best[1][1], "max_steps": best[1][2], "variant": best[1][3],
-                     "pairs": best[1][4], "seconds": best[0]}, "candidates": report}
+                     "pairs": best[1][4], "jit": best[2].jit is not None, "seconds": best[0]},
+            "candidates": report}

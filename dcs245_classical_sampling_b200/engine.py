@@ -175,7 +175,7 @@ class InplaceConditionalBlockGPU:
 
     # ------------------------------------------------------------------ allocation
     def alloc(self, dtype=np.complex64, device=0, fp64_kernel_path=None, mode=None, items=None,
-              hbm_budget=None, jit=False):
+              hbm_budget=None, jit=None):
         """Allocate device buffers (conditional_block_inplace_gpu.py:18-34).
 
         dtype: complex64 (FP32 arithmetic) or complex128 (FP64 arithmetic).
@@ -184,7 +184,8 @@ class InplaceConditionalBlockGPU:
         items: concurrent work items (slices) per launch; default = as many slices as fit
         in the HBM budget (default 85% of free device memory).
         jit: in fused mode with register runs, run the groups as plan-specialised kernels
-        compiled for this plan with NVRTC (jit.py)."""
+        compiled for this plan with NVRTC (jit.py); default: the tuned setting of this plan and
+        device (autotune_cache.json), else off."""
         if np.dtype(dtype) not in (np.dtype(np.complex64), np.dtype(np.complex128)):
             raise ValueError(dtype)
         if mode is None:  # fused passes pay off once the tables are far larger than a tile
@@ -224,7 +225,7 @@ class InplaceConditionalBlockGPU:
             self.fused_config = {"max_dim": cfg.get("max_dim", 13), "low": cfg.get("low", 4),
                                  "max_steps": cfg.get("max_steps", 24), "variant": cfg.get("variant", 0),
                                  "pairs": cfg.get("pairs", False)}
-            self.jit = bool(jit)
+            self.jit = bool(cfg.get("jit", False) if jit is None else jit)
             self.fplan = self._build_fplan()
             self.items = 1
         self.table = torch.empty(self.items * table_entries, dtype=tdtype, device=self.device)
@@ -278,15 +279,20 @@ class InplaceConditionalBlockGPU:
         self.fplan = self._build_fplan()
         self.maxbits = torch.zeros(self.items * (len(self.fplan.groups) + 1), dtype=torch.int64, device=self.device)
 
-    def autotune(self, x_bits=None, candidates=None):
-        """Time the fused tile-shape candidates on this engine's table and keep the fastest."""
+    def autotune(self, x_bits=None, candidates=None, jit=None):
+        """Time the fused tile-shape candidates on this engine's table and keep the fastest
+        (jit: as plan-specialised group kernels; default: the engine's setting)."""
         from . import autotune as at
         if self.mode != "fused":
             return None
         x = np.zeros(self.n, np.uint8) if x_bits is None else x_bits
         _, items = self.params.items(x)
         prm = torch.from_numpy(items[0][1].view(np.int64).copy()).to(self.device)
-        rep = at.tune(self, prm, **({"candidates": candidates} if candidates else {}))
+        jit = self.jit if jit is None else bool(jit)
+        if self.fplan.jit is not None:
+            self.fplan.jit.close()
+        rep = at.tune(self, prm, jit=jit, **({"candidates": candidates} if candidates else {}))
+        self.jit = jit
         self.fused_config = {k: rep["best"][k] for k in ("max_dim", "low", "max_steps", "variant", "pairs")}
         self.scale = torch.zeros(self.items * _lib.SCALE_DTYPE.itemsize // 8, dtype=torch.int64,
                                  device=self.device)

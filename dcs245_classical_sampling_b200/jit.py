@@ -18,10 +18,7 @@ import os
 from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
-import numpy as np
-
 from . import _lib
-from .plan import orbit_kind
 
 HERE = Path(__file__).resolve().parent
 HEADER = HERE / "csrc" / "runs_jit.cuh"
@@ -216,12 +213,16 @@ def compile_plan(plan, fp, lib=None, minb=3, parts=8):
 class JitPlan:
     """Loaded group kernels of one fused plan (current CUDA device)."""
 
-    def __init__(self, plan, fp, lib=None, minb=3, parts=8):
+    def __init__(self, plan, fp, lib=None, minb=None, parts=8):
+        """minb: CTAs per SM the registers are sized for (default: 2 if the plan's variant has
+        bit 0, else 3)."""
         self.lib = lib or _lib.load()
         self.fp = fp
         self.kernels = {}
         self._libs = []
         self._images = []
+        if minb is None:
+            minb = 2 if len(fp.groups) and int(fp.groups[0]["variant"]) & 1 else 3
         sms = self.lib.dcs_sm_count()
         for img, gis in compile_plan(plan, fp, self.lib, minb, parts):
             buf = ctypes.create_string_buffer(img, len(img))
