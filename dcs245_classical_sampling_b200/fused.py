@@ -295,9 +295,11 @@ def _plan_runs(steps, first, count, tsteps, truns, dim, R, tbit, slot_of):
         active = slot_mask(steps[s0].active_in)
         inactive = [q for q in range(dim) if not (active >> slot_of(q)) & 1 and q not in roles
                     and not (support >> q) & 1]
-        # pad to R dimensions with unit vectors of active coordinates outside the run's support,
-        # the highest first (the low coordinates stay with the threads of a warp)
-        for q in reversed(range(dim)):
+        # pad to R dimensions with unit vectors of active coordinates outside the run's support:
+        # tile bit 0 first (local entries j and j + e_0 are then one aligned 16-byte word, moved
+        # by one shared-memory instruction), then the highest (the low coordinates stay with the
+        # threads of a warp)
+        for q in [0] + list(reversed(range(1, dim))):
             if len(basis) >= R:
                 break
             if q not in roles and q not in inactive and not (support >> q) & 1:

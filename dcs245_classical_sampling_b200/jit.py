@@ -23,7 +23,7 @@ from . import _lib
 HERE = Path(__file__).resolve().parent
 HEADER = HERE / "csrc" / "runs_jit.cuh"
 CACHE_DIR = HERE / "_jit_cache"
-KERNEL_VERSION = 1  # bump when the generated code changes meaning
+KERNEL_VERSION = 2  # bump when the generated code changes meaning
 
 ONE_VECTOR = (0, 1, 3, 5, 7)
 
@@ -120,8 +120,16 @@ def group_source(plan, fp, gi, minb=3):
         L.append("                    const uint32_t t0 = tp | tu;")
         L.append(f"                    tu = ((tu | ~{mhi3}u) + 1u) & {mhi3}u;")
         L.append(f"                    float2 v[{1 << R}];")
-        for j, o in enumerate(offs):
-            L.append(f"                    v[{j}] = *reinterpret_cast<const float2*>(shb + (t0 ^ {o}u));")
+        # local bit k0 with basis vector e_0: entries j and j | 2^k0 are one aligned 16-byte word
+        k0 = next((k for k in range(R) if int(tr["off"][1 << k]) == 1), None)
+        pairs = [(j, j | (1 << k0)) for j in range(1 << R) if not (j >> k0) & 1] if k0 is not None else None
+        if pairs:
+            for j, j1 in pairs:
+                L.append(f"                    {{ const float4 q = *reinterpret_cast<const float4*>(shb + (t0 ^ {offs[j]}u)); "
+                         f"v[{j}] = make_float2(q.x, q.y); v[{j1}] = make_float2(q.z, q.w); }}")
+        else:
+            for j, o in enumerate(offs):
+                L.append(f"                    v[{j}] = *reinterpret_cast<const float2*>(shb + (t0 ^ {o}u));")
         for i in range(n):
             si = s + i
             st = fp.tile_steps[first + si]
@@ -140,8 +148,13 @@ def group_source(plan, fp, gi, minb=3):
             else:
                 call = f"jit::body4<{R}, {k1}, {k2}, {mix}, {B}, {dead}, {sk}, {ska}>{args};"
             L.append(f"                    {call}")
-        for j, o in enumerate(offs):
-            L.append(f"                    *reinterpret_cast<float2*>(shb + (t0 ^ {o}u)) = v[{j}];")
+        if pairs:
+            for j, j1 in pairs:
+                L.append(f"                    *reinterpret_cast<float4*>(shb + (t0 ^ {offs[j]}u)) = "
+                         f"make_float4(v[{j}].x, v[{j}].y, v[{j1}].x, v[{j1}].y);")
+        else:
+            for j, o in enumerate(offs):
+                L.append(f"                    *reinterpret_cast<float2*>(shb + (t0 ^ {o}u)) = v[{j}];")
         L.append("                }")
         L.append("            }")
         L.append("        }")

@@ -34,6 +34,7 @@ def main():
     ap.add_argument("--low", type=int, default=4)
     ap.add_argument("--variant", type=int, default=0)
     ap.add_argument("--pairs", action="store_true", help="two steps per shared-memory round trip")
+    ap.add_argument("--jit", action="store_true", help="plan-specialised group kernels (register-run variants)")
     a = ap.parse_args()
     lib = _lib.load()
     w = build_workload(a.workload)
@@ -58,6 +59,9 @@ def main():
     sub = P.BlockPlan(**{**bp.__dict__, "steps": steps})
     if a.mode == "fused":
         fp = build_fused_plan(sub, max_dim=a.max_dim, low=a.low, variant=a.variant, pairs=a.pairs)
+        if a.jit:
+            from .jit import JitPlan
+            fp.jit = JitPlan(sub, fp, lib)
         nmax = len(fp.groups)
     else:
         dsteps = device_steps(steps)
