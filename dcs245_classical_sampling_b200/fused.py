@@ -86,6 +86,8 @@ class FusedPlan:
     dsteps: np.ndarray
     tile_runs: np.ndarray = None
     jit: object = None  # jit.JitPlan: plan-specialised group kernels (loaded), or None
+    # register-run plans: with pairs=True the generated kernels take two cosets per iteration
+    coset_pairs: bool = False
     spans: list = field(default_factory=list)      # (first, count) per group
     universe: list = field(default_factory=list)   # |U| per group
     tiles: list = field(default_factory=list)      # tile count per group
@@ -346,7 +348,8 @@ def build_fused_plan(plan, max_dim=13, low=4, max_steps=MAX_GROUP_STEPS, max_ext
     groups = np.zeros(len(spans), dtype=_lib.GROUP_DTYPE)
     tsteps = np.zeros(len(steps), dtype=_lib.TILE_STEP_DTYPE)
     truns = np.zeros(len(steps), dtype=_lib.TILE_RUN_DTYPE) if variant & 4 else None
-    fp = FusedPlan(groups=groups, tile_steps=tsteps, dsteps=device_steps(steps), spans=list(spans), tile_runs=truns)
+    fp = FusedPlan(groups=groups, tile_steps=tsteps, dsteps=device_steps(steps), spans=list(spans), tile_runs=truns,
+                   coset_pairs=bool(pairs and variant & 4))
     for gi, (first, count) in enumerate(spans):
         U = 0
         vecs = []

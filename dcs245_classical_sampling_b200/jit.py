@@ -23,7 +23,7 @@ from . import _lib
 HERE = Path(__file__).resolve().parent
 HEADER = HERE / "csrc" / "runs_jit.cuh"
 CACHE_DIR = HERE / "_jit_cache"
-KERNEL_VERSION = 2  # bump when the generated code changes meaning
+KERNEL_VERSION = 3  # bump when the generated code changes meaning
 
 ONE_VECTOR = (0, 1, 3, 5, 7)
 
@@ -54,7 +54,11 @@ def _deposit_expr(g):
 
 
 def group_source(plan, fp, gi, minb=3):
-    """CUDA source of the kernel of group gi (``dcs_g<gi>``); None if the group has no runs."""
+    """CUDA source of the kernel of group gi (``dcs_g<gi>``); None if the group has no runs.
+
+    With ``fp.coset_pairs`` a thread takes two cosets per loop iteration where it has an even
+    number of them: the shared-memory loads of both are issued before either is computed."""
+    coset_pairs = bool(getattr(fp, "coset_pairs", False))
     g = fp.groups[gi]
     if not int(g["variant"]) & 4:
         return None
@@ -115,21 +119,25 @@ def group_source(plan, fp, gi, minb=3):
             L.append(f"                tp = jit::ins0(tp, {p});")
         L.append("                tp <<= 3;")
         L.append("                uint32_t tu = 0;")
-        L.append("#pragma unroll 1")
-        L.append(f"                for (int k = 0; k < {niter}; ++k) {{")
-        L.append("                    const uint32_t t0 = tp | tu;")
-        L.append(f"                    tu = ((tu | ~{mhi3}u) + 1u) & {mhi3}u;")
-        L.append(f"                    float2 v[{1 << R}];")
         # local bit k0 with basis vector e_0: entries j and j | 2^k0 are one aligned 16-byte word
         k0 = next((k for k in range(R) if int(tr["off"][1 << k]) == 1), None)
         pairs = [(j, j | (1 << k0)) for j in range(1 << R) if not (j >> k0) & 1] if k0 is not None else None
-        if pairs:
-            for j, j1 in pairs:
-                L.append(f"                    {{ const float4 q = *reinterpret_cast<const float4*>(shb + (t0 ^ {offs[j]}u)); "
-                         f"v[{j}] = make_float2(q.x, q.y); v[{j1}] = make_float2(q.z, q.w); }}")
-        else:
-            for j, o in enumerate(offs):
-                L.append(f"                    v[{j}] = *reinterpret_cast<const float2*>(shb + (t0 ^ {o}u));")
+        # two cosets per iteration (their shared loads issued together) when the plan asks for it
+        cos = ["a", "b"] if coset_pairs and niter % 2 == 0 else ["a"]
+        L.append("#pragma unroll 1")
+        L.append(f"                for (int k = 0; k < {niter // len(cos)}; ++k) {{")
+        for c in cos:
+            L.append(f"                    const uint32_t t0{c} = tp | tu;")
+            L.append(f"                    tu = ((tu | ~{mhi3}u) + 1u) & {mhi3}u;")
+            L.append(f"                    float2 v{c}[{1 << R}];")
+        for c in cos:
+            if pairs:
+                for j, j1 in pairs:
+                    L.append(f"                    {{ const float4 q = *reinterpret_cast<const float4*>(shb + (t0{c} ^ "
+                             f"{offs[j]}u)); v{c}[{j}] = make_float2(q.x, q.y); v{c}[{j1}] = make_float2(q.z, q.w); }}")
+            else:
+                for j, o in enumerate(offs):
+                    L.append(f"                    v{c}[{j}] = *reinterpret_cast<const float2*>(shb + (t0{c} ^ {o}u));")
         for i in range(n):
             si = s + i
             st = fp.tile_steps[first + si]
@@ -139,22 +147,24 @@ def group_source(plan, fp, gi, minb=3):
             sk, ska = int(st["sK"]) & 1, int(st["sKa"]) & 1
             k1, k2, mix = int(st["rk1"]), int(st["rk2"]), int(st["rmix"])
             tb3 = (int(st["tbeta"]) << 3) & 0xFFFFFFFF
-            m0 = f"(((uint32_t)__popc(t0 & {tb3}u) ^ (csm >> {si})) & 1u) << 31"
-            args = f"(v, fw[{si}], ovy[{si}] >> 1, {m0})"
-            if kind in ONE_VECTOR:
-                call = f"jit::body1<{kind}, {R}, {k1}, {B}, {dead}, {sk}, {ska}>{args};"
-            elif kind in (2, 4):
-                call = f"jit::body0<{kind}, {R}, {B}, {dead}>{args};"
+            for c in cos:
+                m0 = f"(((uint32_t)__popc(t0{c} & {tb3}u) ^ (csm >> {si})) & 1u) << 31"
+                args = f"(v{c}, fw[{si}], ovy[{si}] >> 1, {m0})"
+                if kind in ONE_VECTOR:
+                    call = f"jit::body1<{kind}, {R}, {k1}, {B}, {dead}, {sk}, {ska}>{args};"
+                elif kind in (2, 4):
+                    call = f"jit::body0<{kind}, {R}, {B}, {dead}>{args};"
+                else:
+                    call = f"jit::body4<{R}, {k1}, {k2}, {mix}, {B}, {dead}, {sk}, {ska}>{args};"
+                L.append(f"                    {call}")
+        for c in cos:
+            if pairs:
+                for j, j1 in pairs:
+                    L.append(f"                    *reinterpret_cast<float4*>(shb + (t0{c} ^ {offs[j]}u)) = "
+                             f"make_float4(v{c}[{j}].x, v{c}[{j}].y, v{c}[{j1}].x, v{c}[{j1}].y);")
             else:
-                call = f"jit::body4<{R}, {k1}, {k2}, {mix}, {B}, {dead}, {sk}, {ska}>{args};"
-            L.append(f"                    {call}")
-        if pairs:
-            for j, j1 in pairs:
-                L.append(f"                    *reinterpret_cast<float4*>(shb + (t0 ^ {offs[j]}u)) = "
-                         f"make_float4(v[{j}].x, v[{j}].y, v[{j1}].x, v[{j1}].y);")
-        else:
-            for j, o in enumerate(offs):
-                L.append(f"                    *reinterpret_cast<float2*>(shb + (t0 ^ {o}u)) = v[{j}];")
+                for j, o in enumerate(offs):
+                    L.append(f"                    *reinterpret_cast<float2*>(shb + (t0{c} ^ {o}u)) = v{c}[{j}];")
         L.append("                }")
         L.append("            }")
         L.append("        }")

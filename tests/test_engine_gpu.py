@@ -79,13 +79,14 @@ def test_fused_kernel_variants_match_reference(golden, name, variant):
 
 
 @pytest.mark.parametrize("name", ["c1", "small", "c2"])
-@pytest.mark.parametrize("variant", [4, 12])
-def test_plan_specialised_kernels_match_reference(golden, name, variant):
+@pytest.mark.parametrize("variant,pairs", [(4, False), (12, False), (4, True), (13, True)])
+def test_plan_specialised_kernels_match_reference(golden, name, variant, pairs):
     """Group kernels generated and compiled for the plan (jit.py) against the reference blocks,
-    and against the library's register-run kernel on the same configuration."""
+    and against the library's register-run kernel on the same configuration (pairs: two cosets
+    per loop iteration in the generated kernels)."""
     case, arrays = golden(name)
     eng = _engine(case, arrays, np.complex64, mode="fused")
-    eng.set_fused_config(variant=variant, pairs=False, max_dim=13, low=4, jit=False)
+    eng.set_fused_config(variant=variant, pairs=pairs, max_dim=13, low=4, jit=False)
     lib_blocks = [eng.block(_x(rec))[0].cpu().numpy() for rec in case["protocol"]["records"]]
     eng.set_fused_config(jit=True)
     assert eng.fplan.jit is not None and eng.fplan.jit.kernels
