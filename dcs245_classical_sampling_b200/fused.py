@@ -88,6 +88,8 @@ class FusedPlan:
     jit: object = None  # jit.JitPlan: plan-specialised group kernels (loaded), or None
     # register-run plans: with pairs=True the generated kernels take two cosets per iteration
     coset_pairs: bool = False
+    # generated kernels: first and last run of a tile read and write the table directly
+    direct_io: bool = True
     spans: list = field(default_factory=list)      # (first, count) per group
     universe: list = field(default_factory=list)   # |U| per group
     tiles: list = field(default_factory=list)      # tile count per group

@@ -23,7 +23,7 @@ from . import _lib
 HERE = Path(__file__).resolve().parent
 HEADER = HERE / "csrc" / "runs_jit.cuh"
 CACHE_DIR = HERE / "_jit_cache"
-KERNEL_VERSION = 3  # bump when the generated code changes meaning
+KERNEL_VERSION = 4  # bump when the generated code changes meaning
 
 ONE_VECTOR = (0, 1, 3, 5, 7)
 
@@ -53,36 +53,86 @@ def _deposit_expr(g):
     return " | ".join(terms) if terms else "0ull"
 
 
+def _group_runs(fp, gi):
+    """[(first step within the group, step count)] of the register runs of group gi."""
+    g = fp.groups[gi]
+    first, count = int(g["first"]), int(g["count"])
+    out, s = [], 0
+    while s < count:
+        n = int(fp.tile_steps[first + s]["run_len"])
+        if n < 1:
+            raise ValueError(f"group {gi}: malformed run at step {first + s}")
+        out.append((s, n))
+        s += n
+    return out
+
+
+def uses_tile_buffer(fp, gi):
+    """False when the group's kernel keeps no tile in shared memory (direct I/O, one run)."""
+    return not (getattr(fp, "direct_io", True) and len(_group_runs(fp, gi)) == 1
+                and _direct_ok(fp, gi))
+
+
+def _direct_ok(fp, gi):
+    """Direct I/O needs one coset-skip mask for the whole group (coset slots keep their activity
+    inside a group, so this holds for every plan the planner builds)."""
+    g = fp.groups[gi]
+    first, count = int(g["first"]), int(g["count"])
+    return len({int(fp.tile_steps[first + s]["cskip"]) for s in range(count)}) == 1
+
+
 def group_source(plan, fp, gi, minb=3):
     """CUDA source of the kernel of group gi (``dcs_g<gi>``); None if the group has no runs.
 
-    With ``fp.coset_pairs`` a thread takes two cosets per loop iteration where it has an even
-    number of them: the shared-memory loads of both are issued before either is computed."""
+    Direct I/O (``fp.direct_io``, the default): the first run of a tile loads its cosets from
+    the table into registers and the last run stores them to the table, scaled, with the max;
+    shared memory holds the tile only between runs.  The table address of tile entry t is the
+    XOR-linear map addr(t) = (t & lowmask) ^ sum of basis vectors of t's high bits, so entry j of
+    the coset of t0 sits at base ^ addr(t0) ^ addr(off_j), the last term a constant of the plan.
+    Without it, the tile is staged in shared memory on load and store (the library kernel's
+    scheme).  With ``fp.coset_pairs`` a thread takes two cosets per loop iteration where it has
+    an even number of them."""
     coset_pairs = bool(getattr(fp, "coset_pairs", False))
     g = fp.groups[gi]
     if not int(g["variant"]) & 4:
         return None
+    direct = bool(getattr(fp, "direct_io", True)) and _direct_ok(fp, gi)
     R = 4 if int(g["variant"]) & 8 else 3
     first, count = int(g["first"]), int(g["count"])
     TD, LOW = int(g["tile_dim"]), int(g["low_bits"])
     T = 1 << TD
+    lowmask = (1 << LOW) - 1
     in_mask = int(fp.dsteps[first]["in_mask"])
     out_mask = int(g["out_mask"])
+    in_inact = ~in_mask & 0xFFFFFFFFFFFFFFFF
+    out_inact = ~out_mask & 0xFFFFFFFFFFFFFFFF
     pair_in = LOW >= 1 and (in_mask & 1)
     pair_out = LOW >= 1 and (out_mask & 1)
     nb = max(1, TD - LOW)
-    basis = ", ".join(_u64(g["basis"][i]) for i in range(nb))
-    betas = ", ".join(_u64(fp.dsteps[first + s]["beta"]) for s in range(count))
+    basis = [int(g["basis"][i]) for i in range(16)]
+
+    def gaddr(t):
+        a = t & lowmask
+        for i in range(TD - LOW):
+            if (t >> (LOW + i)) & 1:
+                a ^= basis[i]
+        return a
+
+    runs = _group_runs(fp, gi)
     L = []
-    L.append(f"__constant__ uint64_t g{gi}_basis[{nb}] = {{{basis}}};")
-    L.append(f"__constant__ uint64_t g{gi}_beta[{count}] = {{{betas}}};")
+    L.append(f"__constant__ uint64_t g{gi}_basis[{nb}] = {{{', '.join(_u64(basis[i]) for i in range(nb))}}};")
+    L.append(f"__constant__ uint64_t g{gi}_beta[{count}] = "
+             f"{{{', '.join(_u64(fp.dsteps[first + s]['beta']) for s in range(count))}}};")
     L.append(f'extern "C" __global__ void __launch_bounds__(256, {minb})')
     L.append(f"dcs_g{gi}(float2* __restrict__ E, const jit_param* __restrict__ params, "
              "unsigned long long* __restrict__ maxbits, jit_scale* __restrict__ scale) {")
     L.append(f"    constexpr int TD = {TD}, LOW = {LOW}, T = 1 << TD, COUNT = {count}, FIRST = {first};")
     L.append("    extern __shared__ __align__(16) unsigned char smem[];")
-    L.append("    float2* sh = reinterpret_cast<float2*>(smem);")
-    L.append("    uint64_t* hi_tab = reinterpret_cast<uint64_t*>(smem + sizeof(float2) * T);")
+    if uses_tile_buffer(fp, gi):
+        L.append("    float2* sh = reinterpret_cast<float2*>(smem);")
+        L.append("    uint64_t* hi_tab = reinterpret_cast<uint64_t*>(smem + sizeof(float2) * T);")
+    else:
+        L.append("    uint64_t* hi_tab = reinterpret_cast<uint64_t*>(smem);")
     L.append("    __shared__ float4 fw[COUNT];")
     L.append("    __shared__ int ovy[COUNT];")
     L.append("    __shared__ uint32_t cs_sh;")
@@ -91,19 +141,25 @@ def group_source(plan, fp, gi, minb=3):
     L.append("    float lm = 0.f;")
     L.append(f"    for (uint64_t tile = blockIdx.x; tile < {_u64(1 << int(g['coset_m']))}; tile += gridDim.x) {{")
     L.append(f"        const uint64_t base = {_deposit_expr(g)};")
-    L.append(f"        jit::load_tile<T, LOW, {'true' if pair_in else 'false'}>(E, sh, hi_tab, base, "
-             f"{_u64(~in_mask)});")
-    L.append(f"        jit::sign_bits<COUNT>(g{gi}_beta, base, ovy, &cs_sh);")
-    L.append('        asm volatile("cp.async.wait_all;\\n" ::: "memory");')
-    L.append("        __syncthreads();")
+    if direct:
+        L.append(f"        jit::sign_bits<COUNT>(g{gi}_beta, base, ovy, &cs_sh);")
+        L.append("        __syncthreads();")
+    else:
+        L.append(f"        jit::load_tile<T, LOW, {'true' if pair_in else 'false'}>(E, sh, hi_tab, base, "
+                 f"{_u64(in_inact)});")
+        L.append(f"        jit::sign_bits<COUNT>(g{gi}_beta, base, ovy, &cs_sh);")
+        L.append('        asm volatile("cp.async.wait_all;\\n" ::: "memory");')
+        L.append("        __syncthreads();")
     L.append("        const uint32_t csm = cs_sh;")
     L.append("        unsigned char* shb = smem;")
-    s = 0
-    while s < count:
+    if direct:
+        L.append(f"        if (!(base & {_u64(fp.tile_steps[first]['cskip'])})) {{")
+    for ri, (s, n) in enumerate(runs):
+        src_g = direct and ri == 0
+        dst_g = direct and ri == len(runs) - 1
         ts0 = fp.tile_steps[first + s]
         tr = fp.tile_runs[first + s]
-        n = int(ts0["run_len"])
-        if n < 1 or int(tr["count"]) != n or int(tr["r"]) != R:
+        if int(tr["count"]) != n or int(tr["r"]) != R:
             raise ValueError(f"group {gi}: malformed run at step {first + s}")
         nins = int(tr["nins"])
         ins = [int(x) for x in tr["ins"][:nins]]
@@ -111,8 +167,11 @@ def group_source(plan, fp, gi, minb=3):
         niter = NB >> 8 if NB > 256 else 1
         mhi3 = int(tr["mhi"]) << 3
         offs = [int(tr["off"][j]) << 3 for j in range(1 << R)]
-        L.append(f"        // run: steps {first + s}..{first + s + n - 1}, {NB} cosets of {1 << R} entries")
-        L.append(f"        if (!(base & {_u64(ts0['cskip'])})) {{")
+        G = [gaddr(int(tr["off"][j])) for j in range(1 << R)]
+        L.append(f"        // run: steps {first + s}..{first + s + n - 1}, {NB} cosets of {1 << R} entries"
+                 f"{', from the table' if src_g else ''}{', to the table' if dst_g else ''}")
+        if not direct:
+            L.append(f"        if (!(base & {_u64(ts0['cskip'])})) {{")
         L.append(f"            if ((int)threadIdx.x < {NB}) {{")
         L.append("                uint32_t tp = threadIdx.x;")
         for p in ins:
@@ -122,7 +181,6 @@ def group_source(plan, fp, gi, minb=3):
         # local bit k0 with basis vector e_0: entries j and j | 2^k0 are one aligned 16-byte word
         k0 = next((k for k in range(R) if int(tr["off"][1 << k]) == 1), None)
         pairs = [(j, j | (1 << k0)) for j in range(1 << R) if not (j >> k0) & 1] if k0 is not None else None
-        # two cosets per iteration (their shared loads issued together) when the plan asks for it
         cos = ["a", "b"] if coset_pairs and niter % 2 == 0 else ["a"]
         L.append("#pragma unroll 1")
         L.append(f"                for (int k = 0; k < {niter // len(cos)}; ++k) {{")
@@ -130,8 +188,22 @@ def group_source(plan, fp, gi, minb=3):
             L.append(f"                    const uint32_t t0{c} = tp | tu;")
             L.append(f"                    tu = ((tu | ~{mhi3}u) + 1u) & {mhi3}u;")
             L.append(f"                    float2 v{c}[{1 << R}];")
+            if src_g or dst_g:
+                L.append(f"                    const uint64_t a0{c} = base ^ hi_tab[t0{c} >> {3 + LOW}] ^ "
+                         f"(uint64_t)((t0{c} >> 3) & {lowmask}u);")
         for c in cos:
-            if pairs:
+            if src_g:
+                if pairs and pair_in:
+                    for j, j1 in pairs:
+                        L.append(f"                    {{ const uint64_t a = a0{c} ^ {_u64(G[j])}; "
+                                 f"if (a & {_u64(in_inact)}) {{ v{c}[{j}] = v{c}[{j1}] = make_float2(0.f, 0.f); }} "
+                                 f"else {{ const float4 q = __ldcg(reinterpret_cast<const float4*>(E + a)); "
+                                 f"v{c}[{j}] = make_float2(q.x, q.y); v{c}[{j1}] = make_float2(q.z, q.w); }} }}")
+                else:
+                    for j in range(1 << R):
+                        L.append(f"                    {{ const uint64_t a = a0{c} ^ {_u64(G[j])}; "
+                                 f"v{c}[{j}] = (a & {_u64(in_inact)}) ? make_float2(0.f, 0.f) : __ldcg(E + a); }}")
+            elif pairs:
                 for j, j1 in pairs:
                     L.append(f"                    {{ const float4 q = *reinterpret_cast<const float4*>(shb + (t0{c} ^ "
                              f"{offs[j]}u)); v{c}[{j}] = make_float2(q.x, q.y); v{c}[{j1}] = make_float2(q.z, q.w); }}")
@@ -158,7 +230,20 @@ def group_source(plan, fp, gi, minb=3):
                     call = f"jit::body4<{R}, {k1}, {k2}, {mix}, {B}, {dead}, {sk}, {ska}>{args};"
                 L.append(f"                    {call}")
         for c in cos:
-            if pairs:
+            if dst_g:
+                if pairs and pair_out:
+                    for j, j1 in pairs:
+                        L.append(f"                    {{ const uint64_t a = a0{c} ^ {_u64(G[j])}; "
+                                 f"if (!(a & {_u64(out_inact)})) {{ const float4 q = make_float4(v{c}[{j}].x * sc, "
+                                 f"v{c}[{j}].y * sc, v{c}[{j1}].x * sc, v{c}[{j1}].y * sc); "
+                                 "lm = fmaxf(lm, fmaxf(q.x * q.x + q.y * q.y, q.z * q.z + q.w * q.w)); "
+                                 "*reinterpret_cast<float4*>(E + a) = q; } }")
+                else:
+                    for j in range(1 << R):
+                        L.append(f"                    {{ const uint64_t a = a0{c} ^ {_u64(G[j])}; "
+                                 f"if (!(a & {_u64(out_inact)})) {{ const float2 q = make_float2(v{c}[{j}].x * sc, "
+                                 f"v{c}[{j}].y * sc); lm = fmaxf(lm, q.x * q.x + q.y * q.y); E[a] = q; }} }}")
+            elif pairs:
                 for j, j1 in pairs:
                     L.append(f"                    *reinterpret_cast<float4*>(shb + (t0{c} ^ {offs[j]}u)) = "
                              f"make_float4(v{c}[{j}].x, v{c}[{j}].y, v{c}[{j1}].x, v{c}[{j1}].y);")
@@ -167,11 +252,15 @@ def group_source(plan, fp, gi, minb=3):
                     L.append(f"                    *reinterpret_cast<float2*>(shb + (t0{c} ^ {o}u)) = v{c}[{j}];")
         L.append("                }")
         L.append("            }")
+        if not direct:
+            L.append("        }")
+        if not dst_g:
+            L.append("        __syncthreads();")
+    if direct:
         L.append("        }")
-        L.append("        __syncthreads();")
-        s += n
-    L.append(f"        lm = jit::store_tile<T, LOW, {'true' if pair_out else 'false'}>(E, sh, hi_tab, base, "
-             f"{_u64(~out_mask)}, sc, lm);")
+    else:
+        L.append(f"        lm = jit::store_tile<T, LOW, {'true' if pair_out else 'false'}>(E, sh, hi_tab, base, "
+                 f"{_u64(out_inact)}, sc, lm);")
     L.append("        __syncthreads();")
     L.append("    }")
     L.append(f"    jit::block_max(lm, maxbits, {gi + 1});")
@@ -256,7 +345,7 @@ class JitPlan:
             for gi in gis:
                 g = fp.groups[gi]
                 td, low = int(g["tile_dim"]), int(g["low_bits"])
-                smem = 8 * (1 << td) + 8 * (1 << (td - low))
+                smem = 8 * (1 << (td - low)) + (8 * (1 << td) if uses_tile_buffer(fp, gi) else 0)
                 k = ctypes.c_void_p()
                 per_sm = ctypes.c_int()
                 _lib.check(self.lib.dcs_jit_kernel(handle, f"dcs_g{gi}".encode(), smem, ctypes.byref(k),

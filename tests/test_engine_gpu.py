@@ -97,6 +97,24 @@ def test_plan_specialised_kernels_match_reference(golden, name, variant, pairs):
         assert rel_l2(v, lb) < 1e-6
 
 
+@pytest.mark.parametrize("name", ["small", "c2"])
+def test_plan_specialised_kernels_with_staged_tiles(golden, name):
+    """The generated kernels with the tile staged through shared memory on load and store
+    (direct_io off) give the same blocks as the default direct table I/O."""
+    from dcs245_classical_sampling_b200.jit import JitPlan
+    case, arrays = golden(name)
+    eng = _engine(case, arrays, np.complex64, mode="fused")
+    eng.set_fused_config(variant=12, pairs=False, max_dim=13, low=4, jit=True)
+    direct = [eng.block(_x(rec))[0].cpu().numpy() for rec in case["protocol"]["records"]]
+    eng.fplan.jit.close()
+    eng.fplan.direct_io = False
+    eng.fplan.jit = JitPlan(eng.plan, eng.fplan, eng.lib)
+    for rec, d in zip(case["protocol"]["records"], direct):
+        v = eng.block(_x(rec))[0].cpu().numpy()
+        assert rel_l2(v, arrays[f"block_{rec['sample_id']}"]) < 1e-5
+        assert rel_l2(v, d) < 1e-6
+
+
 def test_one_item_at_a_time_equals_batched_slices(golden):
     case, arrays = golden("small")
     a = _engine(case, arrays, np.complex128, items=1)
