@@ -46,9 +46,10 @@ def cached(plan, device_name):
 
 # with plan-specialised group kernels (jit.py; scalar register runs, so no packed variants)
 # (pairs=True with register runs: two cosets per loop iteration in the generated kernels)
-JIT_CANDIDATES = [(13, 3, 24, 12, False), (13, 4, 24, 12, False), (13, 3, 24, 4, False), (13, 4, 24, 4, False),
-                  (13, 3, 24, 4, True), (13, 4, 24, 4, True), (13, 3, 24, 13, True), (13, 3, 24, 13, False),
-                  (13, 5, 24, 12, False), (13, 3, 16, 12, False)]
+# variant bit 1 with register runs: packed FP32x2 groups where tile bit 0 stays free
+JIT_CANDIDATES = [(13, 4, 24, 12, False), (13, 3, 24, 12, False), (13, 4, 24, 4, False), (13, 4, 24, 4, True),
+                  (13, 4, 24, 6, False), (13, 3, 24, 6, False), (13, 4, 24, 14, False), (13, 4, 24, 15, False),
+                  (13, 5, 24, 6, False), (13, 4, 16, 6, False)]
 
 
 def tune(engine, params_dev, candidates=None, repeats=1, save=True, jit=False):

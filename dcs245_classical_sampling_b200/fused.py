@@ -249,7 +249,7 @@ def _run_vectors(st, kind, ts, tbit):
     return [], 0
 
 
-def _plan_runs(steps, first, count, tsteps, truns, dim, R, tbit, slot_of):
+def _plan_runs(steps, first, count, tsteps, truns, dim, R, tbit, slot_of, keep_bit0=False):
     """Split a group's steps into register runs of local dimension R; False if a step does not fit."""
     vr = []
     for s in range(first, first + count):
@@ -301,9 +301,9 @@ def _plan_runs(steps, first, count, tsteps, truns, dim, R, tbit, slot_of):
                     and not (support >> q) & 1]
         # pad to R dimensions with unit vectors of active coordinates outside the run's support:
         # tile bit 0 first (local entries j and j + e_0 are then one aligned 16-byte word, moved
-        # by one shared-memory instruction), then the highest (the low coordinates stay with the
-        # threads of a warp)
-        for q in [0] + list(reversed(range(1, dim))):
+        # by one shared-memory instruction) unless keep_bit0 (packed plans: bit 0 pairs cosets),
+        # then the highest (the low coordinates stay with the threads of a warp)
+        for q in ([] if keep_bit0 else [0]) + list(reversed(range(1, dim))):
             if len(basis) >= R:
                 break
             if q not in roles and q not in inactive and not (support >> q) & 1:
@@ -478,7 +478,8 @@ def build_fused_plan(plan, max_dim=13, low=4, max_steps=MAX_GROUP_STEPS, max_ext
         if variant & 4:
             R = 4 if variant & 8 else 3
             slot_of = lambda q: q if q < l else pivots[q - l]
-            if not _plan_runs(steps, first, count, tsteps, truns, dim, R, tbit, slot_of):
+            # packed plans (bit 1) keep tile bit 0 out of the runs: it is the lane bit
+            if not _plan_runs(steps, first, count, tsteps, truns, dim, R, tbit, slot_of, keep_bit0=bool(variant & 2)):
                 g["variant"] = variant & ~12  # this group keeps the one-step-per-round-trip kernel
         elif pairs:
             _pair_steps(steps, first, count, tsteps, dim, tilepos_of=lambda q: (q < l or q in pivots),

@@ -23,7 +23,7 @@ from . import _lib
 HERE = Path(__file__).resolve().parent
 HEADER = HERE / "csrc" / "runs_jit.cuh"
 CACHE_DIR = HERE / "_jit_cache"
-KERNEL_VERSION = 4  # bump when the generated code changes meaning
+KERNEL_VERSION = 5  # bump when the generated code changes meaning
 
 ONE_VECTOR = (0, 1, 3, 5, 7)
 
@@ -96,6 +96,8 @@ def group_source(plan, fp, gi, minb=3):
     g = fp.groups[gi]
     if not int(g["variant"]) & 4:
         return None
+    if packable(fp, gi):
+        return _packed_source(fp, gi, minb)
     direct = bool(getattr(fp, "direct_io", True)) and _direct_ok(fp, gi)
     R = 4 if int(g["variant"]) & 8 else 3
     first, count = int(g["first"]), int(g["count"])
@@ -261,6 +263,167 @@ def group_source(plan, fp, gi, minb=3):
     else:
         L.append(f"        lm = jit::store_tile<T, LOW, {'true' if pair_out else 'false'}>(E, sh, hi_tab, base, "
                  f"{_u64(out_inact)}, sc, lm);")
+    L.append("        __syncthreads();")
+    L.append("    }")
+    L.append(f"    jit::block_max(lm, maxbits, {gi + 1});")
+    L.append("}")
+    return "\n".join(L) + "\n"
+
+
+def packable(fp, gi):
+    """Packed form for group gi: the plan asks for it (variant bit 1), direct I/O applies, and no
+    run of the group has tile bit 0 in its space or among its coset zero bits."""
+    g = fp.groups[gi]
+    v = int(g["variant"])
+    if not (v & 2 and v & 4) or not getattr(fp, "direct_io", True) or not _direct_ok(fp, gi):
+        return False
+    R = 4 if v & 8 else 3
+    first = int(g["first"])
+    if int(g["tile_dim"]) < 1:
+        return False
+    for s, _ in _group_runs(fp, gi):
+        tr = fp.tile_runs[first + s]
+        nins = int(tr["nins"])
+        if nins >= int(g["tile_dim"]) or (nins and int(tr["ins"][0]) == 0):
+            return False
+        if any(int(tr["off"][j]) & 1 for j in range(1 << R)):
+            return False
+    return True
+
+
+def _packed_source(fp, gi, minb):
+    """Packed FP32x2 form of group gi: a thread takes the coset pair (t0, t0 | 1) as the two lanes
+    of its float2 values (runs_jit.cuh pbody*).  Between runs the tile sits in shared memory as
+    (re_2i, re_2i+1, im_2i, im_2i+1) per entry pair, one 16-byte word per local entry of a pair;
+    the first run reads the table and the last one writes it (direct I/O)."""
+    g = fp.groups[gi]
+    R = 4 if int(g["variant"]) & 8 else 3
+    first, count = int(g["first"]), int(g["count"])
+    TD, LOW = int(g["tile_dim"]), int(g["low_bits"])
+    T = 1 << TD
+    lowmask = (1 << LOW) - 1
+    in_mask = int(fp.dsteps[first]["in_mask"])
+    out_mask = int(g["out_mask"])
+    in_inact = ~in_mask & 0xFFFFFFFFFFFFFFFF
+    out_inact = ~out_mask & 0xFFFFFFFFFFFFFFFF
+    nb = max(1, TD - LOW)
+    basis = [int(g["basis"][i]) for i in range(16)]
+
+    def gaddr(t):
+        a = t & lowmask
+        for i in range(TD - LOW):
+            if (t >> (LOW + i)) & 1:
+                a ^= basis[i]
+        return a
+
+    runs = _group_runs(fp, gi)
+    L = []
+    L.append(f"__constant__ uint64_t g{gi}_basis[{nb}] = {{{', '.join(_u64(basis[i]) for i in range(nb))}}};")
+    L.append(f"__constant__ uint64_t g{gi}_beta[{count}] = "
+             f"{{{', '.join(_u64(fp.dsteps[first + s]['beta']) for s in range(count))}}};")
+    L.append(f'extern "C" __global__ void __launch_bounds__(256, {minb})')
+    L.append(f"dcs_g{gi}(float2* __restrict__ E, const jit_param* __restrict__ params, "
+             "unsigned long long* __restrict__ maxbits, jit_scale* __restrict__ scale) {")
+    L.append(f"    constexpr int TD = {TD}, LOW = {LOW}, T = 1 << TD, COUNT = {count}, FIRST = {first};")
+    L.append("    extern __shared__ __align__(16) unsigned char smem[];")
+    if len(runs) > 1:
+        L.append("    uint64_t* hi_tab = reinterpret_cast<uint64_t*>(smem + sizeof(float2) * T);")
+    else:
+        L.append("    uint64_t* hi_tab = reinterpret_cast<uint64_t*>(smem);")
+    L.append("    __shared__ float4 fw[COUNT];")
+    L.append("    __shared__ int ovy[COUNT];")
+    L.append("    __shared__ uint32_t cs_sh;")
+    L.append(f"    const float sc = jit::prologue<TD, LOW, COUNT, FIRST>(params, g{gi}_basis, maxbits, {gi}, scale, "
+             "fw, ovy, hi_tab);")
+    L.append("    float lm = 0.f;")
+    L.append(f"    for (uint64_t tile = blockIdx.x; tile < {_u64(1 << int(g['coset_m']))}; tile += gridDim.x) {{")
+    L.append(f"        const uint64_t base = {_deposit_expr(g)};")
+    L.append(f"        jit::sign_bits<COUNT>(g{gi}_beta, base, ovy, &cs_sh);")
+    L.append("        __syncthreads();")
+    L.append("        const uint32_t csm = cs_sh;")
+    L.append("        unsigned char* shb = smem;")
+    L.append(f"        if (!(base & {_u64(fp.tile_steps[first]['cskip'])})) {{")
+    for ri, (s, n) in enumerate(runs):
+        src_g = ri == 0
+        dst_g = ri == len(runs) - 1
+        tr = fp.tile_runs[first + s]
+        nins = int(tr["nins"])
+        ins = [int(x) for x in tr["ins"][:nins]]
+        NB2 = T >> (nins + 1)
+        niter = NB2 >> 8 if NB2 > 256 else 1
+        mhi = int(tr["mhi"])
+        mhi3 = (mhi & (mhi - 1)) << 3  # tile bit 0 is the lane bit
+        offs = [int(tr["off"][j]) << 3 for j in range(1 << R)]
+        G = [gaddr(int(tr["off"][j])) for j in range(1 << R)]
+        L.append(f"        // run: steps {first + s}..{first + s + n - 1}, {NB2} coset pairs of {1 << R} entries"
+                 f"{', from the table' if src_g else ''}{', to the table' if dst_g else ''}")
+        L.append(f"            if ((int)threadIdx.x < {NB2}) {{")
+        L.append("                uint32_t tp = threadIdx.x << 1;")
+        for p in ins:
+            L.append(f"                tp = jit::ins0(tp, {p});")
+        L.append("                tp <<= 3;")
+        L.append("                uint32_t tu = 0;")
+        L.append("#pragma unroll 1")
+        L.append(f"                for (int k = 0; k < {niter}; ++k) {{")
+        L.append("                    const uint32_t t0 = tp | tu;")
+        L.append(f"                    tu = ((tu | ~{mhi3}u) + 1u) & {mhi3}u;")
+        L.append(f"                    jit::C2 v[{1 << R}];")
+        if src_g or dst_g:
+            L.append(f"                    const uint64_t a0 = base ^ hi_tab[t0 >> {3 + LOW}] ^ "
+                     f"(uint64_t)((t0 >> 3) & {lowmask}u);")
+        for j in range(1 << R):
+            if src_g:
+                if not in_inact & 1:
+                    L.append(f"                    {{ const uint64_t a = a0 ^ {_u64(G[j])}; if (a & {_u64(in_inact)}) "
+                             f"v[{j}] = jit::C2{{make_float2(0.f, 0.f), make_float2(0.f, 0.f)}}; else {{ "
+                             f"const float4 q = __ldcg(reinterpret_cast<const float4*>(E + a)); "
+                             f"v[{j}] = jit::C2{{make_float2(q.x, q.z), make_float2(q.y, q.w)}}; }} }}")
+                else:
+                    L.append(f"                    {{ const uint64_t a = a0 ^ {_u64(G[j])}; const float2 q = "
+                             f"(a & {_u64(in_inact)}) ? make_float2(0.f, 0.f) : __ldcg(E + a); "
+                             f"v[{j}] = jit::C2{{make_float2(q.x, 0.f), make_float2(q.y, 0.f)}}; }}")
+            else:
+                L.append(f"                    {{ const float4 q = *reinterpret_cast<const float4*>(shb + (t0 ^ {offs[j]}u)); "
+                         f"v[{j}] = jit::C2{{make_float2(q.x, q.y), make_float2(q.z, q.w)}}; }}")
+        for i in range(n):
+            si = s + i
+            st = fp.tile_steps[first + si]
+            kind = int(fp.dsteps[first + si]["kind"])
+            B = _beff(kind, st, R)
+            dead = int(st["rdead"])
+            sk, ska = int(st["sK"]) & 1, int(st["sKa"]) & 1
+            k1, k2, mix = int(st["rk1"]), int(st["rk2"]), int(st["rmix"])
+            tb = int(st["tbeta"])
+            tb0 = tb & 1
+            tb3 = (tb << 3) & 0xFFFFFFFF
+            m0 = f"(((uint32_t)__popc(t0 & {tb3}u) ^ (csm >> {si})) & 1u) << 31"
+            args = f"(v, fw[{si}], ovy[{si}] >> 1, {m0})"
+            if kind in ONE_VECTOR:
+                call = f"jit::pbody1<{kind}, {R}, {k1}, {B}, {dead}, {sk}, {ska}, {tb0}>{args};"
+            elif kind in (2, 4):
+                call = f"jit::pbody0<{kind}, {R}, {B}, {dead}, {tb0}>{args};"
+            else:
+                call = f"jit::pbody4<{R}, {k1}, {k2}, {mix}, {B}, {dead}, {sk}, {ska}, {tb0}>{args};"
+            L.append(f"                    {call}")
+        for j in range(1 << R):
+            if dst_g:
+                if not out_inact & 1:
+                    L.append(f"                    {{ const uint64_t a = a0 ^ {_u64(G[j])}; if (!(a & {_u64(out_inact)})) {{ "
+                             f"const float4 q = make_float4(v[{j}].re.x * sc, v[{j}].im.x * sc, v[{j}].re.y * sc, "
+                             f"v[{j}].im.y * sc); lm = fmaxf(lm, fmaxf(q.x * q.x + q.y * q.y, q.z * q.z + q.w * q.w)); "
+                             "*reinterpret_cast<float4*>(E + a) = q; } }")
+                else:
+                    L.append(f"                    {{ const uint64_t a = a0 ^ {_u64(G[j])}; if (!(a & {_u64(out_inact)})) {{ "
+                             f"const float2 q = make_float2(v[{j}].re.x * sc, v[{j}].im.x * sc); "
+                             "lm = fmaxf(lm, q.x * q.x + q.y * q.y); E[a] = q; } }")
+            else:
+                L.append(f"                    *reinterpret_cast<float4*>(shb + (t0 ^ {offs[j]}u)) = make_float4("
+                         f"v[{j}].re.x, v[{j}].re.y, v[{j}].im.x, v[{j}].im.y);")
+        L.append("                }")
+        L.append("            }")
+        if not dst_g:
+            L.append("        __syncthreads();")
+    L.append("        }")
     L.append("        __syncthreads();")
     L.append("    }")
     L.append(f"    jit::block_max(lm, maxbits, {gi + 1});")

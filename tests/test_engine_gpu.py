@@ -79,7 +79,7 @@ def test_fused_kernel_variants_match_reference(golden, name, variant):
 
 
 @pytest.mark.parametrize("name", ["c1", "small", "c2"])
-@pytest.mark.parametrize("variant,pairs", [(4, False), (12, False), (4, True), (13, True)])
+@pytest.mark.parametrize("variant,pairs", [(4, False), (12, False), (4, True), (13, True), (6, False), (15, False)])
 def test_plan_specialised_kernels_match_reference(golden, name, variant, pairs):
     """Group kernels generated and compiled for the plan (jit.py) against the reference blocks,
     and against the library's register-run kernel on the same configuration (pairs: two cosets
