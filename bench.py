@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="ring64_d73_t314_k20")
     ap.add_argument("--mode", default="fused", choices=["fused", "device", "plain"])
+    ap.add_argument("--storage", default=None, choices=["float16"],
+                    help="binary16 table storage (the approximate half-storage tier; --mode device or plain)")
     ap.add_argument("--plain-samples", type=int, default=1)
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -223,7 +225,7 @@ def gpu_arm(args):
     t0 = time.perf_counter()
     eng = InplaceConditionalBlockGPU(w["graph"], w["unitaries"], w["n"], w["order"], w["parity_operations"],
                                      w["open_vertices"])
-    eng.alloc(np.complex64, device=local, mode=args.mode)
+    eng.alloc(np.complex64, device=local, mode=args.mode, storage=args.storage)
     tune_report = None
     if args.mode == "fused" and args.tune:
         tune_report = eng.autotune(jit=not args.no_jit)
@@ -362,11 +364,12 @@ def gpu_arm(args):
         ach = dom["alg_bytes_per_launch"] / dom["avg_launch_s"] / 1e9
         line = {"metric": METRIC, "value": value, "unit": "samples/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": 1000.0 * elapsed / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "c64",
+                "scaling": "weak", "vs_baseline": None, "dtype": "f16 storage, f64 arithmetic" if args.storage else "c64",
                 "data": "synthetic (seeded 64q ring circuit, PCG64 prefixes and uniforms)",
                 "config": {"workload": args.workload, "block": f"2^{k}", "mode": args.mode,
                            "slices": 1 << len(w["parity_operations"]), "rmax": eng_rmax(w),
-                           "table_bytes": (1 << eng_maxslots(w)) * 8, "batch_per_step": 1,
+                           "table_bytes": (1 << eng_maxslots(w)) * (4 if args.storage else 8), "batch_per_step": 1,
+                           "storage": args.storage or "complex64",
                            "l2": "inputs larger than L2 (128 GiB table per slice pass)",
                            "parallelism": f"replicas x{world}"},
                 "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
@@ -476,7 +479,8 @@ def kernel_roofline(eng, prep, out, stream):
                                                    stream.cuda_stream))
             b.record(stream)
             st = plan.steps[s]
-            evs.append((a, b, ((1 << len(st.active_in)) + (1 << len(st.active_out))) * (16 if eng.use_fp64 else 8)))
+            entry = 16 if eng.use_fp64 else (4 if eng.half else 8)
+            evs.append((a, b, ((1 << len(st.active_in)) + (1 << len(st.active_out))) * entry))
         kernel = "k_step"
     torch.cuda.synchronize()
     tot_t = sum(a.elapsed_time(b) for a, b, _ in evs) / 1000.0

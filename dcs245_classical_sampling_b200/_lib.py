@@ -14,7 +14,7 @@ import numpy as np
 PKG = Path(__file__).resolve().parent
 LIB_PATH = PKG / "libdcs245.so"
 
-C64, C128 = 0, 1
+C64, C128, H16 = 0, 1, 2  # table storage: complex64, complex128, two binary16 components
 MAX_RUNS = 28
 E_ARG, E_CUDA, E_NONFINITE, E_CDF = -1, -2, -3, -4
 

@@ -29,8 +29,9 @@ def nvcc_path():
 
 
 def build(verbose=False, ptxas_info=False, force=False):
-    """Compile every source to an object (in parallel: the register-run kernels take minutes)
-    and link the shared library."""
+    """Compile every stale source to an object (in parallel: the register-run kernels take
+    minutes) and link the shared library.  An object is stale when its source or any header is
+    newer; force=True recompiles everything."""
     from concurrent.futures import ThreadPoolExecutor
     srcs = [CSRC / s for s in SOURCES if (CSRC / s).exists()]
     deps = srcs + list(CSRC.glob("*.cuh")) + [INCLUDE / "dcs245.h"]
@@ -43,8 +44,14 @@ def build(verbose=False, ptxas_info=False, force=False):
     if ptxas_info:
         flags.append("-Xptxas=-v")
 
+    headers = list(CSRC.glob("*.cuh")) + [INCLUDE / "dcs245.h"]
+    newest_header = max(h.stat().st_mtime for h in headers)
+
     def compile_one(src):
         obj = objdir / (src.stem + ".o")
+        if (not force and obj.exists() and obj.stat().st_mtime >= src.stat().st_mtime
+                and obj.stat().st_mtime >= newest_header):
+            return obj, subprocess.CompletedProcess([], 0, "", "")  # object is current
         cmd = [nvcc_path(), *flags, "-c", str(src), "-o", str(obj)]
         if verbose:
             print(" ".join(cmd), flush=True)

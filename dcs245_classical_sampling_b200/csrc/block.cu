@@ -49,10 +49,10 @@ k_accumulate(const S* __restrict__ table, uint64_t table_stride, const __grid_co
             uint32_t i = 0;
             for (int j = 0; j < tm.tr; ++j) i |= (uint32_t)(__popc(sv & tm.linv[j]) & 1) << j;
             const uint64_t c = deposit(i, tm.runs, tm.nruns);
-            const S v = table[(uint64_t)it * table_stride + c];
+            const double2 v = entry_f64(table[(uint64_t)it * table_stride + c]);
             const double m = exp(sc.logscale - log_shift);
             const double cr = coefs[2 * it] * m, ci = coefs[2 * it + 1] * m;
-            const double vr = (double)v.x, vi = (double)v.y;
+            const double vr = v.x, vi = v.y;
             acc.x += vr * cr - vi * ci;
             acc.y += vr * ci + vi * cr;
         }
@@ -247,6 +247,10 @@ extern "C" int dcs_accumulate_batched(int dtype, const void* table, uint64_t tab
                                                    (double2*)total);
     else if (dtype == DCS_C128)
         k_accumulate<double2><<<grid, 256, 0, st>>>((const double2*)table, table_stride, tm, xors, coefs, item_begin,
+                                                    log_shift, scale, (const unsigned long long*)maxbits_final,
+                                                    mstride, (double2*)total);
+    else if (dtype == DCS_H16)
+        k_accumulate<ushort2><<<grid, 256, 0, st>>>((const ushort2*)table, table_stride, tm, xors, coefs, item_begin,
                                                     log_shift, scale, (const unsigned long long*)maxbits_final,
                                                     mstride, (double2*)total);
     else {

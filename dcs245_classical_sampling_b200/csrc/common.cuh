@@ -1,5 +1,6 @@
 // Shared device helpers for the conditional-block kernels (sm_100a).
 #pragma once
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -28,6 +29,41 @@ template <class S> __device__ __forceinline__ S cneg_if(S a, int neg) {
 }
 template <class S> __device__ __forceinline__ S cscale(S a, typename Store<S>::R s) {
     return Store<S>::make(a.x * s, a.y * s);
+}
+
+// Table entries in memory type M, arithmetic in S: M == S for complex64 / complex128 tables;
+// M = ushort2 (two IEEE binary16 components, 4 bytes) with S = double2 for the half-storage
+// tier, which keeps the reference's FP64 arithmetic and rounds only on the store
+// (source/kernel_opt/inplace_half_gpu.py:22-26): FP64 -> FP32 -> binary16, each to nearest even.
+// st() writes an entry and returns |stored value|^2 for the renormalisation max; for binary16
+// that is the max of the rounded values, summed in FP32 as the reference does.
+template <class S, class M> struct Mem;
+template <class S> struct Mem<S, S> {
+    using Q = typename Store<S>::R;  // type of the running max
+    static __device__ __forceinline__ S ld(const S& m) { return m; }
+    static __device__ __forceinline__ Q st(S* E, uint64_t c, S v) {
+        E[c] = v;
+        return v.x * v.x + v.y * v.y;
+    }
+};
+template <> struct Mem<double2, ushort2> {
+    using Q = float;  // |v|^2 of a binary16 pair is exact in FP32 up to the final rounding
+    static __device__ __forceinline__ double2 ld(const ushort2& m) {
+        const float2 f = __half22float2(*reinterpret_cast<const __half2*>(&m));
+        return make_double2((double)f.x, (double)f.y);
+    }
+    static __device__ __forceinline__ float st(ushort2* E, uint64_t c, double2 v) {
+        const __half2 h = __floats2half2_rn(__double2float_rn(v.x), __double2float_rn(v.y));
+        E[c] = *reinterpret_cast<const ushort2*>(&h);
+        const float2 r = __half22float2(h);
+        return r.x * r.x + r.y * r.y;
+    }
+};
+// an entry of any table type as FP64 (re, im)
+__device__ __forceinline__ double2 entry_f64(const float2& v) { return make_double2((double)v.x, (double)v.y); }
+__device__ __forceinline__ double2 entry_f64(const double2& v) { return v; }
+__device__ __forceinline__ double2 entry_f64(const ushort2& v) {
+    return make_double2((double)__half2float(__ushort_as_half(v.x)), (double)__half2float(__ushort_as_half(v.y)));
 }
 
 // parity(c & beta) ^ ov : 1 means the sign is -1

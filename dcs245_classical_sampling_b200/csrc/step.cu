@@ -5,7 +5,8 @@
 // completely before any of its entries is written, orbits are disjoint, so one buffer suffices.
 // Differences by design:
 //   * the scale 2^-e is derived on the device from the previous step's max (no host sync);
-//   * complex64 tables are computed in FP32 (complex128 tables in FP64);
+//   * complex64 tables are computed in FP32 (complex128 tables, and the binary16 tables of
+//     the half-storage tier, in FP64);
 //   * each thread keeps ORB orbits in flight (all loads issued before any arithmetic) so
 //     that enough bytes are outstanding to cover HBM latency;
 //   * the block max is reduced in shared memory and published with one atomicMax per CTA.
@@ -20,14 +21,19 @@ using namespace dcs;
 
 namespace {
 
-template <class S, int KIND, int ORB>
+template <class S, int KIND, int ORB, class M = S>
 __global__ void __launch_bounds__(256)
-k_step(S* __restrict__ table, uint64_t table_stride, const __grid_constant__ dcs_step st, int s,
+k_step(M* __restrict__ table, uint64_t table_stride, const __grid_constant__ dcs_step st, int s,
        const dcs_param* __restrict__ params, uint64_t param_stride,
        unsigned long long* __restrict__ maxbits, uint64_t maxbits_stride, dcs_scale* __restrict__ scale) {
     using R = typename Store<S>::R;
+    using IO = Mem<S, M>;
+    using Q = typename IO::Q;
+    constexpr int NT = 256;  // threads per block (the launch uses exactly this)
+    constexpr int LU = ORB == 8 ? 3 : (ORB == 4 ? 2 : 1);
+    static_assert((1 << LU) == ORB, "ORB is a power of two");
     const int item = blockIdx.y;
-    S* E = table + (uint64_t)item * table_stride;
+    M* E = table + (uint64_t)item * table_stride;
     const dcs_param p = params[(uint64_t)item * param_stride + s];
     unsigned long long* mb = maxbits + (uint64_t)item * maxbits_stride;
     const double m2prev = (double)bits_to_m2<R>(mb[s]);
@@ -40,32 +46,62 @@ k_step(S* __restrict__ table, uint64_t table_stride, const __grid_constant__ dcs
         if (!isfinite(m2prev)) sp->flags |= 1u;
         else if (m2prev == 0.0) sp->flags |= 2u;
     }
-    const S f0 = Store<S>::make((R)p.f0r, (R)p.f0i);
-    const S f1 = Store<S>::make((R)p.f1r, (R)p.f1i);
-    const int ov = p.ov, y = p.y;
+    // the power-of-two scale is folded into the weights: (f * 2^-e) * v == (f * v) * 2^-e exactly
+    // (outside the subnormal range), and the scaled weights drop two multiplies per output
+    const S f0 = cscale(Store<S>::make((R)p.f0r, (R)p.f0i), sc);
+    const S f1 = cscale(Store<S>::make((R)p.f1r, (R)p.f1i), sc);
+    const int y = p.y;
     const uint64_t norbits = 1ull << st.m;
     const bool ident = st.nruns == 0 || (st.nruns == 1 && st.runs[0] == ((uint32_t)st.m << 16));
     const uint64_t beta = st.beta, K = st.K, Ka = st.Ka, pbit = st.pivot_bit;
-    R lm = 0;
-    const uint64_t chunk = (uint64_t)blockDim.x * ORB;
+    // Orbit x = base | u << 8 | t (t = thread, u = orbit slot of the thread, base a multiple of
+    // NT * ORB).  The deposit into the table's slots is OR-linear over those disjoint bit
+    // fields and the sign parity(c & beta) is XOR-linear, so both are split into a per-thread
+    // part, ORB compile-time combinations of the deposits of bits 8.. 8+LU-1, and one full
+    // deposit per iteration.
+    auto dep = [&](uint64_t x) { return ident ? x : deposit(x, st.runs, st.nruns); };
+    auto par = [&](uint64_t c) { return (int)(__popcll(c & beta) & 1); };
+    const uint64_t dt = dep(threadIdx.x);
+    uint64_t du[LU];
+    int pu = 0;  // bit u = parity of deposit(u << 8) & beta
+#pragma unroll
+    for (int b = 0; b < LU; ++b) du[b] = dep(1ull << (8 + b));
+#pragma unroll
+    for (int u = 0; u < ORB; ++u) {
+        uint64_t d = 0;
+#pragma unroll
+        for (int b = 0; b < LU; ++b)
+            if (u >> b & 1) d |= du[b];
+        pu |= par(d) << u;
+    }
+    const int st_ov = p.ov ^ par(dt);           // sign of c = parity(base) ^ bit u of pu ^ st_ov
+    const int pK = par(K), pKa = par(Ka);       // sign(c ^ K) = sign(c) ^ pK, likewise for Ka
+    Q lm = 0;
+    constexpr uint64_t chunk = (uint64_t)NT * ORB;
     for (uint64_t base = (uint64_t)blockIdx.x * chunk; base < norbits; base += (uint64_t)gridDim.x * chunk) {
+        const uint64_t cb = dep(base) | dt;
+        const int sb = par(dep(base)) ^ st_ov;
         uint64_t c[ORB];
-        S a[ORB], b[ORB], g[ORB], h[ORB];
+        M ra[ORB], rb[ORB], rg[ORB], rh[ORB];  // raw entries: converted to S only when combined
         bool ok[ORB];
 #pragma unroll
         for (int u = 0; u < ORB; ++u) {
-            const uint64_t x = base + threadIdx.x + (uint64_t)u * blockDim.x;
+            const uint64_t x = base + threadIdx.x + (uint64_t)u * NT;
             ok[u] = x < norbits;
-            c[u] = ident ? x : deposit(x, st.runs, st.nruns);
+            uint64_t cu = cb;
+#pragma unroll
+            for (int b = 0; b < LU; ++b)
+                if (u >> b & 1) cu |= du[b];
+            c[u] = cu;
             if (ok[u]) {
-                a[u] = E[c[u]];
-                if constexpr (KIND == DCS_KIND_MIX) b[u] = E[c[u] ^ Ka];
+                ra[u] = E[cu];
+                if constexpr (KIND == DCS_KIND_MIX) rb[u] = E[cu ^ Ka];
                 if constexpr (KIND == DCS_KIND_REPLACE || KIND == DCS_KIND_FIXED_SHRINK ||
                               KIND == DCS_KIND_SHRINK2 || KIND == DCS_KIND_SHRINK4)
-                    b[u] = E[c[u] ^ K];
+                    rb[u] = E[cu ^ K];
                 if constexpr (KIND == DCS_KIND_SHRINK4) {
-                    g[u] = E[c[u] ^ Ka];
-                    h[u] = E[c[u] ^ Ka ^ K];
+                    rg[u] = E[cu ^ Ka];
+                    rh[u] = E[cu ^ Ka ^ K];
                 }
             }
         }
@@ -73,64 +109,55 @@ k_step(S* __restrict__ table, uint64_t table_stride, const __grid_constant__ dcs
         for (int u = 0; u < ORB; ++u) {
             if (!ok[u]) continue;
             const uint64_t cc = c[u];
+            const int sgn = sb ^ (pu >> u & 1);  // 1: entry cc carries the sign -1
+            S a, b, g, h;
+            a = IO::ld(ra[u]);
+            if constexpr (KIND != DCS_KIND_GROW && KIND != DCS_KIND_DIAG && KIND != DCS_KIND_FIXED) b = IO::ld(rb[u]);
+            if constexpr (KIND == DCS_KIND_SHRINK4) {
+                g = IO::ld(rg[u]);
+                h = IO::ld(rh[u]);
+            }
             S o0, o1;
             if constexpr (KIND == DCS_KIND_GROW) {
-                o0 = cmul(f0, a[u]);
-                o1 = cmul(f1, cneg_if(a[u], neg_sign(cc, beta, ov)));
-                o0 = cscale(o0, sc); o1 = cscale(o1, sc);
-                E[cc] = o0; E[cc | pbit] = o1;
-                lm = fmax(lm, fmax(o0.x * o0.x + o0.y * o0.y, o1.x * o1.x + o1.y * o1.y));
+                o0 = cmul(f0, a);
+                o1 = cmul(f1, cneg_if(a, sgn));
+                const Q m0 = IO::st(E, cc, o0), m1 = IO::st(E, cc | pbit, o1);
+                lm = fmax(lm, fmax(m0, m1));
             } else if constexpr (KIND == DCS_KIND_MIX) {
                 const uint64_t d = cc ^ Ka;
-                o0 = cadd(cmul(f0, a[u]), cmul(f1, cneg_if(b[u], neg_sign(d, beta, ov))));
-                o1 = cadd(cmul(f0, b[u]), cmul(f1, cneg_if(a[u], neg_sign(cc, beta, ov))));
-                o0 = cscale(o0, sc); o1 = cscale(o1, sc);
-                E[cc] = o0; E[d] = o1;
-                lm = fmax(lm, fmax(o0.x * o0.x + o0.y * o0.y, o1.x * o1.x + o1.y * o1.y));
+                o0 = cadd(cmul(f0, a), cmul(f1, cneg_if(b, sgn ^ pKa)));
+                o1 = cadd(cmul(f0, b), cmul(f1, cneg_if(a, sgn)));
+                const Q m0 = IO::st(E, cc, o0), m1 = IO::st(E, d, o1);
+                lm = fmax(lm, fmax(m0, m1));
             } else if constexpr (KIND == DCS_KIND_DIAG) {
-                o0 = cmul(cadd(f0, cneg_if(f1, neg_sign(cc, beta, ov))), a[u]);
-                o0 = cscale(o0, sc);
-                E[cc] = o0;
-                lm = fmax(lm, o0.x * o0.x + o0.y * o0.y);
+                o0 = cmul(cadd(f0, cneg_if(f1, sgn)), a);
+                lm = fmax(lm, IO::st(E, cc, o0));
             } else if constexpr (KIND == DCS_KIND_REPLACE) {
                 const uint64_t d = cc ^ K;
-                o0 = cmul(f0, cadd(a[u], b[u]));
-                o1 = cmul(f1, cadd(cneg_if(a[u], neg_sign(cc, beta, ov)), cneg_if(b[u], neg_sign(d, beta, ov))));
-                o0 = cscale(o0, sc); o1 = cscale(o1, sc);
-                E[cc] = o0; E[d] = o1;
-                lm = fmax(lm, fmax(o0.x * o0.x + o0.y * o0.y, o1.x * o1.x + o1.y * o1.y));
+                o0 = cmul(f0, cadd(a, b));
+                o1 = cmul(f1, cadd(cneg_if(a, sgn), cneg_if(b, sgn ^ pK)));
+                const Q m0 = IO::st(E, cc, o0), m1 = IO::st(E, d, o1);
+                lm = fmax(lm, fmax(m0, m1));
             } else if constexpr (KIND == DCS_KIND_FIXED) {
-                o0 = cmul(y ? cneg_if(f1, neg_sign(cc, beta, ov)) : f0, a[u]);
-                o0 = cscale(o0, sc);
-                E[cc] = o0;
-                lm = fmax(lm, o0.x * o0.x + o0.y * o0.y);
+                o0 = cmul(y ? cneg_if(f1, sgn) : f0, a);
+                lm = fmax(lm, IO::st(E, cc, o0));
             } else if constexpr (KIND == DCS_KIND_FIXED_SHRINK) {
-                const uint64_t d = cc ^ K;
-                o0 = y ? cmul(f1, cadd(cneg_if(a[u], neg_sign(cc, beta, ov)), cneg_if(b[u], neg_sign(d, beta, ov))))
-                       : cmul(f0, cadd(a[u], b[u]));
-                o0 = cscale(o0, sc);
-                E[cc] = o0;
-                lm = fmax(lm, o0.x * o0.x + o0.y * o0.y);
+                o0 = y ? cmul(f1, cadd(cneg_if(a, sgn), cneg_if(b, sgn ^ pK))) : cmul(f0, cadd(a, b));
+                lm = fmax(lm, IO::st(E, cc, o0));
             } else if constexpr (KIND == DCS_KIND_SHRINK4) {
-                const uint64_t c1 = cc ^ K, d = cc ^ Ka, d1 = d ^ K;
-                o0 = cadd(cmul(f0, cadd(a[u], b[u])),
-                          cmul(f1, cadd(cneg_if(g[u], neg_sign(d, beta, ov)), cneg_if(h[u], neg_sign(d1, beta, ov)))));
-                o1 = cadd(cmul(f0, cadd(g[u], h[u])),
-                          cmul(f1, cadd(cneg_if(a[u], neg_sign(cc, beta, ov)), cneg_if(b[u], neg_sign(c1, beta, ov)))));
-                o0 = cscale(o0, sc); o1 = cscale(o1, sc);
-                E[cc] = o0; E[d] = o1;
-                lm = fmax(lm, fmax(o0.x * o0.x + o0.y * o0.y, o1.x * o1.x + o1.y * o1.y));
+                const uint64_t d = cc ^ Ka;
+                const int sd = sgn ^ pKa;
+                o0 = cadd(cmul(f0, cadd(a, b)), cmul(f1, cadd(cneg_if(g, sd), cneg_if(h, sd ^ pK))));
+                o1 = cadd(cmul(f0, cadd(g, h)), cmul(f1, cadd(cneg_if(a, sgn), cneg_if(b, sgn ^ pK))));
+                const Q m0 = IO::st(E, cc, o0), m1 = IO::st(E, d, o1);
+                lm = fmax(lm, fmax(m0, m1));
             } else {  // DCS_KIND_SHRINK2
-                const uint64_t d = cc ^ K;
-                o0 = cadd(cmul(cadd(f0, cneg_if(f1, neg_sign(cc, beta, ov))), a[u]),
-                          cmul(cadd(f0, cneg_if(f1, neg_sign(d, beta, ov))), b[u]));
-                o0 = cscale(o0, sc);
-                E[cc] = o0;
-                lm = fmax(lm, o0.x * o0.x + o0.y * o0.y);
+                o0 = cadd(cmul(cadd(f0, cneg_if(f1, sgn)), a), cmul(cadd(f0, cneg_if(f1, sgn ^ pK)), b));
+                lm = fmax(lm, IO::st(E, cc, o0));
             }
         }
     }
-    const unsigned long long bm = block_max_u64(max_bits(lm));
+    const unsigned long long bm = block_max_u64(max_bits((R)lm));
     if (threadIdx.x == 0 && bm) atomicMax(&mb[s + 1], bm);
 }
 
@@ -200,11 +227,12 @@ k_ref_step(S* __restrict__ E, uint64_t norbits, const uint64_t* __restrict__ T, 
 
 constexpr int kThreads = 256;
 
-template <class S, int KIND>
-int launch_kind(S* table, uint64_t table_stride, const dcs_step& st, int s, const dcs_param* params,
+template <class S, int KIND, class M = S>
+int launch_kind(M* table, uint64_t table_stride, const dcs_step& st, int s, const dcs_param* params,
                 uint64_t param_stride, unsigned long long* maxbits, uint64_t mstride, dcs_scale* scale,
                 int nitems, cudaStream_t stream) {
-    constexpr int ORB = sizeof(S) == 8 ? 4 : 2;
+    // orbits in flight per thread: 64 B of loads for MIX-like kinds at every entry size
+    constexpr int ORB = sizeof(M) == 16 ? 2 : (sizeof(M) == 8 ? 4 : 8);
     const uint64_t norbits = 1ull << st.m;
     const uint64_t per_block = (uint64_t)kThreads * ORB;
     uint64_t blocks = (norbits + per_block - 1) / per_block;
@@ -212,19 +240,19 @@ int launch_kind(S* table, uint64_t table_stride, const dcs_step& st, int s, cons
     if (blocks > cap) blocks = cap;
     if (blocks < 1) blocks = 1;
     dim3 grid((unsigned)blocks, (unsigned)nitems);
-    k_step<S, KIND, ORB><<<grid, kThreads, 0, stream>>>(table, table_stride, st, s, params, param_stride,
-                                                        maxbits, mstride, scale);
+    k_step<S, KIND, ORB, M><<<grid, kThreads, 0, stream>>>(table, table_stride, st, s, params, param_stride,
+                                                           maxbits, mstride, scale);
     DCS_CHECK_LAUNCH("k_step launch");
     return DCS_OK;
 }
 
-template <class S>
-int launch_step(S* table, uint64_t table_stride, const dcs_step& st, int s, const dcs_param* params,
+template <class S, class M = S>
+int launch_step(M* table, uint64_t table_stride, const dcs_step& st, int s, const dcs_param* params,
                 uint64_t param_stride, unsigned long long* maxbits, uint64_t mstride, dcs_scale* scale,
                 int nitems, cudaStream_t stream) {
     switch (st.kind) {
 #define DCS_CASE(K) \
-    case K: return launch_kind<S, K>(table, table_stride, st, s, params, param_stride, maxbits, mstride, scale, nitems, stream);
+    case K: return launch_kind<S, K, M>(table, table_stride, st, s, params, param_stride, maxbits, mstride, scale, nitems, stream);
         DCS_CASE(DCS_KIND_GROW)
         DCS_CASE(DCS_KIND_MIX)
         DCS_CASE(DCS_KIND_DIAG)
@@ -310,6 +338,9 @@ extern "C" int dcs_slice_steps_batched(int dtype, void* table, uint64_t table_st
         else if (dtype == DCS_C128)
             rc = launch_step<double2>((double2*)table, table_stride, steps[s], s, params, param_stride,
                                       (unsigned long long*)maxbits, (uint64_t)nsteps + 1, scale, nitems, st);
+        else if (dtype == DCS_H16)
+            rc = launch_step<double2, ushort2>((ushort2*)table, table_stride, steps[s], s, params, param_stride,
+                                              (unsigned long long*)maxbits, (uint64_t)nsteps + 1, scale, nitems, st);
         else {
             dcs_host::set_error("dcs_slice_steps: unknown dtype %d", dtype);
             return DCS_E_ARG;

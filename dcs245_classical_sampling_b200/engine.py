@@ -175,7 +175,7 @@ class InplaceConditionalBlockGPU:
 
     # ------------------------------------------------------------------ allocation
     def alloc(self, dtype=np.complex64, device=0, fp64_kernel_path=None, mode=None, items=None,
-              hbm_budget=None, jit=None):
+              hbm_budget=None, jit=None, storage=None):
         """Allocate device buffers (conditional_block_inplace_gpu.py:18-34).
 
         dtype: complex64 (FP32 arithmetic) or complex128 (FP64 arithmetic).
@@ -185,14 +185,24 @@ class InplaceConditionalBlockGPU:
         in the HBM budget (default 85% of free device memory).
         jit: in fused mode with register runs, run the groups as plan-specialised kernels
         compiled for this plan with NVRTC (jit.py); default: the tuned setting of this plan and
-        device (autotune_cache.json), else off."""
+        device (autotune_cache.json), else off.
+        storage: "float16" stores each entry as two IEEE binary16 components (4 bytes), combines
+        them in FP64 and rounds every stored value FP64 -> FP32 -> binary16: the reference's
+        approximate half-storage tier (kernel_opt/inplace_half_gpu.py:37-78), which halves the
+        table of complex64; complex64 dtype and the "device" / "plain" executors only."""
         if np.dtype(dtype) not in (np.dtype(np.complex64), np.dtype(np.complex128)):
             raise ValueError(dtype)
+        if storage not in (None, "float16"):
+            raise ValueError(f"storage {storage!r}")
+        half = storage == "float16"
+        if half and np.dtype(dtype) != np.dtype(np.complex64):
+            raise ValueError("Half storage exports complex64; use the complex128 executor for complex128")
         if mode is None:  # fused passes pay off once the tables are far larger than a tile
-            mode = "fused" if np.dtype(dtype) == np.dtype(np.complex64) and self.plan.maxslots >= 26 else "device"
+            mode = ("fused" if np.dtype(dtype) == np.dtype(np.complex64) and self.plan.maxslots >= 26 and not half
+                    else "device")
         if mode not in ("plain", "device", "fused"):
             raise ValueError(mode)
-        if mode == "fused" and np.dtype(dtype) != np.dtype(np.complex64):
+        if mode == "fused" and (np.dtype(dtype) != np.dtype(np.complex64) or half):
             raise ValueError("the fused executor stores complex64 tables")
         self.lib = _lib.load()
         if not torch.cuda.is_available():
@@ -201,7 +211,9 @@ class InplaceConditionalBlockGPU:
         torch.cuda.set_device(self.device)
         self.mode = mode
         self.inplace_fp64 = self.use_fp64 = np.dtype(dtype) == np.dtype(np.complex128)
-        self.dcode = _lib.C128 if self.use_fp64 else _lib.C64
+        self.half = half
+        self.inplace_storage = "float16-components" if half else np.dtype(dtype).name
+        self.dcode = _lib.H16 if half else (_lib.C128 if self.use_fp64 else _lib.C64)
         plan = self.plan
         self.inplace_steps = plan.steps
         self.inplace_maxslots = plan.maxslots
@@ -210,7 +222,7 @@ class InplaceConditionalBlockGPU:
         self.dsteps = device_steps(plan.steps)
         self.nsteps = len(plan.steps)
         tdtype = torch.complex128 if self.use_fp64 else torch.complex64
-        entry = 16 if self.use_fp64 else 8
+        entry = 16 if self.use_fp64 else (4 if half else 8)
         table_entries = 1 << plan.maxslots
         nslice_items = 1 << len(plan.slices)
         if items is None:
@@ -228,14 +240,17 @@ class InplaceConditionalBlockGPU:
             self.jit = bool(cfg.get("jit", False) if jit is None else jit)
             self.fplan = self._build_fplan()
             self.items = 1
-        self.table = torch.empty(self.items * table_entries, dtype=tdtype, device=self.device)
+        if half:  # (re, im) binary16 pairs
+            self.table = torch.empty(self.items * table_entries * 2, dtype=torch.float16, device=self.device)
+        else:
+            self.table = torch.empty(self.items * table_entries, dtype=tdtype, device=self.device)
         self.table_stride = table_entries
         self.maxbits = torch.zeros(self.items * (self._nmax() + 1), dtype=torch.int64, device=self.device)
         self.scale = torch.zeros(self.items * _lib.SCALE_DTYPE.itemsize // 8, dtype=torch.int64,
                                  device=self.device)
         self.d_params = torch.zeros(self.items * self.nsteps * _lib.PARAM_DTYPE.itemsize // 8, dtype=torch.int64,
                                     device=self.device)
-        self.one_bits = (np.array([1.0], np.float64).view(np.int64)[0] if self.use_fp64
+        self.one_bits = (np.array([1.0], np.float64).view(np.int64)[0] if self.use_fp64 or half
                          else int(np.array([1.0], np.float32).view(np.uint32)[0]))
         self.term_runs, self.term_nruns = pack_runs(plan.terminal_slots)
         self.tbasis = np.array(plan.terminal_basis + [0], dtype=np.uint64)
@@ -309,7 +324,12 @@ class InplaceConditionalBlockGPU:
         mb[:n_items, 0] = self.one_bits
         self.scale.view(self.items, -1)[:n_items].zero_()
         # empty environment = 1 at address 0 of every item (inplace_gpu.py:108)
-        self.table.view(self.items, self.table_stride)[:n_items, 0] = 1
+        if getattr(self, "half", False):
+            t = self.table.view(self.items, self.table_stride, 2)
+            t[:n_items, 0, 0] = 1
+            t[:n_items, 0, 1] = 0
+        else:
+            self.table.view(self.items, self.table_stride)[:n_items, 0] = 1
 
     def prepare(self, x_list, w=None, part=0, parts=1):
         """Host bookkeeping for a batch of prefixes and ONE host->device upload.
@@ -369,7 +389,8 @@ class InplaceConditionalBlockGPU:
                     self.dcode, _lib.ptr(self.table), self.table_stride, self.dsteps.ctypes.data, params_ptr,
                     self.nsteps, self.nsteps, s, 1, _lib.ptr(self.maxbits), _lib.ptr(self.scale), n_items, st))
                 bits = mb[:n_items, s + 1].cpu().numpy()  # host sync per step, as the reference
-                m2 = (bits.view(np.float64) if self.use_fp64 else bits.astype(np.uint32).view(np.float32))
+                m2 = (bits.view(np.float64) if self.use_fp64 or self.half
+                      else bits.astype(np.uint32).view(np.float32))
                 if not np.all(np.isfinite(m2)):
                     raise ArithmeticError("Nonfinite in-place environment")
                 if np.all(m2 == 0):
@@ -448,7 +469,8 @@ class InplaceConditionalBlockGPU:
 
     def _meta(self, seconds, part, parts, count):
         return {"seconds": seconds, "part": part, "parts": parts, "slices_evaluated": count,
-                "prefix_dtype": "complex128" if self.use_fp64 else "complex64", "rmax": self.rmax,
+                "prefix_dtype": "complex128" if self.use_fp64 else "complex64",
+                "inplace_storage": self.inplace_storage, "rmax": self.rmax,
                 "terminal_rank": self.terminal_rank, "work_per_slice": self.work,
                 "open_vertices": self.open_full,
                 "vector_scale": "sqrt(2^(n-k)); sum all complex parts before probabilities"}

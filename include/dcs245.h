@@ -50,6 +50,11 @@ extern "C" {
 /* storage types of the in-place table */
 #define DCS_C64 0  /* float2: complex64 storage, FP32 arithmetic */
 #define DCS_C128 1 /* double2: complex128 storage, FP64 arithmetic */
+/* two IEEE binary16 components per entry (4 bytes), FP64 arithmetic, each output rounded
+ * FP64 -> FP32 -> binary16 to nearest even; max bits are FP64 bits of the rounded |v|^2:
+ * the half-storage tier of the reference (source/kernel_opt/inplace_half_gpu.py), an approximate
+ * variant; the per-step executors and the terminal gather take it, the fused executors do not */
+#define DCS_H16 2
 
 /* orbit kinds (same numbering as the reference kernel's `kind`) */
 #define DCS_KIND_GROW 0

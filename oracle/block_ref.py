@@ -212,6 +212,102 @@ def execute(steps, f, yfix, fut, maxslots, dtype=np.complex128):
     return E[_addr(active)], ls, offset
 
 
+def _to_half(x):
+    """Round FP64 values to binary16 as float_to_half_((float)x) does: FP64 -> FP32 -> binary16,
+    each to nearest even (inplace_half_gpu.py:18-24)."""
+    return x.astype(np.float32).astype(np.float16)
+
+
+def execute_half(steps, f, yfix, fut, maxslots):
+    """inplace_half_gpu.py:59-78 with the orbit kernel of inplace_gpu.py:20-63 — the half-storage
+    tier: every entry is stored as two binary16 components, read back exactly into FP64, combined
+    in FP64, multiplied by 2^-e of the PREVIOUS step's max (1 before the first step), and rounded
+    on the store.  The max is taken over the stored (rounded) values, |v|^2 summed in FP32.
+
+    Returns (terminal environment as complex64, log scale, final offset), or (None, log scale,
+    offset) when a step leaves an all-zero table (inplace_half_gpu.py:74)."""
+    re = np.zeros(1 << maxslots, np.float16)
+    im = np.zeros(1 << maxslots, np.float16)
+    re[0] = 1.0
+    offset = 0
+    ls = 0.0
+    maximum = 1.0
+
+    def rd(c):
+        return re[c].astype(np.float64) + 1j * im[c].astype(np.float64)
+
+    for st in steps:
+        j = st["j"]
+        ov = (offset >> j) & 1
+        offset &= ~(1 << j)
+        f0, f1 = complex(f[st["v"]][0]), complex(f[st["v"]][1])
+        y = int(yfix[st["v"]]) if not st["free"] else 0
+        if y:
+            offset ^= fut[j]
+        e = math.frexp(maximum)[1]
+        scale = math.ldexp(1.0, -e)
+        ls += e * math.log(2.0)
+        kind, beta, K, Ka = st["kind"], st["beta"], st["K"], st["Ka"]
+        ain = st["active_in"]
+        writes = []
+        if kind == "grow":
+            c = _addr(ain)
+            a = rd(c)
+            writes = [(c, f0 * a), (c | np.uint64(1 << st["pivot"]), f1 * (a * _sgn(c, beta, ov)))]
+        elif kind == "mix" and Ka:
+            c = _addr(ain, (st["pivot_a"],))
+            d = c ^ np.uint64(Ka)
+            a, b = rd(c), rd(d)
+            writes = [(c, f0 * a + f1 * (b * _sgn(d, beta, ov))), (d, f0 * b + f1 * (a * _sgn(c, beta, ov)))]
+        elif kind == "mix":
+            c = _addr(ain)
+            writes = [(c, (f0 + f1 * _sgn(c, beta, ov)) * rd(c))]
+        elif kind == "replace":
+            c = _addr(ain, (st["pivot"],))
+            d = c ^ np.uint64(K)
+            a, b = rd(c), rd(d)
+            writes = [(c, f0 * (a + b)), (d, f1 * (a * _sgn(c, beta, ov) + b * _sgn(d, beta, ov)))]
+        elif kind == "fixed":
+            c = _addr(ain)
+            writes = [(c, (f1 * _sgn(c, beta, ov) if y else f0) * rd(c))]
+        elif kind == "fixed_shrink":
+            c = _addr(ain, (st["pivot"],))
+            d = c ^ np.uint64(K)
+            a, b = rd(c), rd(d)
+            writes = [(c, f1 * (a * _sgn(c, beta, ov) + b * _sgn(d, beta, ov)) if y else f0 * (a + b))]
+        elif kind == "shrink" and Ka:
+            c = _addr(ain, (st["pivot"], st["pivot_a"]))
+            c1 = c ^ np.uint64(K)
+            d = c ^ np.uint64(Ka)
+            d1 = d ^ np.uint64(K)
+            a, b, g, h = rd(c), rd(c1), rd(d), rd(d1)
+            writes = [(c, f0 * (a + b) + f1 * (g * _sgn(d, beta, ov) + h * _sgn(d1, beta, ov))),
+                      (d, f0 * (g + h) + f1 * (a * _sgn(c, beta, ov) + b * _sgn(c1, beta, ov)))]
+        elif kind == "shrink":
+            c = _addr(ain, (st["pivot"],))
+            d = c ^ np.uint64(K)
+            a, b = rd(c), rd(d)
+            writes = [(c, (f0 + f1 * _sgn(c, beta, ov)) * a + (f0 + f1 * _sgn(d, beta, ov)) * b)]
+        else:
+            raise ValueError(kind)
+        m2 = np.float32(0)
+        for c, v in writes:  # every orbit is read before any write: the orbits are disjoint
+            hr, hi = _to_half(v.real * scale), _to_half(v.imag * scale)
+            re[c], im[c] = hr, hi
+            r, i = hr.astype(np.float32), hi.astype(np.float32)
+            if len(r):
+                m2 = max(m2, np.max(r * r + i * i))
+        if not np.isfinite(m2):
+            raise ArithmeticError("Nonfinite half-storage environment")
+        if m2 == 0:
+            return None, ls, offset
+        maximum = math.sqrt(float(m2))
+    active = steps[-1]["active_out"] if steps else ()
+    t = _addr(active)
+    env = re[t].astype(np.float32) + 1j * im[t].astype(np.float32)
+    return env.astype(np.complex64), ls, offset
+
+
 class OracleEngine:
     """Restatement of ``InplaceConditionalBlockGPU`` (conditional_block_gpu.py:25-177 and
     conditional_block_inplace_gpu.py:18-38) on the CPU in complex128."""
@@ -309,8 +405,10 @@ class OracleEngine:
             out.append((coef, f, yfix, flips))
         return out
 
-    def block(self, x_bits, w=None, part=0, parts=1):
-        """conditional_block_gpu.py:128-177 — returns the sqrt(D)-scaled complex128 block."""
+    def block(self, x_bits, w=None, part=0, parts=1, storage=None):
+        """conditional_block_gpu.py:128-177 — returns the sqrt(D)-scaled complex128 block.
+
+        storage="float16" contracts every slice with the half-storage executor (execute_half)."""
         k = len(self.open_full)
         total = np.zeros(1 << k, np.complex128)
         count = 0
@@ -318,13 +416,18 @@ class OracleEngine:
             count += 1
             if not coef:
                 continue
-            env, ls, offset = execute(self.steps, f, yfix, self.fut, self.maxslots)
+            if storage == "float16":
+                env, ls, offset = execute_half(self.steps, f, yfix, self.fut, self.maxslots)
+                if env is None:
+                    continue
+            else:
+                env, ls, offset = execute(self.steps, f, yfix, self.fut, self.maxslots)
             if not np.any(env):
                 continue
             freeflip = sum(int(flips[q]) << j for j, q in enumerate(self.open_red))
             idx = self.syndrome_map ^ np.uint64((offset >> self.stop) ^ freeflip)
             c = coef * math.exp(ls - (self.N_full - self.n + k) * 0.5 * math.log(2.0))
-            total[idx.astype(np.int64)] += env * c
+            total[idx.astype(np.int64)] += env.astype(np.complex128) * c  # FP64, as the reference
         tail(total, k, self.phase, [self.U_full[q] for q in self.open_full])
         return total, {"slices_evaluated": count, "terminal_rank": len(self.terminal_basis)}
 

@@ -214,14 +214,37 @@ def test_draw_errors():
         draw_checked(np.ones(6, complex), 0.5)
 
 
+@pytest.mark.parametrize("mode", ["device", "plain"])
+@pytest.mark.parametrize("name", CASES)
+def test_half_storage_matches_oracle(golden, name, mode):
+    """The half-storage tier (inplace_half_gpu.py): binary16 tables, FP64 arithmetic, rounding
+    FP64 -> FP32 -> binary16 on every store, max of the stored values.  Against the oracle's
+    emulation of the same executor the block agrees to FP64 rounding (a differently ordered FP64
+    sum flips a binary16 rounding with probability ~2^-40 per entry); against the exact
+    reference block it is within the tier's own error."""
+    from oracle import block_ref
+    case, arrays = golden(name)
+    eng = _engine(case, arrays, np.complex64, mode=mode, storage="float16")
+    assert eng.table.dtype == torch.float16
+    oeng = block_ref.OracleEngine(arrays["graph"], arrays["unitaries"], case["n"], case["order"],
+                                  case["parity_operations"], case["open_vertices"])
+    for rec in case["protocol"]["records"][: (1 if name == "c2" else None)]:
+        v, meta = eng.block(_x(rec))
+        assert meta["inplace_storage"] == "float16-components"
+        want, _ = oeng.block(_x(rec), storage="float16")
+        got = v.cpu().numpy()
+        assert rel_l2(got, want) < 1e-9, rel_l2(got, want)
+        assert rel_l2(got, arrays[f"block_{rec['sample_id']}"]) < 5e-3
+
+
 def test_nonfinite_table_raises(golden):
     """An infinite maximum raises ArithmeticError (inplace_gpu.py:121).  NaN entries are
     dropped by fmax exactly as in the reference kernel, so an all-NaN table reads as zero:
     the slice is skipped and the draw of the resulting zero block raises."""
     from dcs245_classical_sampling_b200.sampling import draw_checked
     case, arrays = golden("c1")
-    for dtype in (np.complex64, np.complex128):
-        eng = _engine(case, arrays, dtype)
+    for dtype, storage in ((np.complex64, None), (np.complex128, None), (np.complex64, "float16")):
+        eng = _engine(case, arrays, dtype, storage=storage)
         with pytest.raises(ArithmeticError):
             eng.block(_x(case["protocol"]["records"][0]), w=np.array([1e300, 1e300]) if dtype == np.complex128
                       else np.array([1e30, 1e30]))

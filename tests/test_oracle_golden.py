@@ -109,3 +109,34 @@ def test_oracle_matches_brute_force():
             ov = abs(np.vdot(got, want)) / np.linalg.norm(got) / np.linalg.norm(want)
             assert ov == pytest.approx(1.0, abs=1e-12)
             assert np.linalg.norm(got) == pytest.approx(np.linalg.norm(want), rel=1e-12)
+
+
+@pytest.mark.parametrize("name", ["c1", "small"])
+def test_half_storage_oracle_is_close_to_reference(golden, name):
+    """The half-storage executor (inplace_half_gpu.py) is approximate: binary16 rounding of every
+    stored value leaves the block within a few 1e-3 of the exact one, and not equal to it."""
+    case, arrays = golden(name)
+    eng = _engine(case, arrays)
+    for rec in case["protocol"]["records"]:
+        x = np.array([int(c) for c in rec["input_data_bits"]], np.uint8)
+        got, meta = eng.block(x, storage="float16")
+        err = rel_l2(got, arrays[f"block_{rec['sample_id']}"])
+        assert 1e-6 < err < 5e-3, err
+
+
+def test_half_storage_rounding_order():
+    """FP64 -> FP32 -> binary16, each to nearest even (inplace_half_gpu.py:18-24): a value just
+    above a binary16 tie that FP32 rounds onto the tie goes to the even neighbour."""
+    one_ulp = 2.0 ** -10
+    tie = 1.0 + one_ulp / 2                       # halfway between 1 and 1 + 2^-10
+    x = np.array([tie + 2.0 ** -40, tie + 2.0 ** -20, -tie - 2.0 ** -40])
+    got = block_ref._to_half(x).astype(np.float64)
+    assert list(got) == [1.0, 1.0 + one_ulp, -1.0]
+
+
+def test_half_storage_zero_table_is_skipped():
+    """A step that leaves an all-zero table ends the slice (inplace_half_gpu.py:74)."""
+    step = {"j": 0, "v": 0, "free": True, "kind": "mix", "beta": 0, "K": 0, "Ka": 0,
+            "active_in": (), "active_out": ()}
+    env, ls, offset = block_ref.execute_half([step], {0: np.array([0.0, 0.0])}, {}, [0], 1)
+    assert env is None and offset == 0

@@ -64,3 +64,16 @@ def test_workload_sizes():
     for name, (n, depth, t, seed, k, npar) in WORKLOADS.items():
         w = build_workload(name)
         assert w["N"] == n + t and len(w["open_vertices"]) == k and len(w["parity_operations"]) == npar
+
+
+def test_half_storage_argument_errors(golden):
+    """alloc rejects the half-storage tier with complex128, with the fused executor, and unknown
+    storage names, before touching a device."""
+    case, arrays = golden("c1")
+    from dcs245_classical_sampling_b200.engine import InplaceConditionalBlockGPU
+    eng = InplaceConditionalBlockGPU(arrays["graph"], arrays["unitaries"], case["n"], case["order"],
+                                     case["parity_operations"], case["open_vertices"])
+    for kw in ({"dtype": np.complex128, "storage": "float16"}, {"mode": "fused", "storage": "float16"},
+               {"storage": "bfloat16"}):
+        with pytest.raises(ValueError):
+            eng.alloc(**kw)
