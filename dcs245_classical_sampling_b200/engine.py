@@ -196,7 +196,7 @@ class InplaceConditionalBlockGPU:
             raise ValueError(f"storage {storage!r}")
         half = storage == "float16"
         if half and np.dtype(dtype) != np.dtype(np.complex64):
-            raise ValueError("Half storage exports complex64; use the complex128 executor for complex128")
+            raise ValueError("Half storage exports complex64; use baseline executor for complex128")
         if mode is None:  # fused passes pay off once the tables are far larger than a tile
             mode = ("fused" if np.dtype(dtype) == np.dtype(np.complex64) and self.plan.maxslots >= 26 and not half
                     else "device")
@@ -469,8 +469,7 @@ class InplaceConditionalBlockGPU:
 
     def _meta(self, seconds, part, parts, count):
         return {"seconds": seconds, "part": part, "parts": parts, "slices_evaluated": count,
-                "prefix_dtype": "complex128" if self.use_fp64 else "complex64",
-                "inplace_storage": self.inplace_storage, "rmax": self.rmax,
+                "prefix_dtype": "complex128" if self.use_fp64 else "complex64", "rmax": self.rmax,
                 "terminal_rank": self.terminal_rank, "work_per_slice": self.work,
                 "open_vertices": self.open_full,
                 "vector_scale": "sqrt(2^(n-k)); sum all complex parts before probabilities"}
@@ -483,3 +482,27 @@ class InplaceConditionalBlockGPU:
             self.alloc()
         out, _ = self._run(list(x_list), w)
         return out
+
+
+class HalfConditionalBlockGPU(InplaceConditionalBlockGPU):
+    """Drop-in for the reference's half-storage engine (sampling/conditional_block_half_gpu.py:11-35):
+    binary16 tables with FP64 arithmetic (``alloc(storage="float16")``), and the block's meta
+    annotated with the storage, as the reference's worker and verifier expect
+    (production/worker.py:86, production/verify.py:460-462)."""
+
+    HALF_META = {"intermediate_storage": "float16 real/imaginary components",
+                 "local_arithmetic": "FP64 then float32-to-float16 rounded storage",
+                 "coherent_accumulation": "complex128",
+                 "approximation_scope": "Whole-vector quality requires independent FP64 validation"}
+
+    def alloc(self, dtype=np.complex64, device=0, fp64_kernel_path=None, mode=None, items=None,
+              hbm_budget=None, jit=None, storage="float16"):
+        if storage != "float16":
+            raise ValueError("HalfConditionalBlockGPU stores float16 components")
+        return super().alloc(dtype=dtype, device=device, fp64_kernel_path=fp64_kernel_path, mode=mode,
+                             items=items, hbm_budget=hbm_budget, storage="float16")
+
+    def block(self, *args, **kwargs):
+        vector, meta = super().block(*args, **kwargs)
+        meta.update(self.HALF_META)
+        return vector, meta

@@ -228,13 +228,33 @@ def test_half_storage_matches_oracle(golden, name, mode):
     assert eng.table.dtype == torch.float16
     oeng = block_ref.OracleEngine(arrays["graph"], arrays["unitaries"], case["n"], case["order"],
                                   case["parity_operations"], case["open_vertices"])
+    assert eng.inplace_storage == "float16-components"
     for rec in case["protocol"]["records"][: (1 if name == "c2" else None)]:
         v, meta = eng.block(_x(rec))
-        assert meta["inplace_storage"] == "float16-components"
+        assert meta["prefix_dtype"] == "complex64"
         want, _ = oeng.block(_x(rec), storage="float16")
         got = v.cpu().numpy()
         assert rel_l2(got, want) < 1e-9, rel_l2(got, want)
         assert rel_l2(got, arrays[f"block_{rec['sample_id']}"]) < 5e-3
+
+
+def test_half_engine_class_matches_reference_surface(golden):
+    """HalfConditionalBlockGPU: the reference class name, alloc(dtype, device), the meta
+    annotations its worker and verifier read, and the same block as alloc(storage="float16")."""
+    from dcs245_classical_sampling_b200.engine import HalfConditionalBlockGPU
+    case, arrays = golden("small")
+    eng = HalfConditionalBlockGPU(arrays["graph"], arrays["unitaries"], case["n"], case["order"],
+                                  case["parity_operations"], case["open_vertices"])
+    eng.alloc(np.complex64, 0)
+    plain = _engine(case, arrays, np.complex64, mode="device", storage="float16")
+    rec = case["protocol"]["records"][0]
+    v, meta = eng.block(_x(rec))
+    w, _ = plain.block(_x(rec))
+    assert torch.equal(v, w)
+    assert meta["intermediate_storage"] == "float16 real/imaginary components"
+    assert meta["prefix_dtype"] == "complex64" and meta["parts"] == 1
+    with pytest.raises(ValueError):
+        eng.alloc(np.complex128)
 
 
 def test_nonfinite_table_raises(golden):
