@@ -55,6 +55,7 @@ _D = ctypes.c_double
 # name: (restype, argtypes)
 SIGNATURES = {
     "dcs_abi_version": (_I, []),
+    "dcs_prefix_cut_ranks": (_I, [_P, _I, _P, _I, _P]),
     "dcs_last_error": (ctypes.c_char_p, []),
     "dcs_sm_count": (_I, []),
     "dcs_struct_size": (ctypes.c_size_t, [_I]),

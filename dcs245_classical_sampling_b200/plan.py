@@ -255,49 +255,19 @@ def deposit_runs(mask: int):
 # cut ranks and the greedy parity-slice chooser (planner; CPU)
 # ---------------------------------------------------------------------------
 
-def _pack_rows(M):
-    """uint8 (R, C) -> uint64 (R, ceil(C/64)) little-endian bit packing."""
-    R, C = M.shape
-    W = (C + 63) // 64
-    pad = np.zeros((R, W * 64), dtype=np.uint8)
-    pad[:, :C] = M
-    bits = np.packbits(pad.reshape(R, W, 64)[:, :, ::-1], axis=2)  # MSB-first per 64
-    return bits.view(">u8").reshape(R, W).astype(np.uint64)
-
-
 def prefix_cut_ranks(A, order):
-    """Cut rank of every proper prefix of `order` on the induced subgraph (length M-1)."""
-    order = list(order)
+    """Cut rank of every proper prefix of `order` on the induced subgraph (length M-1), as
+    prefix_ranks_matrix (parity_slicing.py:35-54) computes it; native GF(2) elimination in the
+    library (dcs_prefix_cut_ranks)."""
+    from . import _lib
+    order = np.ascontiguousarray(np.asarray(list(order), dtype=np.int32))
     M = len(order)
     if M < 2:
         return np.zeros(0, dtype=np.int64)
-    As = np.asarray(A, dtype=np.uint8)[np.ix_(order, order)]
-    G = np.zeros((M, 2 * M), dtype=np.uint8)
-    G[:, 0::2] = np.eye(M, dtype=np.uint8)
-    G[:, 1::2] = As
-    P = _pack_rows(G)
-    r = 0
-    piv = np.zeros(2 * M, dtype=np.int64)
-    for c in range(2 * M):
-        w, b = divmod(c, 64)
-        bit = np.uint64(1) << np.uint64(b)
-        col = (P[r:, w] & bit) != 0
-        nz = np.flatnonzero(col)
-        if nz.size == 0:
-            continue
-        p = r + int(nz[0])
-        if p != r:
-            P[[r, p]] = P[[p, r]]
-        rows = np.flatnonzero((P[:, w] & bit) != 0)
-        rows = rows[rows != r]
-        if rows.size:
-            P[rows] ^= P[r]
-        piv[c] = 1
-        r += 1
-        if r == M:
-            break
-    cum = np.cumsum(piv)
-    return np.array([cum[2 * i - 1] - i for i in range(1, M)], dtype=np.int64)
+    A = np.ascontiguousarray(np.asarray(A, dtype=np.uint8))
+    out = np.zeros(M - 1, dtype=np.int32)
+    _lib.check(_lib.load().dcs_prefix_cut_ranks(A.ctypes.data, A.shape[0], order.ctypes.data, M, out.ctypes.data))
+    return out.astype(np.int64)
 
 
 def _profile_cost(A, order):

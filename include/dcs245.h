@@ -200,6 +200,13 @@ int dcs_sm_count(void);
  * 6 dcs_tile_run. */
 size_t dcs_struct_size(int which);
 
+/* Host planner (no device work): the GF(2) cut rank of every proper prefix of a vertex order on
+ * the induced subgraph, ranks[i-1] = rank A[order[0..i-1], order[i..m-1]] for i = 1..m-1.
+ * adj: n x n symmetric 0/1 bytes, row-major; order: m distinct vertices.  Replaces
+ * prefix_ranks_matrix (source/dcs_rankwidth/parity_slicing.py:35-54), the cost of every trial in
+ * choose_parity_slices (:62-105). */
+int dcs_prefix_cut_ranks(const uint8_t *adj, int n, const int32_t *order, int m, int32_t *ranks);
+
 /* Reference-compatible single step (kernel `inplace_step`, inplace_gpu.py:20-63): the same
  * arguments in the same order, with the address table T (nb x 256 uint64, device) and a
  * host-chosen scale.  `dmax` receives atomicMax of the float/double bits of |x|^2 and must be

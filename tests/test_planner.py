@@ -77,3 +77,35 @@ def test_half_storage_argument_errors(golden):
                {"storage": "bfloat16"}):
         with pytest.raises(ValueError):
             eng.alloc(**kw)
+
+
+def test_native_cut_ranks_equal_gf2_rank_of_each_cut():
+    """dcs_prefix_cut_ranks against a plain GF(2) rank of A[prefix, suffix] on random graphs,
+    including orders over a subset of the vertices (the chooser's `alive` lists)."""
+    rng = np.random.default_rng(11)
+
+    def gf2_rank(M):
+        M = M.copy() % 2
+        r = 0
+        for c in range(M.shape[1]):
+            p = [i for i in range(r, M.shape[0]) if M[i, c]]
+            if not p:
+                continue
+            M[[r, p[0]]] = M[[p[0], r]]
+            for i in range(M.shape[0]):
+                if i != r and M[i, c]:
+                    M[i] ^= M[r]
+            r += 1
+        return r
+
+    for n, dens in ((5, 0.5), (17, 0.3), (70, 0.1), (130, 0.05)):
+        A = (rng.random((n, n)) < dens).astype(np.uint8)
+        A = np.triu(A, 1)
+        A = A | A.T
+        for sub in (n, max(2, n - 3)):
+            order = [int(v) for v in rng.permutation(n)[:sub]]
+            got = P.prefix_cut_ranks(A, order)
+            want = [gf2_rank(A[np.ix_(order[:i], order[i:])]) for i in range(1, sub)]
+            assert list(got) == want
+    with pytest.raises(Exception):
+        P.prefix_cut_ranks(np.zeros((3, 3), np.uint8), [0, 1, 5])
