@@ -25,7 +25,8 @@ STEP_DTYPE = np.dtype([
 ])
 PARAM_DTYPE = np.dtype([("f0r", "<f8"), ("f0i", "<f8"), ("f1r", "<f8"), ("f1i", "<f8"),
                         ("ov", "<i4"), ("y", "<i4")])
-SCALE_DTYPE = np.dtype([("logscale", "<f8"), ("exponent_sum", "<i8"), ("flags", "<u4"), ("pad", "<u4")])
+SCALE_DTYPE = np.dtype([("logscale", "<f8"), ("exponent_sum", "<i8"), ("flags", "<u4"), ("pad", "<u4"),
+                        ("phase", "<f8")])
 GROUP_DTYPE = np.dtype([
     ("first", "<i4"), ("count", "<i4"), ("tile_dim", "<i4"), ("low_bits", "<i4"),
     ("coset_m", "<i4"), ("ncoset_runs", "<i4"), ("step_tile_off", "<i4"), ("variant", "<i4"),

@@ -51,7 +51,14 @@ k_accumulate(const S* __restrict__ table, uint64_t table_stride, const __grid_co
             const uint64_t c = deposit(i, tm.runs, tm.nruns);
             const double2 v = entry_f64(table[(uint64_t)it * table_stride + c]);
             const double m = exp(sc.logscale - log_shift);
-            const double cr = coefs[2 * it] * m, ci = coefs[2 * it + 1] * m;
+            double cr = coefs[2 * it] * m, ci = coefs[2 * it + 1] * m;
+            if (sc.phase != 0.0) {  // step factors divided out by the plan-specialised kernels
+                double sp, cp;
+                sincos(sc.phase, &sp, &cp);
+                const double r = cr * cp - ci * sp;
+                ci = cr * sp + ci * cp;
+                cr = r;
+            }
             const double vr = v.x, vi = v.y;
             acc.x += vr * cr - vi * ci;
             acc.y += vr * ci + vi * cr;

@@ -12,10 +12,14 @@
 // dcs_param and dcs_scale in include/dcs245.h (the library checks their sizes).
 #pragma once
 
+#ifdef __CUDACC_RTC__
 typedef unsigned int uint32_t;
 typedef unsigned long long uint64_t;
 typedef long long int64_t;
 typedef int int32_t;
+#else  // the same source built offline with nvcc (register and spill checks)
+#include <stdint.h>
+#endif
 
 struct jit_param {
     double f0r, f0i, f1r, f1i;
@@ -25,6 +29,7 @@ struct jit_scale {
     double logscale;
     int64_t exponent_sum;
     uint32_t flags, pad;
+    double phase;
 };
 
 #define JK_GROW 0
@@ -64,43 +69,44 @@ __device__ __forceinline__ float2 zaddg(float2 a, float2 b) {
 }
 
 // ---------------------------------------------------------------- orbit bodies
+// The weights are unit weights (prologue): f0 = 1 at every free step, and at a fixed step the
+// weight its y selects is 1, so no body multiplies by f0.
+//
 // One-vector kinds along local bit K: orbits {j, j | 2^K} for j with bit K clear and no DEAD
 // bit.  Sign of representative j: (-1)^(m0 + <j, B>), so F1p / F1n = s f1 for <j, B> even /
 // odd.  SK / SKA: the partner signs (-1)^sK, (-1)^sKa.  Formulas: the per-step kernel's
-// (reference: source/kernel_opt/inplace_gpu.py:29-58).
+// (reference: source/kernel_opt/inplace_gpu.py:29-58) with f0 = 1.
 template <int KIND, int R, int K, int B, int DEAD, int SK, int SKA, int J = 0>
-__device__ __forceinline__ void orb1(float2 (&v)[1 << R], float2 f0, float2 F1p, float2 F1n, float2 Fap, float2 Fan,
-                                     int y) {
+__device__ __forceinline__ void orb1(float2 (&v)[1 << R], float2 F1p, float2 F1n, float2 Fap, float2 Fan, int y) {
     if constexpr (J < (1 << R)) {
         if constexpr (!(J & (1 << K)) && !(J & DEAD)) {
             constexpr int D = J | (1 << K);
             constexpr bool N = cpar(J & B);
             const float2 F1 = N ? F1n : F1p;
             const float2 x = v[J], b = v[D];
-            if constexpr (KIND == JK_GROW) {
-                v[J] = zmul(f0, x);
+            if constexpr (KIND == JK_GROW) {  // v[J] = x stays
                 v[D] = zmul(F1, x);
             } else if constexpr (KIND == JK_MIX) {
-                v[J] = zmadd(f0, x, zmul(N ? Fan : Fap, b));
-                v[D] = zmadd(f0, b, zmul(F1, x));
+                v[J] = zmadd(N ? Fan : Fap, b, x);
+                v[D] = zmadd(F1, x, b);
             } else if constexpr (KIND == JK_REPLACE) {
-                v[J] = zmul(f0, zadd(x, b));
+                v[J] = zadd(x, b);
                 v[D] = zmul(F1, zaddg<SK>(x, b));
             } else if constexpr (KIND == JK_FIXED_SHRINK) {
-                v[J] = y ? zmul(F1, zaddg<SK>(x, b)) : zmul(f0, zadd(x, b));
+                v[J] = y ? zmul(F1, zaddg<SK>(x, b)) : zadd(x, b);
             } else {  // JK_SHRINK2
-                v[J] = zmadd(f0, zadd(x, b), zmul(F1, zaddg<SK>(x, b)));
+                v[J] = zmadd(F1, zaddg<SK>(x, b), zadd(x, b));
             }
         }
-        orb1<KIND, R, K, B, DEAD, SK, SKA, J + 1>(v, f0, F1p, F1n, Fap, Fan, y);
+        orb1<KIND, R, K, B, DEAD, SK, SKA, J + 1>(v, F1p, F1n, Fap, Fan, y);
     }
 }
 template <int KIND, int R, int K, int B, int DEAD, int SK, int SKA>
 __device__ __forceinline__ void body1(float2 (&v)[1 << R], float4 f, int y, uint32_t m0) {
-    const float2 f0 = f2(f.x, f.y), f1 = f2(f.z, f.w);
+    const float2 f1 = f2(f.z, f.w);
     const float2 F1p = sflip(f1, m0), F1n = sflip(f1, m0 ^ kSign);
     constexpr uint32_t ka = SKA ? kSign : 0u;
-    orb1<KIND, R, K, B, DEAD, SK, SKA>(v, f0, F1p, F1n, sflip(F1p, ka), sflip(F1n, ka), y);
+    orb1<KIND, R, K, B, DEAD, SK, SKA>(v, F1p, F1n, sflip(F1p, ka), sflip(F1n, ka), y);
 }
 
 // One-entry kinds: every local entry without a DEAD bit.
@@ -113,39 +119,38 @@ __device__ __forceinline__ void orb0(float2 (&v)[1 << R], float2 Fp, float2 Fn) 
 }
 template <int KIND, int R, int B, int DEAD>
 __device__ __forceinline__ void body0(float2 (&v)[1 << R], float4 f, int y, uint32_t m0) {
-    const float2 f0 = f2(f.x, f.y), f1 = f2(f.z, f.w);
+    const float2 f1 = f2(f.z, f.w);
     const float2 F1p = sflip(f1, m0), F1n = sflip(f1, m0 ^ kSign);
-    if constexpr (KIND == JK_DIAG) {  // (f0 + s f1) x
-        orb0<R, B, DEAD>(v, zadd(f0, F1p), zadd(f0, F1n));
-    } else {  // JK_FIXED: y ? s f1 x : f0 x
+    if constexpr (KIND == JK_DIAG) {  // (1 + s f1) x
+        orb0<R, B, DEAD>(v, f2(1.f + F1p.x, F1p.y), f2(1.f + F1n.x, F1n.y));
+    } else {  // JK_FIXED: y ? s x : x (the selected weight is 1)
         if (y) orb0<R, B, DEAD>(v, F1p, F1n);
-        else orb0<R, 0, DEAD>(v, f0, f0);
     }
 }
 
 // Four-entry shrink along local bits K1 (K's role) and K2 (Ka's role); MIX bit 0: K's local
 // mask also has K2, bit 1: Ka's has K1.
-//   o_c = f0 (x + b) + s_d f1 (g + gK h) ;  o_{c^Ka} = f0 (g + h) + s_c f1 (x + gK b).
+//   o_c = (x + b) + s_d f1 (g + gK h) ;  o_{c^Ka} = (g + h) + s_c f1 (x + gK b).
 template <int R, int K1, int K2, int MIX, int B, int DEAD, int SK, int J = 0>
-__device__ __forceinline__ void orb4(float2 (&v)[1 << R], float2 f0, float2 F1p, float2 F1n, float2 Fap, float2 Fan) {
+__device__ __forceinline__ void orb4(float2 (&v)[1 << R], float2 F1p, float2 F1n, float2 Fap, float2 Fan) {
     if constexpr (J < (1 << R)) {
         if constexpr (!(J & ((1 << K1) | (1 << K2))) && !(J & DEAD)) {
             constexpr int MK = (1 << K1) | ((MIX & 1) ? (1 << K2) : 0);
             constexpr int MKA = (1 << K2) | ((MIX & 2) ? (1 << K1) : 0);
             constexpr bool N = cpar(J & B);
             const float2 x = v[J], b = v[J ^ MK], g = v[J ^ MKA], h = v[J ^ MK ^ MKA];
-            v[J] = zmadd(f0, zadd(x, b), zmul(N ? Fan : Fap, zaddg<SK>(g, h)));
-            v[J ^ MKA] = zmadd(f0, zadd(g, h), zmul(N ? F1n : F1p, zaddg<SK>(x, b)));
+            v[J] = zmadd(N ? Fan : Fap, zaddg<SK>(g, h), zadd(x, b));
+            v[J ^ MKA] = zmadd(N ? F1n : F1p, zaddg<SK>(x, b), zadd(g, h));
         }
-        orb4<R, K1, K2, MIX, B, DEAD, SK, J + 1>(v, f0, F1p, F1n, Fap, Fan);
+        orb4<R, K1, K2, MIX, B, DEAD, SK, J + 1>(v, F1p, F1n, Fap, Fan);
     }
 }
 template <int R, int K1, int K2, int MIX, int B, int DEAD, int SK, int SKA>
 __device__ __forceinline__ void body4(float2 (&v)[1 << R], float4 f, int y, uint32_t m0) {
-    const float2 f0 = f2(f.x, f.y), f1 = f2(f.z, f.w);
+    const float2 f1 = f2(f.z, f.w);
     const float2 F1p = sflip(f1, m0), F1n = sflip(f1, m0 ^ kSign);
     constexpr uint32_t ka = SKA ? kSign : 0u;
-    orb4<R, K1, K2, MIX, B, DEAD, SK>(v, f0, F1p, F1n, sflip(F1p, ka), sflip(F1n, ka));
+    orb4<R, K1, K2, MIX, B, DEAD, SK>(v, F1p, F1n, sflip(F1p, ka), sflip(F1n, ka));
 }
 
 // ---------------------------------------------------------------- packed bodies
@@ -286,23 +291,46 @@ __device__ __forceinline__ int scale_exponent(double m2) {
     return e;
 }
 
-// Pass scale 2^-e from the previous pass's max (block 0 records it), the group's step weights
-// into shared memory, and the table of high tile-coordinate addresses.
-template <int TD, int LOW, int COUNT, int FIRST>
+// Unit weights: a step multiplies every entry it writes by f0 or f1, so its factor c can leave
+// the table: c = f0 (at a fixed step, the weight its y selects), the kernel applies (f0, f1) / c,
+// whose weight on c's side is exactly 1, and log|c| and arg c go into the item's scale.  The
+// scalar bodies then drop every multiplication by f0.  The host keeps f0 != 0 at the free steps
+// of items that run these kernels.
+__device__ __forceinline__ double2 step_factor(const jit_param& p, bool fixed) {
+    return (fixed && (p.y & 1)) ? make_double2(p.f1r, p.f1i) : make_double2(p.f0r, p.f0i);
+}
+__device__ __forceinline__ float4 unit_weights(const jit_param& p, bool fixed) {
+    if (fixed) return (p.y & 1) ? make_float4(0.f, 0.f, 1.f, 0.f) : make_float4(1.f, 0.f, 0.f, 0.f);
+    const double n = p.f0r * p.f0r + p.f0i * p.f0i;  // f1 / f0
+    const double wr = (p.f1r * p.f0r + p.f1i * p.f0i) / n, wi = (p.f1i * p.f0r - p.f1r * p.f0i) / n;
+    return make_float4(1.f, 0.f, (float)wr, (float)wi);
+}
+
+// Pass scale 2^-e from the previous pass's max and the group's step factors (block 0 records
+// both), the unit step weights into shared memory, and the table of high tile-coordinate
+// addresses.  FIXMASK bit i: step FIRST + i is a fixed kind.
+template <int TD, int LOW, int COUNT, int FIRST, uint32_t FIXMASK>
 __device__ __forceinline__ float prologue(const jit_param* __restrict__ params, const uint64_t* basis,
                                           const unsigned long long* maxbits, int group, jit_scale* scale,
                                           float4* fw, int* ovy, uint64_t* hi_tab) {
     const double m2prev = (double)__uint_as_float((uint32_t)maxbits[group]);
     const int e = scale_exponent(m2prev);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
-        scale->logscale += (double)e * 0.69314718055994530942;
+        double lg = 0.0, ph = 0.0;
+        for (int i = 0; i < COUNT; ++i) {
+            const double2 c = step_factor(params[FIRST + i], (FIXMASK >> i) & 1u);
+            lg += 0.5 * log(c.x * c.x + c.y * c.y);
+            ph += atan2(c.y, c.x);
+        }
+        scale->logscale += (double)e * 0.69314718055994530942 + lg;
+        scale->phase += ph;
         scale->exponent_sum += e;
         if (!isfinite(m2prev)) scale->flags |= 1u;
         else if (m2prev == 0.0) scale->flags |= 2u;
     }
     if (threadIdx.x < COUNT) {
         const jit_param p = params[FIRST + threadIdx.x];
-        fw[threadIdx.x] = make_float4((float)p.f0r, (float)p.f0i, (float)p.f1r, (float)p.f1i);
+        fw[threadIdx.x] = unit_weights(p, (FIXMASK >> threadIdx.x) & 1u);
         ovy[threadIdx.x] = (p.ov & 1) | ((p.y & 1) << 1);
     }
     for (int h = threadIdx.x; h < (1 << (TD - LOW)); h += kThreads) {

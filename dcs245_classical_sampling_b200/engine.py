@@ -220,6 +220,8 @@ class InplaceConditionalBlockGPU:
         self.inplace_rmax = plan.inplace_rmax
         self.inplace_terminal_basis = dict(zip(plan.terminal_slots, plan.terminal_basis))
         self.dsteps = device_steps(plan.steps)
+        # free steps: the plan-specialised kernels divide f0 out of their weights
+        self.free_steps = ~np.isin(self.dsteps["kind"], (4, 5))  # DCS_KIND_FIXED, DCS_KIND_FIXED_SHRINK
         self.nsteps = len(plan.steps)
         tdtype = torch.complex128 if self.use_fp64 else torch.complex64
         entry = 16 if self.use_fp64 else (4 if half else 8)
@@ -238,6 +240,7 @@ class InplaceConditionalBlockGPU:
                                  "max_steps": cfg.get("max_steps", 24), "variant": cfg.get("variant", 0),
                                  "pairs": cfg.get("pairs", False)}
             self.jit = bool(cfg.get("jit", False) if jit is None else jit)
+            self.jit_minb = cfg.get("minb")
             self.fplan = self._build_fplan()
             self.items = 1
         if half:  # (re, im) binary16 pairs
@@ -280,16 +283,19 @@ class InplaceConditionalBlockGPU:
         fp = build_fused_plan(self.plan, **self.fused_config)
         if getattr(self, "jit", False) and fp.tile_runs is not None:
             from .jit import JitPlan
-            fp.jit = JitPlan(self.plan, fp, self.lib)
+            fp.jit = JitPlan(self.plan, fp, self.lib, minb=getattr(self, "jit_minb", None))
         return fp
 
-    def set_fused_config(self, jit=None, **cfg):
+    def set_fused_config(self, jit=None, minb=None, **cfg):
         """Rebuild the fused plan with another tile shape (max_dim, low, max_steps, variant, pairs);
-        jit=True/False switches the plan-specialised group kernels on or off."""
+        jit=True/False switches the plan-specialised group kernels on or off; minb: CTAs per SM
+        their registers are sized for (default: 2 with variant bit 0, else 3)."""
         if self.mode != "fused":
             raise ValueError("set_fused_config needs mode='fused'")
         if jit is not None:
             self.jit = bool(jit)
+        if minb is not None:
+            self.jit_minb = int(minb)
         self.fused_config = {**self.fused_config, **cfg}
         self.fplan = self._build_fplan()
         self.maxbits = torch.zeros(self.items * (len(self.fplan.groups) + 1), dtype=torch.int64, device=self.device)
@@ -308,6 +314,7 @@ class InplaceConditionalBlockGPU:
             self.fplan.jit.close()
         rep = at.tune(self, prm, jit=jit, **({"candidates": candidates} if candidates else {}))
         self.jit = jit
+        self.jit_minb = rep["best"].get("minb")
         self.fused_config = {k: rep["best"][k] for k in ("max_dim", "low", "max_steps", "variant", "pairs")}
         self.scale = torch.zeros(self.items * _lib.SCALE_DTYPE.itemsize // 8, dtype=torch.int64,
                                  device=self.device)
@@ -355,6 +362,8 @@ class InplaceConditionalBlockGPU:
                 begin.append(begin[-1] + sum(1 for it in chunk if it[0] == bb))
             chunks.append((c0, len(chunk), blocks_in[0], len(blocks_in), len(begin_all)))
             begin_all.extend(begin)
+        unit_ok = [all(self.unit_weights_ok(it[2]) for it in work[c0:c0 + cn]) if self.mode == "fused" else True
+                   for c0, cn, _, _, _ in chunks]
         host_params = (np.concatenate([it[2] for it in work]) if n else
                        np.zeros(1, _lib.PARAM_DTYPE)).view(np.int64)
         coefs = np.zeros(2 * max(1, n), np.float64)
@@ -370,17 +379,30 @@ class InplaceConditionalBlockGPU:
         o1 = host_params.size
         o2 = o1 + coefs.size
         o3 = o2 + xors.size
-        return {"n_items": n, "chunks": chunks, "counts": counts, "nblocks": len(x_list), "dev": dev,
+        return {"n_items": n, "chunks": chunks, "unit_ok": unit_ok, "counts": counts, "nblocks": len(x_list),
+                "dev": dev,
                 "pinned": pinned, "params": dev[:o1], "coefs": dev[o1:o2].view(torch.float64),
                 "xors": dev[o2:o3], "begin": dev[o3:].to(torch.int32), "h2d_bytes": blob.nbytes}
 
-    def _run_steps(self, params_ptr, n_items):
+    def unit_weights_ok(self, params):
+        """Whether an item's step weights (a dcs_param array) can run the plan-specialised kernels,
+        which divide f0 out of every free step: f0 != 0 there, and |f1 / f0| <= 2^32 so that a
+        group of steps stays inside the FP32 range between renormalisations."""
+        p = params[self.free_steps]
+        a0 = np.hypot(p["f0r"], p["f0i"])
+        return bool(np.all(a0 > 0) and np.all(np.hypot(p["f1r"], p["f1i"]) <= 2.0 ** 32 * a0))
+
+    def _run_steps(self, params_ptr, n_items, unit_ok=True):
         lib, st = self.lib, self._stream()
         nm = self._nmax() + 1
         if self.mode == "fused":
             f = self.fplan
-            _lib.check(f.launch(lib, _lib.ptr(self.table), params_ptr, 0, len(f.groups), _lib.ptr(self.maxbits),
-                                _lib.ptr(self.scale), st))
+            if unit_ok:
+                _lib.check(f.launch(lib, _lib.ptr(self.table), params_ptr, 0, len(f.groups), _lib.ptr(self.maxbits),
+                                    _lib.ptr(self.scale), st))
+            else:  # library kernels take the weights as they are
+                _lib.check(f.launch_library(lib, _lib.ptr(self.table), params_ptr, 0, len(f.groups),
+                                            _lib.ptr(self.maxbits), _lib.ptr(self.scale), st))
             return
         if self.mode == "plain":
             mb = self.maxbits.view(self.items, nm)
@@ -408,9 +430,9 @@ class InplaceConditionalBlockGPU:
         nm = self._nmax() + 1
         entry = _lib.PARAM_DTYPE.itemsize
         launches = 0
-        for c0, cn, b0, nb, boff in prep["chunks"]:
+        for ci, (c0, cn, b0, nb, boff) in enumerate(prep["chunks"]):
             self._reset_items(cn)
-            self._run_steps(_lib.ptr(prep["params"]) + c0 * self.nsteps * entry, cn)
+            self._run_steps(_lib.ptr(prep["params"]) + c0 * self.nsteps * entry, cn, prep["unit_ok"][ci])
             launches += len(self.fplan.groups) if self.mode == "fused" else self.nsteps
             flat = out[b0:b0 + nb].view(torch.float64)
             _lib.check(lib.dcs_accumulate_batched(
@@ -441,9 +463,9 @@ class InplaceConditionalBlockGPU:
         lib = self.lib
         nm = self._nmax() + 1
         entry = _lib.PARAM_DTYPE.itemsize
-        for c0, cn, b0, nb, boff in prep["chunks"]:
+        for ci, (c0, cn, b0, nb, boff) in enumerate(prep["chunks"]):
             self._reset_items(cn)
-            self._run_steps(_lib.ptr(prep["params"]) + c0 * self.nsteps * entry, cn)
+            self._run_steps(_lib.ptr(prep["params"]) + c0 * self.nsteps * entry, cn, prep["unit_ok"][ci])
             flat = out[b0:b0 + nb].view(torch.float64)
             _lib.check(lib.dcs_accumulate_batched(
                 self.dcode, _lib.ptr(self.table), self.table_stride, self.plan.terminal_rank,

@@ -23,7 +23,7 @@ from . import _lib
 HERE = Path(__file__).resolve().parent
 HEADER = HERE / "csrc" / "runs_jit.cuh"
 CACHE_DIR = HERE / "_jit_cache"
-KERNEL_VERSION = 5  # bump when the generated code changes meaning
+KERNEL_VERSION = 6  # bump when the generated code changes meaning
 
 ONE_VECTOR = (0, 1, 3, 5, 7)
 
@@ -79,6 +79,15 @@ def _direct_ok(fp, gi):
     g = fp.groups[gi]
     first, count = int(g["first"]), int(g["count"])
     return len({int(fp.tile_steps[first + s]["cskip"]) for s in range(count)}) == 1
+
+
+def _fixmask(fp, first, count):
+    """Bit s: step first + s is a fixed kind (its factor is the weight its y selects)."""
+    m = 0
+    for s in range(count):
+        if int(fp.dsteps[first + s]["kind"]) in (4, 5):  # DCS_KIND_FIXED, DCS_KIND_FIXED_SHRINK
+            m |= 1 << s
+    return m
 
 
 def group_source(plan, fp, gi, minb=3):
@@ -138,8 +147,8 @@ def group_source(plan, fp, gi, minb=3):
     L.append("    __shared__ float4 fw[COUNT];")
     L.append("    __shared__ int ovy[COUNT];")
     L.append("    __shared__ uint32_t cs_sh;")
-    L.append(f"    const float sc = jit::prologue<TD, LOW, COUNT, FIRST>(params, g{gi}_basis, maxbits, {gi}, scale, "
-             "fw, ovy, hi_tab);")
+    L.append(f"    const float sc = jit::prologue<TD, LOW, COUNT, FIRST, {_fixmask(fp, first, count)}u>(params, "
+             f"g{gi}_basis, maxbits, {gi}, scale, fw, ovy, hi_tab);")
     L.append("    float lm = 0.f;")
     L.append(f"    for (uint64_t tile = blockIdx.x; tile < {_u64(1 << int(g['coset_m']))}; tile += gridDim.x) {{")
     L.append(f"        const uint64_t base = {_deposit_expr(g)};")
@@ -333,8 +342,8 @@ def _packed_source(fp, gi, minb):
     L.append("    __shared__ float4 fw[COUNT];")
     L.append("    __shared__ int ovy[COUNT];")
     L.append("    __shared__ uint32_t cs_sh;")
-    L.append(f"    const float sc = jit::prologue<TD, LOW, COUNT, FIRST>(params, g{gi}_basis, maxbits, {gi}, scale, "
-             "fw, ovy, hi_tab);")
+    L.append(f"    const float sc = jit::prologue<TD, LOW, COUNT, FIRST, {_fixmask(fp, first, count)}u>(params, "
+             f"g{gi}_basis, maxbits, {gi}, scale, fw, ovy, hi_tab);")
     L.append("    float lm = 0.f;")
     L.append(f"    for (uint64_t tile = blockIdx.x; tile < {_u64(1 << int(g['coset_m']))}; tile += gridDim.x) {{")
     L.append(f"        const uint64_t base = {_deposit_expr(g)};")
@@ -498,6 +507,7 @@ class JitPlan:
         self._images = []
         if minb is None:
             minb = 2 if len(fp.groups) and int(fp.groups[0]["variant"]) & 1 else 3
+        self.minb = int(minb)
         sms = self.lib.dcs_sm_count()
         for img, gis in compile_plan(plan, fp, self.lib, minb, parts):
             buf = ctypes.create_string_buffer(img, len(img))

@@ -77,7 +77,7 @@ def main():
         dsteps = device_steps(steps)
         nmax = last
     maxbits = torch.zeros(nmax + 1, dtype=torch.int64, device=dev)
-    scale = torch.zeros(3, dtype=torch.int64, device=dev)
+    scale = torch.zeros(_lib.SCALE_DTYPE.itemsize // 8, dtype=torch.int64, device=dev)
     one = (int(np.array([1.0], np.float64).view(np.int64)[0]) if half
            else int(np.array([1.0], np.float32).view(np.uint32)[0]))
     per_launch = []

@@ -79,6 +79,13 @@ class DeviceCircuit:
             freeflips.append(sum(int(fl[q]) << jj for jj, q in enumerate(sp.open_red)))
         self.nslices = len(coefs)
         assert self.nslices == len(items)
+        # the plan-specialised kernels divide f0 out of the free steps' weights: every weight row
+        # a prefix can select (slices flip only f1) must pass the engine's check
+        rows = np.zeros(2 * S, _lib.PARAM_DTYPE)
+        for b in (0, 1):
+            rows["f0r"][b::2], rows["f0i"][b::2] = fsel[:, 4 * b], fsel[:, 4 * b + 1]
+            rows["f1r"][b::2], rows["f1i"][b::2] = fsel[:, 4 * b + 2], fsel[:, 4 * b + 3]
+        self.unit_ok = all(engine.unit_weights_ok(rows[b::2]) for b in (0, 1))
         self.nsteps, self.nfixed = S, nfixed
         dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(device)
         self.fsel = dev(fsel)
@@ -133,6 +140,8 @@ class CircuitRunner:
         self.lib = _lib.load()
         self.dc = DeviceCircuit(self.engine, self.device)
         assert self.dc.nslices == L
+        if self.mode == "fused" and self.engine.jit and not self.dc.unit_ok:
+            self.engine.set_fused_config(jit=False)  # weights the plan-specialised kernels cannot take
         self.max_samples = max_samples if self.mode == "fused" else max(1, min(max_samples, items // L) or 1)
         self.k = self.engine.k
         self.stream = torch.cuda.Stream(self.device)

@@ -105,6 +105,8 @@ typedef struct dcs_scale {
     int64_t exponent_sum;
     uint32_t flags; /* bit 0: a nonfinite maximum was seen; bit 1: the table became zero */
     uint32_t pad;
+    double phase;   /* radians: the argument of the step factors the plan-specialised kernels divide
+                       out of the weights (the table is e^{logscale + i phase} times its entries) */
 } dcs_scale;
 
 /* One fused pass: steps [first, first+count) applied to every coset tile of `tile_dim`

@@ -93,8 +93,37 @@ def test_plan_specialised_kernels_match_reference(golden, name, variant, pairs):
     for rec, lb in zip(case["protocol"]["records"], lib_blocks):
         v, _ = eng.block(_x(rec))
         v = v.cpu().numpy()
-        assert rel_l2(v, arrays[f"block_{rec['sample_id']}"]) < 1e-5
-        assert rel_l2(v, lb) < 1e-6
+        want = arrays[f"block_{rec['sample_id']}"]
+        err = rel_l2(v, want)
+        assert err < 1e-5
+        # the generated kernels divide f0 out of the weights (unit weights), so their FP32
+        # rounding differs from the library kernels'; their error must stay as small
+        assert err <= max(2.0 * rel_l2(lb, want), 2e-6), (err, rel_l2(lb, want))
+
+
+def test_plan_specialised_kernels_fall_back_without_unit_weights(golden):
+    """A free step whose f0 is zero (a custom reference bra orthogonal to the first column of
+    its unitary) cannot divide f0 out: that item runs the library kernels and the block still
+    equals the oracle's."""
+    from oracle import block_ref
+    case, arrays = golden("small")
+    eng = _engine(case, arrays, np.complex64, mode="fused")
+    eng.set_fused_config(variant=12, pairs=False, max_dim=13, low=4, jit=True)
+    oeng = block_ref.OracleEngine(arrays["graph"], arrays["unitaries"], case["n"], case["order"],
+                                  case["parity_operations"], case["open_vertices"])
+    n = case["n"]
+    refs = [q for q in range(n, len(arrays["graph"])) if q in eng.plan.relabel and q not in eng.plan.slices
+            and eng.plan.relabel[q] not in eng.plan.fixed]
+    q = refs[0]
+    U = np.asarray(eng.plan.U_full[q])
+    w = {r: np.array([1.0, np.exp(1j * np.pi / 4)]) for r in range(n, len(arrays["graph"]))}
+    w[q] = np.array([U[1, 0], -U[0, 0]])  # w . U[:, 0] = 0: f0 = 0 at q's step
+    x = _x(case["protocol"]["records"][0])
+    prep = eng.prepare([x], w)
+    assert not all(prep["unit_ok"])
+    v, _ = eng.block(x, w)
+    want, _ = oeng.block(x, w)
+    assert rel_l2(v.cpu().numpy(), want) < 1e-5
 
 
 @pytest.mark.parametrize("name", ["small", "c2"])
