@@ -81,8 +81,8 @@ SIGNATURES = {
     "dcs_jit_free": (None, [_P]),
     "dcs_jit_load": (_I, [_P, ctypes.POINTER(_P)]),
     "dcs_jit_unload": (_I, [_P]),
-    "dcs_jit_kernel": (_I, [_P, ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(_P), ctypes.POINTER(_I)]),
-    "dcs_jit_launch": (_I, [_P, ctypes.c_uint, ctypes.c_size_t, _P, _P, _P, _P, _P]),
+    "dcs_jit_kernel": (_I, [_P, ctypes.c_char_p, ctypes.c_size_t, _I, ctypes.POINTER(_P), ctypes.POINTER(_I)]),
+    "dcs_jit_launch": (_I, [_P, ctypes.c_uint, _I, ctypes.c_size_t, _P, _P, _P, _P, _P]),
 }
 
 

@@ -68,6 +68,7 @@ def tune(engine, params_dev, candidates=None, repeats=1, save=True, jit=False):
     for cand in candidates:
         max_dim, low, max_steps, variant, pairs = cand[:5]
         minb = cand[5] if len(cand) > 5 else None  # CTAs per SM of the generated kernels
+        threads = cand[6] if len(cand) > 6 else 256  # threads per CTA of the generated kernels
         try:
             fp = build_fused_plan(engine.plan, max_dim=max_dim, low=low, max_steps=max_steps, variant=variant,
                                   pairs=pairs)
@@ -75,7 +76,7 @@ def tune(engine, params_dev, candidates=None, repeats=1, save=True, jit=False):
             continue
         if jit and fp.tile_runs is not None:
             from .jit import JitPlan
-            fp.jit = JitPlan(engine.plan, fp, lib, minb=minb)
+            fp.jit = JitPlan(engine.plan, fp, lib, minb=minb, threads=threads)
         need = len(fp.groups) + 1
         if engine.maxbits.numel() < need:
             engine.maxbits = torch.zeros(need, dtype=torch.int64, device=engine.device)
@@ -97,7 +98,8 @@ def tune(engine, params_dev, candidates=None, repeats=1, save=True, jit=False):
         t = min(times[1:]) if len(times) > 1 else times[0]
         report.append({"max_dim": max_dim, "low": low, "max_steps": max_steps, "variant": variant,
                        "pairs": pairs, "jit": fp.jit is not None,
-                       "minb": fp.jit.minb if fp.jit is not None else None, "groups": len(fp.groups),
+                       "minb": fp.jit.minb if fp.jit is not None else None,
+                       "threads": fp.jit.threads if fp.jit is not None else None, "groups": len(fp.groups),
                        "seconds": t})
         if best is None or t < best[0]:
             if best is not None and best[2].jit is not None:
@@ -113,12 +115,14 @@ def tune(engine, params_dev, candidates=None, repeats=1, save=True, jit=False):
         data[f"{fingerprint(engine.plan)}|{torch.cuda.get_device_name(engine.device)}"] = {
             "max_dim": best[1][0], "low": best[1][1], "max_steps": best[1][2], "variant": best[1][3],
             "pairs": best[1][4], "jit": best[2].jit is not None,
-            "minb": best[2].jit.minb if best[2].jit is not None else None, "seconds": best[0]}
+            "minb": best[2].jit.minb if best[2].jit is not None else None,
+            "threads": best[2].jit.threads if best[2].jit is not None else None, "seconds": best[0]}
         try:
             CACHE.write_text(json.dumps(data, indent=1) + "\n")
         except OSError:
             pass
     return {"best": {"max_dim": best[1][0], "low": best[1][1], "max_steps": best[1][2], "variant": best[1][3],
                      "pairs": best[1][4], "jit": best[2].jit is not None,
-                     "minb": best[2].jit.minb if best[2].jit is not None else None, "seconds": best[0]},
+                     "minb": best[2].jit.minb if best[2].jit is not None else None,
+                     "threads": best[2].jit.threads if best[2].jit is not None else None, "seconds": best[0]},
             "candidates": report}

@@ -89,8 +89,9 @@ extern "C" int dcs_jit_unload(void* library) {
     return e == cudaSuccess ? DCS_OK : dcs_host::check_cuda(e, "cudaLibraryUnload");
 }
 
-extern "C" int dcs_jit_kernel(void* library, const char* name, size_t smem, void** kernel, int* blocks_per_sm) {
-    if (!library || !name || !kernel || !blocks_per_sm) {
+extern "C" int dcs_jit_kernel(void* library, const char* name, size_t smem, int threads, void** kernel,
+                              int* blocks_per_sm) {
+    if (!library || !name || !kernel || !blocks_per_sm || threads < 32 || threads > 1024 || threads % 32) {
         dcs_host::set_error("dcs_jit_kernel: invalid arguments");
         return DCS_E_ARG;
     }
@@ -100,20 +101,21 @@ extern "C" int dcs_jit_kernel(void* library, const char* name, size_t smem, void
     e = cudaFuncSetAttribute((const void*)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return dcs_host::check_cuda(e, "jit kernel smem attribute");
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)k, 256, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)k, threads, smem);
     if (e != cudaSuccess) return dcs_host::check_cuda(e, "jit kernel occupancy");
     *kernel = (void*)k;
     *blocks_per_sm = per_sm;
     return DCS_OK;
 }
 
-extern "C" int dcs_jit_launch(void* kernel, unsigned grid, size_t smem, void* table, const dcs_param* params,
-                              uint64_t* maxbits, dcs_scale* scale, void* stream) {
-    if (!kernel || !grid || !table || !params || !maxbits || !scale) {
+extern "C" int dcs_jit_launch(void* kernel, unsigned grid, int threads, size_t smem, void* table,
+                              const dcs_param* params, uint64_t* maxbits, dcs_scale* scale, void* stream) {
+    if (!kernel || !grid || !table || !params || !maxbits || !scale || threads < 32 || threads > 1024 || threads % 32) {
         dcs_host::set_error("dcs_jit_launch: invalid arguments");
         return DCS_E_ARG;
     }
     void* args[4] = {&table, (void*)&params, &maxbits, &scale};
-    const cudaError_t e = cudaLaunchKernel((const void*)kernel, dim3(grid), dim3(256), args, smem, (cudaStream_t)stream);
+    const cudaError_t e =
+        cudaLaunchKernel((const void*)kernel, dim3(grid), dim3(threads), args, smem, (cudaStream_t)stream);
     return e == cudaSuccess ? DCS_OK : dcs_host::check_cuda(e, "jit kernel launch");
 }

@@ -43,7 +43,10 @@ struct jit_scale {
 
 namespace jit {
 
-constexpr int kThreads = 256;
+#ifndef DCS_JIT_THREADS
+#define DCS_JIT_THREADS 256
+#endif
+constexpr int kThreads = DCS_JIT_THREADS;  // threads per CTA of every kernel of the unit
 constexpr uint32_t kSign = 0x80000000u;
 
 __host__ __device__ constexpr int cpar(int x) { return x ? ((x & 1) ^ cpar(x >> 1)) : 0; }

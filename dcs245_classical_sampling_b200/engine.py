@@ -241,6 +241,7 @@ class InplaceConditionalBlockGPU:
                                  "pairs": cfg.get("pairs", False)}
             self.jit = bool(cfg.get("jit", False) if jit is None else jit)
             self.jit_minb = cfg.get("minb")
+            self.jit_threads = cfg.get("threads") or 256
             self.fplan = self._build_fplan()
             self.items = 1
         if half:  # (re, im) binary16 pairs
@@ -283,19 +284,23 @@ class InplaceConditionalBlockGPU:
         fp = build_fused_plan(self.plan, **self.fused_config)
         if getattr(self, "jit", False) and fp.tile_runs is not None:
             from .jit import JitPlan
-            fp.jit = JitPlan(self.plan, fp, self.lib, minb=getattr(self, "jit_minb", None))
+            fp.jit = JitPlan(self.plan, fp, self.lib, minb=getattr(self, "jit_minb", None),
+                             threads=getattr(self, "jit_threads", 256))
         return fp
 
-    def set_fused_config(self, jit=None, minb=None, **cfg):
+    def set_fused_config(self, jit=None, minb=None, threads=None, **cfg):
         """Rebuild the fused plan with another tile shape (max_dim, low, max_steps, variant, pairs);
         jit=True/False switches the plan-specialised group kernels on or off; minb: CTAs per SM
-        their registers are sized for (default: 2 with variant bit 0, else 3)."""
+        their registers are sized for (default: 2 with variant bit 0, else 3); threads: per CTA of
+        those kernels (default 256)."""
         if self.mode != "fused":
             raise ValueError("set_fused_config needs mode='fused'")
         if jit is not None:
             self.jit = bool(jit)
         if minb is not None:
             self.jit_minb = int(minb)
+        if threads is not None:
+            self.jit_threads = int(threads)
         self.fused_config = {**self.fused_config, **cfg}
         self.fplan = self._build_fplan()
         self.maxbits = torch.zeros(self.items * (len(self.fplan.groups) + 1), dtype=torch.int64, device=self.device)
@@ -315,6 +320,7 @@ class InplaceConditionalBlockGPU:
         rep = at.tune(self, prm, jit=jit, **({"candidates": candidates} if candidates else {}))
         self.jit = jit
         self.jit_minb = rep["best"].get("minb")
+        self.jit_threads = rep["best"].get("threads") or 256
         self.fused_config = {k: rep["best"][k] for k in ("max_dim", "low", "max_steps", "variant", "pairs")}
         self.scale = torch.zeros(self.items * _lib.SCALE_DTYPE.itemsize // 8, dtype=torch.int64,
                                  device=self.device)

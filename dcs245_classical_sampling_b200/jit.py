@@ -90,7 +90,7 @@ def _fixmask(fp, first, count):
     return m
 
 
-def group_source(plan, fp, gi, minb=3):
+def group_source(plan, fp, gi, minb=3, threads=256):
     """CUDA source of the kernel of group gi (``dcs_g<gi>``); None if the group has no runs.
 
     Direct I/O (``fp.direct_io``, the default): the first run of a tile loads its cosets from
@@ -100,12 +100,18 @@ def group_source(plan, fp, gi, minb=3):
     the coset of t0 sits at base ^ addr(t0) ^ addr(off_j), the last term a constant of the plan.
     Without it, the tile is staged in shared memory on load and store (the library kernel's
     scheme).  With ``fp.coset_pairs`` a thread takes two cosets per loop iteration where it has
-    an even number of them."""
+    an even number of them.  `threads` per CTA: a power of two from 128 to 1024 (the packed form
+    takes 256 only)."""
+    if threads not in (128, 256, 512, 1024):
+        raise ValueError(f"threads {threads}")
+    lognt = threads.bit_length() - 1
     coset_pairs = bool(getattr(fp, "coset_pairs", False))
     g = fp.groups[gi]
     if not int(g["variant"]) & 4:
         return None
     if packable(fp, gi):
+        if threads != 256:
+            raise ValueError("the packed group kernels run 256 threads per CTA")
         return _packed_source(fp, gi, minb)
     direct = bool(getattr(fp, "direct_io", True)) and _direct_ok(fp, gi)
     R = 4 if int(g["variant"]) & 8 else 3
@@ -134,7 +140,7 @@ def group_source(plan, fp, gi, minb=3):
     L.append(f"__constant__ uint64_t g{gi}_basis[{nb}] = {{{', '.join(_u64(basis[i]) for i in range(nb))}}};")
     L.append(f"__constant__ uint64_t g{gi}_beta[{count}] = "
              f"{{{', '.join(_u64(fp.dsteps[first + s]['beta']) for s in range(count))}}};")
-    L.append(f'extern "C" __global__ void __launch_bounds__(256, {minb})')
+    L.append(f'extern "C" __global__ void __launch_bounds__({threads}, {minb})')
     L.append(f"dcs_g{gi}(float2* __restrict__ E, const jit_param* __restrict__ params, "
              "unsigned long long* __restrict__ maxbits, jit_scale* __restrict__ scale) {")
     L.append(f"    constexpr int TD = {TD}, LOW = {LOW}, T = 1 << TD, COUNT = {count}, FIRST = {first};")
@@ -175,8 +181,9 @@ def group_source(plan, fp, gi, minb=3):
         nins = int(tr["nins"])
         ins = [int(x) for x in tr["ins"][:nins]]
         NB = T >> nins
-        niter = NB >> 8 if NB > 256 else 1
-        mhi3 = int(tr["mhi"]) << 3
+        niter = NB >> lognt if NB > threads else 1
+        free = [b for b in range(TD) if b not in ins]  # thread index bits fill free[:lognt]
+        mhi3 = sum(1 << b for b in free[lognt:]) << 3
         offs = [int(tr["off"][j]) << 3 for j in range(1 << R)]
         G = [gaddr(int(tr["off"][j])) for j in range(1 << R)]
         L.append(f"        // run: steps {first + s}..{first + s + n - 1}, {NB} cosets of {1 << R} entries"
@@ -440,12 +447,12 @@ def _packed_source(fp, gi, minb):
     return "\n".join(L) + "\n"
 
 
-def plan_sources(plan, fp, minb=3, parts=8):
+def plan_sources(plan, fp, minb=3, parts=8, threads=256):
     """Translation units (source strings) holding the group kernels, spread over `parts` units
     so that NVRTC compiles them in parallel; returns [(source, [group indices])]."""
     groups = [gi for gi in range(len(fp.groups)) if int(fp.groups[gi]["variant"]) & 4]
     # balance by generated size
-    bodies = {gi: group_source(plan, fp, gi, minb) for gi in groups}
+    bodies = {gi: group_source(plan, fp, gi, minb, threads) for gi in groups}
     units = [([], 0) for _ in range(max(1, min(parts, len(groups))))]
     for gi in sorted(groups, key=lambda q: -len(bodies[q])):
         k = min(range(len(units)), key=lambda u: units[u][1])
@@ -454,7 +461,8 @@ def plan_sources(plan, fp, minb=3, parts=8):
     for gis, _ in units:
         if not gis:
             continue
-        src = '#include "runs_jit.cuh"\n\n' + "\n".join(bodies[gi] for gi in sorted(gis))
+        src = (f"#define DCS_JIT_THREADS {threads}\n" '#include "runs_jit.cuh"\n\n' +
+               "\n".join(bodies[gi] for gi in sorted(gis)))
         out.append((src, sorted(gis)))
     return out
 
@@ -485,10 +493,10 @@ def compile_source(lib, source, name="dcs_plan.cu"):
     return data
 
 
-def compile_plan(plan, fp, lib=None, minb=3, parts=8):
+def compile_plan(plan, fp, lib=None, minb=3, parts=8, threads=256):
     """[(cubin, [group indices])] for a fused plan (NVRTC in parallel threads)."""
     lib = lib or _lib.load()
-    units = plan_sources(plan, fp, minb, parts)
+    units = plan_sources(plan, fp, minb, parts, threads)
     with ThreadPoolExecutor(max_workers=len(units) or 1) as ex:
         images = list(ex.map(lambda u: compile_source(lib, u[0], f"dcs_plan_{u[1][0]}.cu"), units))
     return [(img, gis) for img, (_, gis) in zip(images, units)]
@@ -497,7 +505,7 @@ def compile_plan(plan, fp, lib=None, minb=3, parts=8):
 class JitPlan:
     """Loaded group kernels of one fused plan (current CUDA device)."""
 
-    def __init__(self, plan, fp, lib=None, minb=None, parts=8):
+    def __init__(self, plan, fp, lib=None, minb=None, parts=8, threads=256):
         """minb: CTAs per SM the registers are sized for (default: 2 if the plan's variant has
         bit 0, else 3)."""
         self.lib = lib or _lib.load()
@@ -508,8 +516,9 @@ class JitPlan:
         if minb is None:
             minb = 2 if len(fp.groups) and int(fp.groups[0]["variant"]) & 1 else 3
         self.minb = int(minb)
+        self.threads = int(threads)
         sms = self.lib.dcs_sm_count()
-        for img, gis in compile_plan(plan, fp, self.lib, minb, parts):
+        for img, gis in compile_plan(plan, fp, self.lib, minb, parts, self.threads):
             buf = ctypes.create_string_buffer(img, len(img))
             self._images.append(buf)
             handle = ctypes.c_void_p()
@@ -521,7 +530,7 @@ class JitPlan:
                 smem = 8 * (1 << (td - low)) + (8 * (1 << td) if uses_tile_buffer(fp, gi) else 0)
                 k = ctypes.c_void_p()
                 per_sm = ctypes.c_int()
-                _lib.check(self.lib.dcs_jit_kernel(handle, f"dcs_g{gi}".encode(), smem, ctypes.byref(k),
+                _lib.check(self.lib.dcs_jit_kernel(handle, f"dcs_g{gi}".encode(), smem, self.threads, ctypes.byref(k),
                                                    ctypes.byref(per_sm)))
                 grid = min(sms * max(1, per_sm.value), 1 << int(g["coset_m"]))
                 self.kernels[gi] = (k, grid, smem)
@@ -534,7 +543,7 @@ class JitPlan:
                 rc = self.fp.launch_library(self.lib, table, params, gi, 1, maxbits, scale, stream)
             else:
                 k, grid, smem = kern
-                rc = self.lib.dcs_jit_launch(k, grid, smem, table, params, maxbits, scale, stream)
+                rc = self.lib.dcs_jit_launch(k, grid, self.threads, smem, table, params, maxbits, scale, stream)
             if rc != 0:
                 return rc
         return 0

@@ -252,20 +252,22 @@ int dcs_fused_runs(void *table, const dcs_step *steps, int nsteps, const dcs_gro
  * dcs_jit_compile compiles CUDA source for sm_100a with NVRTC into a cubin image (release with
  * dcs_jit_free); `log` receives the compiler log.  dcs_jit_load loads an image through the
  * runtime library API.  dcs_jit_kernel looks up a kernel, allows it `smem` bytes of dynamic
- * shared memory and returns its resident blocks per SM.  dcs_jit_launch runs it with 256
- * threads per block on (table, params, maxbits, scale), as dcs_fused_runs runs one group. */
+ * shared memory and returns its resident blocks per SM at `threads` per block.  dcs_jit_launch
+ * runs it with `threads` per block (the count the source was generated for) on (table, params,
+ * maxbits, scale), as dcs_fused_runs runs one group. */
 int dcs_jit_compile(const char *source, const char *name, const char *header_source, const char *header_name,
                     int lineinfo, void **image, size_t *image_size, char *log, size_t log_capacity);
 void dcs_jit_free(void *image);
 int dcs_jit_load(const void *image, void **library);
 int dcs_jit_unload(void *library);
-int dcs_jit_kernel(void *library, const char *name, size_t smem, void **kernel, int *blocks_per_sm);
-int dcs_jit_launch(void *kernel, unsigned grid, size_t smem, void *table, const dcs_param *params, uint64_t *maxbits,
-                   dcs_scale *scale, void *stream);
+int dcs_jit_kernel(void *library, const char *name, size_t smem, int threads, void **kernel, int *blocks_per_sm);
+int dcs_jit_launch(void *kernel, unsigned grid, int threads, size_t smem, void *table, const dcs_param *params,
+                   uint64_t *maxbits, dcs_scale *scale, void *stream);
 
 /* Terminal gather + syndrome scatter + coherent slice accumulation into complex128 blocks.
  * For output block b, items item_begin[b] .. item_begin[b+1]-1 (slices, in slice order) add
  *   total_b[synd(i) ^ xors[it]] += env_it(i) * (coefs[2it] + i coefs[2it+1]) * exp(logscale_it - log_shift)
+ *                                  * exp(i phase_it)
  * with env_it(i) = table[it*table_stride + deposit(i, terminal_runs)], synd(i) = XOR of
  * tbasis[j] (host array, tr entries of k bits) over the bits j of i, i in [0, 2^tr).
  * Items whose scale flags report a zero or nonfinite table, or whose final maximum

@@ -101,6 +101,19 @@ def test_plan_specialised_kernels_match_reference(golden, name, variant, pairs):
         assert err <= max(2.0 * rel_l2(lb, want), 2e-6), (err, rel_l2(lb, want))
 
 
+@pytest.mark.parametrize("threads,minb", [(512, 2), (1024, 1), (128, 6)])
+def test_plan_specialised_kernels_other_block_sizes(golden, threads, minb):
+    """The generated kernels at other thread counts per CTA (the coset index takes as many thread
+    bits) give the reference blocks."""
+    case, arrays = golden("c2")
+    eng = _engine(case, arrays, np.complex64, mode="fused")
+    eng.set_fused_config(variant=4, pairs=False, max_dim=13, low=4, jit=True, threads=threads, minb=minb)
+    assert eng.fplan.jit.threads == threads
+    for rec in case["protocol"]["records"]:
+        v, _ = eng.block(_x(rec))
+        assert rel_l2(v.cpu().numpy(), arrays[f"block_{rec['sample_id']}"]) < 1e-5
+
+
 def test_plan_specialised_kernels_fall_back_without_unit_weights(golden):
     """A free step whose f0 is zero (a custom reference bra orthogonal to the first column of
     its unitary) cannot divide f0 out: that item runs the library kernels and the block still
