@@ -32,10 +32,10 @@ sys.path.insert(0, str(REPO))
 
 METRIC = "samples/s (64q, 2^20 block) served vs plain at c_y≥0.9999; p50/p99 ms"
 # DRAM traffic / algorithmic bytes of one launch of the dominant kernel, measured by ncu on a
-# group of the same plan whose tables are 2^27-2^28 entries (profiles/dcs_g_ring64_prefix_group23.md,
+# group of the same plan whose tables are 2^27-2^28 entries (profiles/dcs_g_ring64_prefix_group21_bytes_low3.md,
 # profiles/k_runs_ring64_prefix_group21.md, profiles/k_fused_ring64_prefix_group23.md): full-size launches cannot be captured with all
 # counters, and the traffic of a group scales with the entries it touches.
-TRAFFIC_RATIO = {"k_runs": 0.9823, "k_fused": 0.9635, "dcs_g (plan-specialised k_runs)": 0.9641}
+TRAFFIC_RATIO = {"k_runs": 0.9823, "k_fused": 0.9635, "dcs_g (plan-specialised k_runs)": 0.9780}
 FALLBACK_HBM = 6650.0
 
 

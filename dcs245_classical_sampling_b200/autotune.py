@@ -47,9 +47,21 @@ def cached(plan, device_name):
 # with plan-specialised group kernels (jit.py; scalar register runs, so no packed variants)
 # (pairs=True with register runs: two cosets per loop iteration in the generated kernels)
 # variant bit 1 with register runs: packed FP32x2 groups where tile bit 0 stays free
-JIT_CANDIDATES = [(13, 4, 24, 12, False), (13, 3, 24, 12, False), (13, 4, 24, 4, False), (13, 4, 24, 4, True),
-                  (13, 4, 24, 6, False), (13, 3, 24, 6, False), (13, 4, 24, 14, False), (13, 4, 24, 15, False),
-                  (13, 5, 24, 6, False), (13, 4, 16, 6, False)]
+JIT_CANDIDATES = [(13, 3, 24, 12, False, None, 256, "bytes"), (13, 4, 24, 12, False, None, 256, "bytes"),
+                  (13, 2, 24, 12, False, None, 256, "bytes"), (13, 3, 24, 4, False, None, 256, "bytes"),
+                  (13, 4, 24, 12, False), (13, 3, 24, 12, False), (13, 4, 24, 4, False), (13, 4, 24, 4, True),
+                  (13, 4, 24, 6, False), (13, 4, 24, 14, False), (13, 4, 24, 15, False)]
+
+
+KEYS = ("max_dim", "low", "max_steps", "variant", "pairs", "minb", "threads", "grouping", "group_cost", "max_extra")
+PLAN_KEYS = ("max_dim", "low", "max_steps", "variant", "pairs", "grouping", "group_cost", "max_extra")
+DEFAULTS = {"minb": None, "threads": 256, "grouping": "greedy", "group_cost": 1 << 30, "max_extra": 1}
+
+
+def candidate(c):
+    """A candidate as a dict of KEYS: a dict, or a tuple in KEYS order (missing tail = defaults)."""
+    d = dict(c) if isinstance(c, dict) else dict(zip(KEYS, c))
+    return {**DEFAULTS, **d}
 
 
 def tune(engine, params_dev, candidates=None, repeats=1, save=True, jit=False):
@@ -65,18 +77,15 @@ def tune(engine, params_dev, candidates=None, repeats=1, save=True, jit=False):
     stream = torch.cuda.current_stream(engine.device)
     report = []
     best = None
-    for cand in candidates:
-        max_dim, low, max_steps, variant, pairs = cand[:5]
-        minb = cand[5] if len(cand) > 5 else None  # CTAs per SM of the generated kernels
-        threads = cand[6] if len(cand) > 6 else 256  # threads per CTA of the generated kernels
+    for cand in map(candidate, candidates):
         try:
-            fp = build_fused_plan(engine.plan, max_dim=max_dim, low=low, max_steps=max_steps, variant=variant,
-                                  pairs=pairs)
+            fp = build_fused_plan(engine.plan, **{k: cand[k] for k in PLAN_KEYS})
         except ValueError:
             continue
         if jit and fp.tile_runs is not None:
             from .jit import JitPlan
-            fp.jit = JitPlan(engine.plan, fp, lib, minb=minb, threads=threads)
+            fp.jit = JitPlan(engine.plan, fp, lib, minb=cand["minb"], threads=cand["threads"])
+            cand = {**cand, "minb": fp.jit.minb}
         need = len(fp.groups) + 1
         if engine.maxbits.numel() < need:
             engine.maxbits = torch.zeros(need, dtype=torch.int64, device=engine.device)
@@ -96,11 +105,7 @@ def tune(engine, params_dev, candidates=None, repeats=1, save=True, jit=False):
             torch.cuda.synchronize(engine.device)
             times.append(a.elapsed_time(b) / 1000.0)
         t = min(times[1:]) if len(times) > 1 else times[0]
-        report.append({"max_dim": max_dim, "low": low, "max_steps": max_steps, "variant": variant,
-                       "pairs": pairs, "jit": fp.jit is not None,
-                       "minb": fp.jit.minb if fp.jit is not None else None,
-                       "threads": fp.jit.threads if fp.jit is not None else None, "groups": len(fp.groups),
-                       "seconds": t})
+        report.append({**cand, "jit": fp.jit is not None, "groups": len(fp.groups), "seconds": t})
         if best is None or t < best[0]:
             if best is not None and best[2].jit is not None:
                 best[2].jit.close()
@@ -110,19 +115,14 @@ def tune(engine, params_dev, candidates=None, repeats=1, save=True, jit=False):
     engine.fplan = best[2]
     nm = len(best[2].groups) + 1
     engine.maxbits = torch.zeros(engine.items * nm, dtype=torch.int64, device=engine.device)
+    chosen = {**{k: best[1][k] for k in PLAN_KEYS}, "jit": best[2].jit is not None,
+              "minb": best[1]["minb"] if best[2].jit is not None else None,
+              "threads": best[1]["threads"] if best[2].jit is not None else None, "seconds": best[0]}
     if save:
         data = _load()
-        data[f"{fingerprint(engine.plan)}|{torch.cuda.get_device_name(engine.device)}"] = {
-            "max_dim": best[1][0], "low": best[1][1], "max_steps": best[1][2], "variant": best[1][3],
-            "pairs": best[1][4], "jit": best[2].jit is not None,
-            "minb": best[2].jit.minb if best[2].jit is not None else None,
-            "threads": best[2].jit.threads if best[2].jit is not None else None, "seconds": best[0]}
+        data[f"{fingerprint(engine.plan)}|{torch.cuda.get_device_name(engine.device)}"] = chosen
         try:
             CACHE.write_text(json.dumps(data, indent=1) + "\n")
         except OSError:
             pass
-    return {"best": {"max_dim": best[1][0], "low": best[1][1], "max_steps": best[1][2], "variant": best[1][3],
-                     "pairs": best[1][4], "jit": best[2].jit is not None,
-                     "minb": best[2].jit.minb if best[2].jit is not None else None,
-                     "threads": best[2].jit.threads if best[2].jit is not None else None, "seconds": best[0]},
-            "candidates": report}
+    return {"best": chosen, "candidates": report}

@@ -238,7 +238,8 @@ class InplaceConditionalBlockGPU:
             cfg = cached(plan, torch.cuda.get_device_name(self.device)) or {}
             self.fused_config = {"max_dim": cfg.get("max_dim", 13), "low": cfg.get("low", 4),
                                  "max_steps": cfg.get("max_steps", 24), "variant": cfg.get("variant", 0),
-                                 "pairs": cfg.get("pairs", False)}
+                                 "pairs": cfg.get("pairs", False), "grouping": cfg.get("grouping", "greedy"),
+                                 "group_cost": cfg.get("group_cost", 1 << 30), "max_extra": cfg.get("max_extra", 1)}
             self.jit = bool(cfg.get("jit", False) if jit is None else jit)
             self.jit_minb = cfg.get("minb")
             self.jit_threads = cfg.get("threads") or 256
@@ -321,7 +322,7 @@ class InplaceConditionalBlockGPU:
         self.jit = jit
         self.jit_minb = rep["best"].get("minb")
         self.jit_threads = rep["best"].get("threads") or 256
-        self.fused_config = {k: rep["best"][k] for k in ("max_dim", "low", "max_steps", "variant", "pairs")}
+        self.fused_config = {k: rep["best"][k] for k in at.PLAN_KEYS}
         self.scale = torch.zeros(self.items * _lib.SCALE_DTYPE.itemsize // 8, dtype=torch.int64,
                                  device=self.device)
         return rep

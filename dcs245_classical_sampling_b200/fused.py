@@ -142,6 +142,55 @@ def group_steps(steps, max_dim=13, low=4, max_steps=MAX_GROUP_STEPS, max_extra=1
     return spans
 
 
+def _feasible_ends(steps, i, max_dim, low, max_steps, max_extra):
+    """Ends j of the groups [i, j) that group_steps' rules allow (span of the orbit vectors and
+    low bits <= max_dim, at most max_steps steps, slot universe <= rank + max_extra)."""
+    vecs, U, rank = [], 0, 0
+    ends = []
+    count = 0
+    S = len(steps)
+    while i + count < S and count < max_steps:
+        st = steps[i + count]
+        U2 = U | slot_mask(st.active_in) | slot_mask(st.active_out) | (
+            (1 << st.pivot) if orbit_kind(st)[0] == KIND_GROW else 0)
+        r2 = max(rank, len(st.active_in), len(st.active_out))
+        v2 = vecs + _orbit_vectors(st)
+        l2 = _low_bits(U2, low)
+        if count and (_dim(v2, l2) > max_dim or bin(U2).count("1") > r2 + max_extra):
+            break
+        vecs, U, rank = v2, U2, r2
+        count += 1
+        ends.append(i + count)
+    return ends
+
+
+def group_steps_min_bytes(steps, max_dim=13, low=4, max_steps=MAX_GROUP_STEPS, max_extra=1, per_group=1 << 30):
+    """Grouping with the fewest table bytes: the groups obey group_steps' rules, and a dynamic
+    program over the group boundaries minimises sum (2^|in_first| + 2^|out_last|) x 8 B plus
+    `per_group` bytes for each group (launch and per-tile costs).  Boundaries land where the
+    table is small instead of where the greedy span fills up."""
+    S = len(steps)
+    inf = float("inf")
+    best = [inf] * (S + 1)
+    prev = [0] * (S + 1)
+    best[0] = 0.0
+    for i in range(S):
+        if best[i] == inf:
+            continue
+        lo_in = 1 << len(steps[i].active_in)
+        for j in _feasible_ends(steps, i, max_dim, low, max_steps, max_extra):
+            c = best[i] + ((lo_in + (1 << len(steps[j - 1].active_out))) * 8 + per_group)
+            if c < best[j]:
+                best[j], prev[j] = c, i
+    spans = []
+    j = S
+    while j:
+        i = prev[j]
+        spans.append((i, j - i))
+        j = i
+    return spans[::-1]
+
+
 PAIR_KINDS = (0, 1, 2, 3, 4, 5, 7)  # every kind but the four-entry shrink
 
 
@@ -343,10 +392,17 @@ def _plan_runs(steps, first, count, tsteps, truns, dim, R, tbit, slot_of, keep_b
 
 
 def build_fused_plan(plan, max_dim=13, low=4, max_steps=MAX_GROUP_STEPS, max_extra=1, spans=None, variant=0,
-                     pairs=False):
+                     pairs=False, grouping="greedy", group_cost=1 << 30):
+    """grouping: "greedy" (group_steps) or "bytes" (group_steps_min_bytes, `group_cost` bytes
+    charged per group)."""
     steps = plan.steps
     if spans is None:
-        spans = group_steps(steps, max_dim, low, max_steps, max_extra)
+        if grouping == "bytes":
+            spans = group_steps_min_bytes(steps, max_dim, low, max_steps, max_extra, group_cost)
+        elif grouping == "greedy":
+            spans = group_steps(steps, max_dim, low, max_steps, max_extra)
+        else:
+            raise ValueError(f"grouping {grouping!r}")
     groups = np.zeros(len(spans), dtype=_lib.GROUP_DTYPE)
     tsteps = np.zeros(len(steps), dtype=_lib.TILE_STEP_DTYPE)
     truns = np.zeros(len(steps), dtype=_lib.TILE_RUN_DTYPE) if variant & 4 else None

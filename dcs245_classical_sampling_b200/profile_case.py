@@ -36,6 +36,8 @@ def main():
     ap.add_argument("--variant", type=int, default=0)
     ap.add_argument("--pairs", action="store_true", help="two steps per shared-memory round trip")
     ap.add_argument("--jit", action="store_true", help="plan-specialised group kernels (register-run variants)")
+    ap.add_argument("--grouping", default="greedy", choices=["greedy", "bytes"],
+                    help="fused groups: greedy spans or fewest table bytes")
     ap.add_argument("--storage", default=None, choices=["float16"],
                     help="binary16 tables with FP64 arithmetic (device mode)")
     a = ap.parse_args()
@@ -68,7 +70,8 @@ def main():
     stream = torch.cuda.current_stream(dev)
     sub = P.BlockPlan(**{**bp.__dict__, "steps": steps})
     if a.mode == "fused":
-        fp = build_fused_plan(sub, max_dim=a.max_dim, low=a.low, variant=a.variant, pairs=a.pairs)
+        fp = build_fused_plan(sub, max_dim=a.max_dim, low=a.low, variant=a.variant, pairs=a.pairs,
+                              grouping=a.grouping)
         if a.jit:
             from .jit import JitPlan
             fp.jit = JitPlan(sub, fp, lib)

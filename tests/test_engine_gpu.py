@@ -101,6 +101,18 @@ def test_plan_specialised_kernels_match_reference(golden, name, variant, pairs):
         assert err <= max(2.0 * rel_l2(lb, want), 2e-6), (err, rel_l2(lb, want))
 
 
+@pytest.mark.parametrize("name", ["small", "c2"])
+@pytest.mark.parametrize("low", [3, 4])
+def test_plan_specialised_kernels_min_bytes_groups(golden, name, low):
+    """The tuned shape: groups of fewest table bytes (grouping="bytes"), 3 or 4 low bits."""
+    case, arrays = golden(name)
+    eng = _engine(case, arrays, np.complex64, mode="fused")
+    eng.set_fused_config(variant=12, pairs=False, max_dim=13, low=low, grouping="bytes", jit=True)
+    for rec in case["protocol"]["records"]:
+        v, _ = eng.block(_x(rec))
+        assert rel_l2(v.cpu().numpy(), arrays[f"block_{rec['sample_id']}"]) < 1e-5
+
+
 @pytest.mark.parametrize("threads,minb", [(512, 2), (1024, 1), (128, 6)])
 def test_plan_specialised_kernels_other_block_sizes(golden, threads, minb):
     """The generated kernels at other thread counts per CTA (the coset index takes as many thread

@@ -486,3 +486,41 @@ def test_grouping_reduces_passes(golden):
     fused = fp.algorithmic_bytes(bp)
     assert len(fp.spans) < len(bp.steps) / 3
     assert fused < per_step / 3
+
+
+@pytest.mark.parametrize("name", ["c1", "small"])
+def test_min_bytes_grouping_emulation_matches_oracle(golden, name):
+    """Groups chosen by the dynamic program (fewest table bytes) obey the greedy rules and give
+    the oracle's environment through the register-run emulation."""
+    from dcs245_classical_sampling_b200.fused import _feasible_ends, group_steps_min_bytes
+    case, arrays = golden(name)
+    bp = P.build_block_plan(arrays["graph"], arrays["unitaries"], case["n"], case["order"],
+                            case["parity_operations"], case["open_vertices"])
+    spans = group_steps_min_bytes(bp.steps, 13, 3)
+    for first, count in spans:
+        assert first + count in _feasible_ends(bp.steps, first, 13, 3, 24, 1)
+    sp = SliceParams(bp)
+    oe = block_ref.OracleEngine(arrays["graph"], arrays["unitaries"], case["n"], case["order"],
+                                case["parity_operations"], case["open_vertices"])
+    x = np.array([int(c) for c in case["protocol"]["records"][0]["input_data_bits"]], np.uint8)
+    _, items = sp.items(x)
+    slices = [s for s in oe.slice_inputs(x) if s[0]]
+    for (coef, params, xor), (ocoef, f, yfix, flips) in zip(items, slices):
+        want, wls, _ = block_ref.execute(oe.steps, f, yfix, oe.fut, oe.maxslots)
+        fp = build_fused_plan(bp, max_dim=13, low=3, variant=12, grouping="bytes")
+        assert fp.spans == spans
+        got, gls = emulate(bp, fp, params)
+        if np.any(want):
+            assert rel_l2(got * math.exp(gls), want * math.exp(wls)) < 1e-12
+
+
+def test_min_bytes_grouping_moves_fewer_bytes(golden):
+    case, arrays = golden("c64plan")
+    bp = P.build_block_plan(arrays["graph"], arrays["unitaries"], case["n"], case["order"],
+                            case["parity_operations"], case["open_vertices"])
+    greedy = build_fused_plan(bp, max_dim=13, low=4)
+    dp = build_fused_plan(bp, max_dim=13, low=4, grouping="bytes", group_cost=0)
+    assert dp.algorithmic_bytes(bp) <= greedy.algorithmic_bytes(bp)
+    assert dp.algorithmic_bytes(bp) < 0.8 * greedy.algorithmic_bytes(bp)  # 150.5 vs 199.5 GiB
+    with pytest.raises(ValueError):
+        build_fused_plan(bp, grouping="other")
