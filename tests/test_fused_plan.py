@@ -447,9 +447,13 @@ def _emulate_packed(st, kind, ts, pr, bases, A, sh, dim):
     return out
 
 
-@pytest.mark.parametrize("name,dims", [("c1", [(13, 4), (6, 2), (4, 0)]), ("small", [(13, 4), (8, 3), (6, 2)]),
-                                       ("c2", [(13, 4)])])
-def test_fused_emulation_matches_oracle(golden, name, dims):
+ALL_MODES = ("plain", "pairs", "packed", "runs3", "runs4", "pruns3")
+
+
+@pytest.mark.parametrize("name,dims,modes", [("c1", [(13, 4), (6, 2), (4, 0)], ALL_MODES),
+                                             ("small", [(13, 4), (8, 3), (6, 2)], ALL_MODES),
+                                             ("c2", [(13, 4)], ("runs4",))])  # 2^22 tables: the tuned mode
+def test_fused_emulation_matches_oracle(golden, name, dims, modes):
     case, arrays = golden(name)
     bp = P.build_block_plan(arrays["graph"], arrays["unitaries"], case["n"], case["order"],
                             case["parity_operations"], case["open_vertices"])
@@ -464,8 +468,7 @@ def test_fused_emulation_matches_oracle(golden, name, dims):
         want, wls, off = block_ref.execute(oe.steps, f, yfix, oe.fut, oe.maxslots)
         freeflip = sum(int(flips[q]) << j for j, q in enumerate(oe.open_red))
         assert xor == (off >> oe.stop) ^ freeflip
-        for (max_dim, low), mode in [(d, m) for d in dims
-                                     for m in ("plain", "pairs", "packed", "runs3", "runs4", "pruns3")]:
+        for (max_dim, low), mode in [(d, m) for d in dims for m in modes]:
             variant = {"runs3": 4, "runs4": 12, "pruns3": 6}.get(mode, 0)
             fp = build_fused_plan(bp, max_dim=max_dim, low=low, pairs=mode == "pairs", variant=variant)
             assert sum(c for _, c in fp.spans) == len(bp.steps)
