@@ -23,7 +23,7 @@ from . import _lib
 HERE = Path(__file__).resolve().parent
 HEADER = HERE / "csrc" / "runs_jit.cuh"
 CACHE_DIR = HERE / "_jit_cache"
-KERNEL_VERSION = 6  # bump when the generated code changes meaning
+KERNEL_VERSION = 7  # bump when the generated code changes meaning
 
 ONE_VECTOR = (0, 1, 3, 5, 7)
 
@@ -152,22 +152,26 @@ def group_source(plan, fp, gi, minb=3, threads=256):
         L.append("    uint64_t* hi_tab = reinterpret_cast<uint64_t*>(smem);")
     L.append("    __shared__ float4 fw[COUNT];")
     L.append("    __shared__ int ovy[COUNT];")
-    L.append("    __shared__ uint32_t cs_sh;")
+    # Direct I/O: the sign bits alternate between two words, so the barrier after a tile's sign
+    # bits is the only one between tiles (the next tile's first shared-memory writes come after
+    # it, and warp 0 cannot pass it before every warp has read the previous word).
+    L.append("    __shared__ uint32_t cs_sh[2];")
     L.append(f"    const float sc = jit::prologue<TD, LOW, COUNT, FIRST, {_fixmask(fp, first, count)}u>(params, "
              f"g{gi}_basis, maxbits, {gi}, scale, fw, ovy, hi_tab);")
     L.append("    float lm = 0.f;")
+    L.append("    uint32_t par = 0;")
     L.append(f"    for (uint64_t tile = blockIdx.x; tile < {_u64(1 << int(g['coset_m']))}; tile += gridDim.x) {{")
     L.append(f"        const uint64_t base = {_deposit_expr(g)};")
     if direct:
-        L.append(f"        jit::sign_bits<COUNT>(g{gi}_beta, base, ovy, &cs_sh);")
+        L.append(f"        jit::sign_bits<COUNT>(g{gi}_beta, base, ovy, &cs_sh[par]);")
         L.append("        __syncthreads();")
     else:
         L.append(f"        jit::load_tile<T, LOW, {'true' if pair_in else 'false'}>(E, sh, hi_tab, base, "
                  f"{_u64(in_inact)});")
-        L.append(f"        jit::sign_bits<COUNT>(g{gi}_beta, base, ovy, &cs_sh);")
+        L.append(f"        jit::sign_bits<COUNT>(g{gi}_beta, base, ovy, &cs_sh[par]);")
         L.append('        asm volatile("cp.async.wait_all;\\n" ::: "memory");')
         L.append("        __syncthreads();")
-    L.append("        const uint32_t csm = cs_sh;")
+    L.append("        const uint32_t csm = cs_sh[par];")
     L.append("        unsigned char* shb = smem;")
     if direct:
         L.append(f"        if (!(base & {_u64(fp.tile_steps[first]['cskip'])})) {{")
@@ -276,10 +280,11 @@ def group_source(plan, fp, gi, minb=3, threads=256):
             L.append("        __syncthreads();")
     if direct:
         L.append("        }")
+        L.append("        par ^= 1u;")
     else:
         L.append(f"        lm = jit::store_tile<T, LOW, {'true' if pair_out else 'false'}>(E, sh, hi_tab, base, "
                  f"{_u64(out_inact)}, sc, lm);")
-    L.append("        __syncthreads();")
+        L.append("        __syncthreads();")
     L.append("    }")
     L.append(f"    jit::block_max(lm, maxbits, {gi + 1});")
     L.append("}")
@@ -348,15 +353,16 @@ def _packed_source(fp, gi, minb):
         L.append("    uint64_t* hi_tab = reinterpret_cast<uint64_t*>(smem);")
     L.append("    __shared__ float4 fw[COUNT];")
     L.append("    __shared__ int ovy[COUNT];")
-    L.append("    __shared__ uint32_t cs_sh;")
+    L.append("    __shared__ uint32_t cs_sh[2];")
     L.append(f"    const float sc = jit::prologue<TD, LOW, COUNT, FIRST, {_fixmask(fp, first, count)}u>(params, "
              f"g{gi}_basis, maxbits, {gi}, scale, fw, ovy, hi_tab);")
     L.append("    float lm = 0.f;")
+    L.append("    uint32_t par = 0;")
     L.append(f"    for (uint64_t tile = blockIdx.x; tile < {_u64(1 << int(g['coset_m']))}; tile += gridDim.x) {{")
     L.append(f"        const uint64_t base = {_deposit_expr(g)};")
-    L.append(f"        jit::sign_bits<COUNT>(g{gi}_beta, base, ovy, &cs_sh);")
+    L.append(f"        jit::sign_bits<COUNT>(g{gi}_beta, base, ovy, &cs_sh[par]);")
     L.append("        __syncthreads();")
-    L.append("        const uint32_t csm = cs_sh;")
+    L.append("        const uint32_t csm = cs_sh[par];")
     L.append("        unsigned char* shb = smem;")
     L.append(f"        if (!(base & {_u64(fp.tile_steps[first]['cskip'])})) {{")
     for ri, (s, n) in enumerate(runs):
@@ -440,7 +446,7 @@ def _packed_source(fp, gi, minb):
         if not dst_g:
             L.append("        __syncthreads();")
     L.append("        }")
-    L.append("        __syncthreads();")
+    L.append("        par ^= 1u;")
     L.append("    }")
     L.append(f"    jit::block_max(lm, maxbits, {gi + 1});")
     L.append("}")
