@@ -77,10 +77,19 @@ def dist_init():
 
 
 def peaks():
+    """HBM copy bandwidth (GB/s) from MEASURED_PEAKS.json (`hbm_gbs`, at the top level or under
+    a per-GPU entry), else the fallback figure."""
     p = REPO / "MEASURED_PEAKS.json"
     if p.exists():
-        d = json.loads(p.read_text())
-        return float(d["hbm_gbs"]), "measured"
+        try:
+            d = json.loads(p.read_text())
+            v = d.get("hbm_gbs") if isinstance(d, dict) else None
+            if v is None and isinstance(d, dict):
+                v = next((x["hbm_gbs"] for x in d.values() if isinstance(x, dict) and "hbm_gbs" in x), None)
+            if v is not None and float(v) > 0:
+                return float(v), "measured"
+        except (ValueError, TypeError, KeyError, StopIteration):
+            pass
     return FALLBACK_HBM, "fallback"
 
 
