@@ -23,7 +23,7 @@ from . import _lib
 HERE = Path(__file__).resolve().parent
 HEADER = HERE / "csrc" / "runs_jit.cuh"
 CACHE_DIR = HERE / "_jit_cache"
-KERNEL_VERSION = 7  # bump when the generated code changes meaning
+KERNEL_VERSION = 8  # bump when the generated code changes meaning
 
 ONE_VECTOR = (0, 1, 3, 5, 7)
 
@@ -188,6 +188,12 @@ def group_source(plan, fp, gi, minb=3, threads=256):
         niter = NB >> lognt if NB > threads else 1
         free = [b for b in range(TD) if b not in ins]  # thread index bits fill free[:lognt]
         mhi3 = sum(1 << b for b in free[lognt:]) << 3
+        free3 = sum(1 << b for b in free) << 3  # bits a representative's byte offset can have
+
+        def sh_off(c, o, free3=free3):
+            """Byte offset of a local entry: t0 ^ o, written t0 + o when o has no bit that t0 can
+            have (then the offset is an immediate of the shared-memory access)."""
+            return f"(t0{c} + {o}u)" if not (o & free3) else f"(t0{c} ^ {o}u)"
         offs = [int(tr["off"][j]) << 3 for j in range(1 << R)]
         G = [gaddr(int(tr["off"][j])) for j in range(1 << R)]
         L.append(f"        // run: steps {first + s}..{first + s + n - 1}, {NB} cosets of {1 << R} entries"
@@ -227,11 +233,12 @@ def group_source(plan, fp, gi, minb=3, threads=256):
                                  f"v{c}[{j}] = (a & {_u64(in_inact)}) ? make_float2(0.f, 0.f) : __ldcg(E + a); }}")
             elif pairs:
                 for j, j1 in pairs:
-                    L.append(f"                    {{ const float4 q = *reinterpret_cast<const float4*>(shb + (t0{c} ^ "
-                             f"{offs[j]}u)); v{c}[{j}] = make_float2(q.x, q.y); v{c}[{j1}] = make_float2(q.z, q.w); }}")
+                    L.append(f"                    {{ const float4 q = *reinterpret_cast<const float4*>(shb + "
+                             f"{sh_off(c, offs[j])}); v{c}[{j}] = make_float2(q.x, q.y); "
+                             f"v{c}[{j1}] = make_float2(q.z, q.w); }}")
             else:
                 for j, o in enumerate(offs):
-                    L.append(f"                    v{c}[{j}] = *reinterpret_cast<const float2*>(shb + (t0{c} ^ {o}u));")
+                    L.append(f"                    v{c}[{j}] = *reinterpret_cast<const float2*>(shb + {sh_off(c, o)});")
         for i in range(n):
             si = s + i
             st = fp.tile_steps[first + si]
@@ -267,11 +274,11 @@ def group_source(plan, fp, gi, minb=3, threads=256):
                                  f"v{c}[{j}].y * sc); lm = fmaxf(lm, q.x * q.x + q.y * q.y); E[a] = q; }} }}")
             elif pairs:
                 for j, j1 in pairs:
-                    L.append(f"                    *reinterpret_cast<float4*>(shb + (t0{c} ^ {offs[j]}u)) = "
+                    L.append(f"                    *reinterpret_cast<float4*>(shb + {sh_off(c, offs[j])}) = "
                              f"make_float4(v{c}[{j}].x, v{c}[{j}].y, v{c}[{j1}].x, v{c}[{j1}].y);")
             else:
                 for j, o in enumerate(offs):
-                    L.append(f"                    *reinterpret_cast<float2*>(shb + (t0{c} ^ {o}u)) = v{c}[{j}];")
+                    L.append(f"                    *reinterpret_cast<float2*>(shb + {sh_off(c, o)}) = v{c}[{j}];")
         L.append("                }")
         L.append("            }")
         if not direct:
