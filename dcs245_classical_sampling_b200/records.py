@@ -5,7 +5,7 @@ one per audit, plus the sampled and reference vectors of every audited sample as
 Its independent CPU verifier (source/production/verify.py:351-618) replays those rows: the
 PCG64 states, the draw record and its CDF intervals, the output bit mapping, the probability
 identities, and for audits the 53-bit CDF-law vector and both overlap witnesses.  The builders
-here make the same rows from this build's engine, sampler and audit, so the reference's
+here make the same rows from this package's engine, sampler and audit, so the reference's
 verifier stays usable on B200 runs.
 
 Not built: the bundle manifest and its validation, hardware.json, the pilot anchor,
