@@ -506,10 +506,13 @@ class InplaceConditionalBlockGPU:
     def blocks(self, x_list, w=None):
         """Blocks of many prefixes; (prefix, slice) work items share launches.
 
-        Returns a complex128 tensor (len(x_list), 2^k) on the device."""
+        Returns a complex128 tensor (len(x_list), 2^k) on the device (no launch for none)."""
         if not self._alloc:
             self.alloc()
-        out, _ = self._run(list(x_list), w)
+        x_list = list(x_list)
+        if not x_list:
+            return torch.zeros((0, 1 << self.k), dtype=torch.complex128, device=self.device)
+        out, _ = self._run(x_list, w)
         return out
 
 

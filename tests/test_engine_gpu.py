@@ -311,6 +311,19 @@ def test_half_engine_class_matches_reference_surface(golden):
         eng.alloc(np.complex128)
 
 
+def test_empty_batch_and_repeated_prefixes(golden):
+    """No prefixes give an empty (0, 2^k) batch without launching; a batch that repeats a prefix
+    gives the same block twice (work items of equal inputs do not interfere)."""
+    case, arrays = golden("small")
+    eng = _engine(case, arrays, np.complex64, mode="device")
+    empty = eng.blocks([])
+    assert empty.shape == (0, 1 << len(case["open_vertices"])) and empty.dtype == torch.complex128
+    x = _x(case["protocol"]["records"][0])
+    two = eng.blocks([x, x]).cpu().numpy()
+    one = eng.block(x)[0].cpu().numpy()
+    assert np.array_equal(two[0], two[1]) and np.array_equal(two[0], one)
+
+
 def test_nonfinite_table_raises(golden):
     """An infinite maximum raises ArithmeticError (inplace_gpu.py:121).  NaN entries are
     dropped by fmax exactly as in the reference kernel, so an all-NaN table reads as zero:
