@@ -124,3 +124,31 @@ def test_row_errors(fixture, tmp_path):
     with pytest.raises(FileExistsError):  # rows and vectors are written once, never replaced
         records.save_vector(tmp_path / "v.npy", approx)
     assert meta["shape"] == [len(approx)] and meta["dtype"] == "complex128"
+
+
+def test_law_vector_grid_counts_by_exact_rationals():
+    """The 53-bit law of records.actual_cdf_law_vector against grid counts computed with exact
+    rationals from the sequential float64 CDF (the check of test_protocol_cpu.py:22-36), on
+    the reference's two vectors and on random ones."""
+    from fractions import Fraction
+    rng = np.random.default_rng(7)
+    vecs = [np.array([0, 1, 1j, 1 + 1j, 0, 2, 1 - 1j, 0], complex),
+            np.array([1e-15, 1e-8j, 1, 1j, 2 + 3j, .17, .21j, .01], complex)]
+    vecs += [rng.normal(size=64) + 1j * rng.normal(size=64) for _ in range(3)]
+    for a in vecs:
+        law, meta = records.actual_cdf_law_vector(a)
+        weights = a.real * a.real + a.imag * a.imag
+        cum, acc = [], 0.0
+        for w in weights:
+            acc = float(acc + float(w))
+            cum.append(acc)
+        cum = [float(c / acc) for c in cum]
+        cum[-1] = 1.0
+        ends = [math.ceil(Fraction.from_float(c) * (1 << 53)) for c in cum]
+        counts = [b - a_ for a_, b in zip([0] + ends[:-1], ends)]
+        assert sum(counts) == 1 << 53
+        target = np.asarray(counts, dtype=float) / 2 ** 53
+        assert np.max(np.abs(np.abs(law) ** 2 - target)) < 4e-16
+        assert meta["grid_total"] == 1 << 53 and abs(meta["law_norm_squared"] - 1) < 1e-12
+        d = sampler_ref.draw(a, .381245)
+        assert target[d["A_index"]] > 0
