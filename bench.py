@@ -16,7 +16,6 @@ from __future__ import annotations
 
 import argparse
 import json
-import math
 import os
 import statistics
 import subprocess
@@ -227,7 +226,7 @@ def gpu_arm(args):
     from dcs245_classical_sampling_b200 import _lib
     from dcs245_classical_sampling_b200 import plan as P
     from dcs245_classical_sampling_b200.engine import InplaceConditionalBlockGPU
-    from dcs245_classical_sampling_b200.sampling import draw_many, make_protocol
+    from dcs245_classical_sampling_b200.sampling import make_protocol
     from dcs245_classical_sampling_b200.workloads import build_workload
 
     w = build_workload(args.workload)

@@ -11,8 +11,6 @@ import hashlib
 import json
 from pathlib import Path
 
-import numpy as np
-
 from . import _lib
 
 CACHE = Path(__file__).resolve().parent / "autotune_cache.json"

@@ -234,7 +234,6 @@ class InplaceConditionalBlockGPU:
         self.items = int(items)
         if mode == "fused":
             from .autotune import cached
-            from .fused import build_fused_plan
             cfg = cached(plan, torch.cuda.get_device_name(self.device)) or {}
             self.fused_config = {"max_dim": cfg.get("max_dim", 13), "low": cfg.get("low", 4),
                                  "max_steps": cfg.get("max_steps", 24), "variant": cfg.get("variant", 0),
