@@ -7,7 +7,9 @@ injected graph), 2 parity slices (4 slices, rmax 34: one 128 GiB complex64 table
 prefixes/uniforms from make_protocol.  Inputs and tables are far larger than L2.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--workload NAME]
-                    [--mode fused|device|plain] [--no-plain] [--no-cpu]
+                    [--mode fused|device|plain] [--no-plain] [--no-cpu] [--no-audit] [--no-configs]
+    python bench.py --serve [--graphs] ...        the serving mix alone
+    python bench.py --profile-case ...            the small profiling case of profiles/
 
 Multi-GPU (torchrun, one rank per GPU): independent replicas, each rank samples its own
 prefixes (weak scaling); the elapsed time is the max over ranks.
@@ -52,7 +54,12 @@ def parse():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-audit", action="store_true")
-    ap.add_argument("--audits", type=int, default=2, help="timed samples audited in complex128")
+    ap.add_argument("--audits", type=int, default=64,
+                    help="generation samples audited in complex128 (ids from an independent PCG64 stream)")
+    ap.add_argument("--audit-seed", type=int, default=24521)
+    ap.add_argument("--audit-mode", default="fused", choices=["fused", "device"],
+                    help="complex128 executor of the audits (fused: plan-specialised kernels in FP64)")
+    ap.add_argument("--no-configs", action="store_true", help="skip the small workloads (16q, 40q) sub-report")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--seed", type=int, default=24520)
     ap.add_argument("--tune", action="store_true", help="autotune the fused tile shape before timing")
@@ -145,7 +152,8 @@ def cpu_baseline(workload, seconds, rank0=True):
     The 2^34-entry complex128 table of the 64-qubit plan does not fit host memory, so the
     sample is the longest prefix of the first slice's steps whose table stays <= 2^24 entries
     (256 MiB); the measured algorithmic bytes/s is converted to samples/s with the full
-    per-sample algorithmic bytes (complex128, all slices)."""
+    per-sample algorithmic bytes (complex128, all slices): an extrapolation, not a measured
+    64-qubit sample."""
     from dcs245_classical_sampling_b200 import plan as P
     from dcs245_classical_sampling_b200.engine import SliceParams
     from dcs245_classical_sampling_b200.sampling import make_protocol
@@ -183,35 +191,87 @@ def cpu_baseline(workload, seconds, rank0=True):
     dt = time.perf_counter() - t0
     bps = alg_sample * reps / dt
     return {"value": bps / per_sample, "unit": "samples/s", "cores": int(lib.oracle_threads()), "kind": "port",
-            "sample": (f"C/OpenMP complex128 executor over the first {last} of {len(bp.steps)} steps of one slice "
-                       f"(tables <= 2^{cap}), {reps} reps in {dt:.1f} s = {bps / 1e9:.2f} GB/s algorithmic; "
-                       f"samples/s = that rate / {per_sample / 2**40:.2f} TiB per sample (all {len(items)} slices)"),
-            "seconds": dt, "algorithmic_gbs": bps / 1e9}
+            "sample": (f"extrapolated: C/OpenMP complex128 executor over the first {last} of {len(bp.steps)} steps "
+                       f"of one slice (tables <= 2^{cap}), {reps} reps in {dt:.1f} s = {bps / 1e9:.2f} GB/s "
+                       f"algorithmic; samples/s = that rate / {per_sample / 2**40:.2f} TiB per sample (all "
+                       f"{len(items)} slices); a complete 64-qubit sample needs a 256 GiB complex128 table"),
+            "seconds": dt, "algorithmic_gbs": bps / 1e9, "steps_sampled": last, "steps_total": len(bp.steps)}
+
+
+# The small workloads, measured completely on the CPU and the GPU (no extrapolation): the
+# 16-qubit case (all 256 samples, as its configuration asks) and the 40-qubit case (a fixed
+# subset of its 1,000 samples on the CPU, all of them on the GPU).
+SMALL_CONFIGS = {"ring16_d20_t24_k8": {"samples": 256, "cpu_samples": 256, "mode": "device"},
+                 "ring40_d45_t190_k16": {"samples": 1000, "cpu_samples": 8, "mode": "fused"}}
+
+
+def cpu_small_configs(seed):
+    """Complete CPU samples (block + draw) of the small workloads: the oracle engine with the
+    C/OpenMP executor (oracle.c.CpuSampler), timed sample by sample."""
+    from dcs245_classical_sampling_b200.sampling import make_protocol
+    from dcs245_classical_sampling_b200.workloads import build_workload
+    from oracle import block_ref
+    from oracle import c as oc
+    lib = oc.load()
+    out = {}
+    for name, cfg in SMALL_CONFIGS.items():
+        w = build_workload(name)
+        eng = block_ref.OracleEngine(w["graph"], w["unitaries"], w["n"], w["order"], w["parity_operations"],
+                                     w["open_vertices"])
+        cs = oc.CpuSampler(eng, lib)
+        recs = make_protocol(seed, cfg["cpu_samples"], w["n"], w["open_vertices"])["records"]
+        t0 = time.perf_counter()
+        idx = []
+        for r in recs:
+            x = np.array([int(c) for c in r["input_data_bits"]], np.uint8)
+            idx.append(cs.sample(x, r["draw_uniform"])["A_index"])
+        dt = time.perf_counter() - t0
+        out[name] = {"value": len(recs) / dt, "unit": "samples/s", "samples": len(recs), "seconds": dt,
+                     "cores": int(lib.oracle_threads()), "kind": "port",
+                     "what": "complete samples: oracle engine + C/OpenMP complex128 executor + NumPy draw",
+                     "indices_head": idx[:8]}
+    return out
 
 
 def reference_arm(args):
+    """The reference's CPU path for this workload, timed on the host cores.  The reference is
+    Python and cannot run on a GPU machine, so its restatement in C (the oracle's executor) runs
+    instead.  Each step is one bounded sample of the 64-qubit plan (cpu_baseline), whose measured
+    duration is ms_per_step; value is the samples/s that rate extrapolates to."""
     rank, world, _ = dist_init()
     if rank != 0:
         return
-    samples = []
+    samples, secs = [], []
     cb = None
+    per_step = max(1.0, args.cpu_seconds / 8)
     for i in range(args.warmup + args.steps):
-        cb = cpu_baseline(args.workload, max(2.0, args.cpu_seconds / 3))
+        t0 = time.perf_counter()
+        cb = cpu_baseline(args.workload, per_step)
         if i >= args.warmup:
             samples.append(cb["value"])
+            secs.append(time.perf_counter() - t0)
     value = float(np.mean(samples))
+    configs = None if args.no_configs else cpu_small_configs(args.seed)
     line = {"metric": METRIC, "value": value, "unit": "samples/s", "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1000.0 / value, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "c128", "data": "synthetic (seeded ring circuit, PCG64 prefixes)",
-            "config": {"workload": args.workload, "block": "2^20", "precision": "complex128 CPU executor"},
+            "warmup": args.warmup, "ms_per_step": 1000.0 * float(np.mean(secs)), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+            "data": "synthetic (seeded ring circuit, PCG64 prefixes)",
+            "config": {"workload": args.workload, "block": "2^20", "precision": "complex128 CPU executor",
+                       "kind": (f"extrapolated from {cb['steps_sampled']} of {cb['steps_total']} steps of one "
+                                "slice: one step of this line is one bounded sample, not one 64-qubit sample"),
+                       "step_seconds": per_step},
             "impl": "reference",
             "cpu_baseline": {"value": value, "unit": "samples/s", "cores": cb["cores"], "kind": "port",
                              "sample": cb["sample"]},
-            "e2e": {"value": value, "unit": "samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": value, "unit": "samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "configs": configs}
     print(json.dumps(line), flush=True)
 
 
 # ---------------------------------------------------------------------------------------------
+GEN_COUNT = 2048  # samples of the 64-qubit generation protocol (the batched configuration's output)
+
+
 def gpu_arm(args):
     import torch
     rank, world, local = dist_init()
@@ -224,9 +284,9 @@ def gpu_arm(args):
     dev = torch.device("cuda", local)
 
     from dcs245_classical_sampling_b200 import _lib
-    from dcs245_classical_sampling_b200 import plan as P
     from dcs245_classical_sampling_b200.engine import InplaceConditionalBlockGPU
-    from dcs245_classical_sampling_b200.sampling import make_protocol
+    from dcs245_classical_sampling_b200.sampling import (STRADDLE_MARGIN, draw_many, make_audit_ids, make_protocol,
+                                                         sample_checked)
     from dcs245_classical_sampling_b200.workloads import build_workload
 
     w = build_workload(args.workload)
@@ -242,10 +302,15 @@ def gpu_arm(args):
     setup_s = time.perf_counter() - t0
     k = eng.k
     total = args.warmup + args.steps
-    proto = make_protocol(args.seed + 1000 * rank, total + args.plain_samples + 2, w["n"], w["open_vertices"])
+    count = max(GEN_COUNT, total + args.plain_samples + 2)
+    # generation protocol (PCG64 prefixes and uniforms) and, from a separate PCG64 stream chosen
+    # before any sample is drawn, the audited sample ids (production/protocol_common.py:22-31)
+    proto = make_protocol(args.seed + 1000 * rank, count, w["n"], w["open_vertices"])
     recs = proto["records"]
     xs = [np.array([int(c) for c in r["input_data_bits"]], np.uint8) for r in recs]
     us = [r["draw_uniform"] for r in recs]
+    audit_ids = (make_audit_ids(args.audit_seed + 1000 * rank, count, 1, args.audits)[0]
+                 if args.audits > 0 and not args.no_audit else [])
     stream = torch.cuda.current_stream(dev)
 
     # ---- device-resident throughput (value): inputs prepared and uploaded before timing
@@ -256,8 +321,6 @@ def gpu_arm(args):
     lib = _lib.load()
     scratch = torch.empty(lib.dcs_draw_scratch_bytes(k, 1), dtype=torch.uint8, device=dev)
     torch.cuda.synchronize(dev)
-
-    group_events = []
 
     def one(i, record=False):
         ev0 = torch.cuda.Event(enable_timing=True) if record else None
@@ -303,35 +366,43 @@ def gpu_arm(args):
     # ---- dominant kernel: time the contraction passes of one extra sample on their own
     dom = kernel_roofline(eng, preps[args.warmup], outs[args.warmup:args.warmup + 1], stream)
 
-    # ---- end to end through the public API (host prefixes in, host record out)
-    from dcs245_classical_sampling_b200.sampling import draw_checked
-    e2e_x = xs[:total]
-    for i in range(min(2, args.warmup)):
-        v, _ = eng.block(e2e_x[i])
-        draw_checked(v, us[i], hashes=False)
+    # ---- end to end through the public API: host prefixes in; per sample the block, its host
+    # copy, the checked draw with NumPy's exact CDF values and the SHA-256 of the weights and
+    # amplitudes out (the reference worker's per-sample record, production/worker.py:105-113)
+    sample_checked(eng, xs[:2], us[:2], hashes=True, exact_cdf=True)
     torch.cuda.synchronize(dev)
     ea = torch.cuda.Event(enable_timing=True)
     eb = torch.cuda.Event(enable_timing=True)
     ea.record(stream)
-    h2d = 0
-    for i in range(args.warmup, total):
-        v, _ = eng.block(e2e_x[i])
-        d = draw_checked(v, us[i], hashes=False)
+    e2e_recs = sample_checked(eng, xs[args.warmup:total], us[args.warmup:total], hashes=True, exact_cdf=True)
     eb.record(stream)
     torch.cuda.synchronize(dev)
     e2e_elapsed = ea.elapsed_time(eb) / 1000.0
     h2d = preps[args.warmup]["h2d_bytes"] + 8  # params/coefs/xors/begin blob + the uniform
-    d2h = _lib.DRAW_DTYPE.itemsize + 8  # draw record + the scale-flag word
+    d2h = (1 << k) * 16 + _lib.DRAW_DTYPE.itemsize + 8 * eng.items  # block + draw record + scale flags
+    e2e_same = all(int(r["A_index"]) == int(d["index"]) for r, d in zip(e2e_recs, draws[args.warmup:total]))
     if world > 1:
         t = torch.tensor([e2e_elapsed], device=dev)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         e2e_elapsed = float(t.item())
 
+    # ---- precision audit, part 1: the audited samples' complex64 blocks with the timed executor
+    audit_c64 = None
+    if audit_ids and rank == 0:
+        ta = time.perf_counter()
+        xa = [xs[i] for i in audit_ids]
+        ua = [us[i] for i in audit_ids]
+        blocks_a = torch.empty((len(xa), 1 << k), dtype=torch.complex128, device=dev)
+        for j, x in enumerate(xa):
+            blocks_a[j] = eng.blocks([x])[0]
+        draws_a = draw_many(blocks_a, ua)
+        torch.cuda.synchronize(dev)
+        audit_c64 = {"ids": audit_ids, "x": xa, "u": ua, "blocks": blocks_a, "draws": draws_a,
+                     "seconds": time.perf_counter() - ta}
+
     fused_cfg = getattr(eng, "fused_config", None)
     if fused_cfg is not None:
         fused_cfg = {**fused_cfg, "jit": bool(getattr(eng.fplan, "jit", None))}
-    eng_items = eng.items
-    blocks64 = outs[args.warmup:total].clone()
     del eng, preps, outs  # release the 128 GiB table before the other engines allocate theirs
     import gc
     gc.collect()
@@ -339,6 +410,7 @@ def gpu_arm(args):
     # ---- plain per-sample path (one launch + one host max read per step), same workload
     plain = None
     if not args.no_plain and args.plain_samples > 0 and rank == 0:
+        from dcs245_classical_sampling_b200.sampling import draw_checked
         peng = InplaceConditionalBlockGPU(w["graph"], w["unitaries"], w["n"], w["order"], w["parity_operations"],
                                           w["open_vertices"])
         peng.alloc(np.complex64, device=local, mode="plain")
@@ -356,12 +428,18 @@ def gpu_arm(args):
         plain = {"value": 1.0 / plain_s, "unit": "samples/s", "samples": args.plain_samples,
                  "path": "one launch + one host max read per vertex step (reference control flow)"}
         del peng
+        gc.collect()
         torch.cuda.empty_cache()
 
-    # ---- precision audit: independent complex128 recontraction (3-slice plan) of timed samples
+    # ---- precision audit, part 2: independent complex128 recontractions of the audited samples
     audit = None
-    if not args.no_audit and rank == 0:
-        audit = run_audit(args, xs, blocks64, local)
+    if audit_c64 is not None:
+        audit = run_audit(args, audit_c64, local)
+        del audit_c64
+
+    configs = None
+    if rank == 0 and world == 1 and not args.no_configs:
+        configs = gpu_small_configs(args, local)
 
     if rank == 0:
         peak, how = peaks()
@@ -369,7 +447,14 @@ def gpu_arm(args):
         if not args.no_cpu and world == 1:
             cb = cpu_baseline(args.workload, args.cpu_seconds)
             cb = {k2: cb[k2] for k2 in ("value", "unit", "cores", "kind", "sample")}
+            if configs is not None:
+                for name, c in cpu_small_configs(args.seed).items():
+                    configs[name]["cpu"] = c
+                    configs[name]["gpu_over_cpu"] = configs[name]["value"] / c["value"]
+                    configs[name]["e2e_over_cpu"] = configs[name]["e2e"]["value"] / c["value"]
         ach = dom["alg_bytes_per_launch"] / dom["avg_launch_s"] / 1e9
+        near = [bool(min(d["uniform"] - d["cdf_lower_exact"], d["cdf_upper_exact"] - d["uniform"]) < STRADDLE_MARGIN)
+                for d in draws[args.warmup:total]]
         line = {"metric": METRIC, "value": value, "unit": "samples/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": 1000.0 * elapsed / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f16 storage, f64 arithmetic" if args.storage else "c64",
@@ -382,7 +467,10 @@ def gpu_arm(args):
                            "parallelism": f"replicas x{world}"},
                 "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
                 "e2e": {"value": args.steps * world / e2e_elapsed, "unit": "samples/s", "h2d_bytes_per_step": h2d,
-                        "d2h_bytes_per_step": d2h},
+                        "d2h_bytes_per_step": d2h,
+                        "api": "sampling.sample_checked: engine blocks, host copy, checked draw with NumPy's exact "
+                               "CDF values and both SHA-256 hashes per sample",
+                        "same_indices_as_value": e2e_same},
                 "gpu_launches": launches,
                 "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
                              "traffic": (TRAFFIC_RATIO[dom["kernel"]] * dom["alg_bytes_per_launch"]
@@ -393,11 +481,18 @@ def gpu_arm(args):
                              "peak_source": f"{how} (MEASURED_PEAKS.json hbm_gbs)" if how == "measured" else
                              "fallback 6650 GB/s", "launches": dom["launches"],
                              "alg_bytes_per_launch": dom["alg_bytes_per_launch"],
-                             "avg_launch_ms": dom["avg_launch_s"] * 1e3, "launch_ms": dom["launch_ms"]},
+                             "avg_launch_ms": dom["avg_launch_s"] * 1e3,
+                             "per_launch": [[b, round(t, 4), round(b / t / 1e6 / peak, 4)]
+                                            for b, t in zip(dom["launch_bytes"], dom["launch_ms"])],
+                             "per_launch_fields": ["algorithmic bytes", "ms (CUDA events)", "fraction of peak"]},
                 "plain": plain, "speedup_vs_plain": (value / plain["value"]) if plain else None,
                 "draws": {"indices": [int(d["index"]) for d in draws[args.warmup:total]],
-                          "ties": int(sum(int(d["tie"]) for d in draws[args.warmup:total]))},
+                          "ties": int(sum(int(d["tie"]) for d in draws[args.warmup:total])),
+                          "near_cdf_edge": int(sum(near)),
+                          "near_cdf_edge_margin": STRADDLE_MARGIN,
+                          "straddles_audited": audit["straddles"] if audit else None},
                 "clocks": clk, "setup_s": setup_s, "cpu_baseline": cb, "audit": audit,
+                "configs": configs,
                 "fused_config": fused_cfg,
                 "autotune": tune_report}
         print(json.dumps(line), flush=True)
@@ -406,38 +501,131 @@ def gpu_arm(args):
         torch.distributed.destroy_process_group()
 
 
-def run_audit(args, xs, blocks64, local):
-    """c_y of the timed complex64 blocks against an independent complex128 recontraction with a
-    different slicing (one more parity slice: rmax 33, 128 GiB complex128), as the reference's
-    audits use inplace_k3_fp64 next to inplace_k2_fp32."""
+def run_audit(args, a64, local):
+    """Config 4: the audited samples' complex64 blocks (contracted by the timed executor) against
+    independent complex128 recontractions with a different slicing (one more parity slice: rmax
+    33, a 128 GiB complex128 table), as the reference's audits use inplace_k3_fp64 next to
+    inplace_k2_fp32 (production/worker.py:137-170).  Per sample: c_y (the normalised overlap,
+    review/full_vector_audit_certificate.py:36), relative L2 error, and the indices both blocks
+    select with the sample's uniform; a differing index is a straddle of a CDF edge and must lie
+    within the complex64 margin of it."""
     import gc
     import torch
     from dcs245_classical_sampling_b200.audit import audit_vector_pair, relative_l2
     from dcs245_classical_sampling_b200.engine import InplaceConditionalBlockGPU
-    from dcs245_classical_sampling_b200.workloads import build_workload
+    from dcs245_classical_sampling_b200.sampling import STRADDLE_MARGIN, draw_many
+    from dcs245_classical_sampling_b200.workloads import WORKLOADS, build_workload
     gc.collect()
     torch.cuda.empty_cache()
-    wa = build_workload(args.workload + "_audit") if args.workload + "_audit" in __import__(
-        "dcs245_classical_sampling_b200.workloads", fromlist=["WORKLOADS"]).WORKLOADS else build_workload(args.workload)
+    name = args.workload + "_audit" if args.workload + "_audit" in WORKLOADS else args.workload
+    wa = build_workload(name)
+    t0 = time.perf_counter()
     ref = InplaceConditionalBlockGPU(wa["graph"], wa["unitaries"], wa["n"], wa["order"], wa["parity_operations"],
                                      wa["open_vertices"])
-    ref.alloc(np.complex128, device=local, mode="device")
-    rows = []
-    n = min(args.audits, blocks64.shape[0])
-    for i in range(n):
-        x = xs[args.warmup + i]
-        t0 = time.perf_counter()
-        v, meta = ref.block(x)
-        sec = time.perf_counter() - t0
-        rec = audit_vector_pair(v, blocks64[i], args.warmup + i)
-        rows.append({"sample": args.warmup + i, "c_y": rec["normalized_conditional_overlap_abs"],
-                     "rel_l2": relative_l2(v, blocks64[i]), "ref_seconds": sec})
+    ref.alloc(np.complex128, device=local, mode=args.audit_mode)
+    setup = time.perf_counter() - t0
+    rows, secs = [], []
+    straddles, bad = 0, 0
+    for j, sid in enumerate(a64["ids"]):
+        ts = time.perf_counter()
+        v, meta = ref.block(a64["x"][j])
+        secs.append(time.perf_counter() - ts)
+        ap = a64["blocks"][j]
+        rec = audit_vector_pair(v, ap, sid)
+        i128 = int(draw_many(v.unsqueeze(0), [a64["u"][j]])[0]["index"])
+        d64 = a64["draws"][j]
+        i64 = int(d64["index"])
+        if i64 != i128:
+            straddles += 1
+            near = min(d64["uniform"] - d64["cdf_lower_exact"], d64["cdf_upper_exact"] - d64["uniform"])
+            bad += int(not near < STRADDLE_MARGIN)
+        rows.append([int(sid), rec["normalized_conditional_overlap_abs"], relative_l2(v, ap), i64, i128])
+    rmax = ref.inplace_rmax
     del ref
     gc.collect()
     torch.cuda.empty_cache()
-    cy = [r["c_y"] for r in rows]
-    return {"plan": wa["name"], "rmax": None, "audited": rows, "min_c_y": min(cy) if cy else None,
-            "mean_c_y": float(np.mean(cy)) if cy else None, "all_c_y_ge_0.9999": all(c >= 0.9999 for c in cy)}
+    cy = [r[1] for r in rows]
+    rl = [r[2] for r in rows]
+    return {"plan": wa["name"], "rmax": rmax, "audited": len(rows), "mode": args.audit_mode,
+            "ids": "64 of the 2048 generation samples, chosen before generation by an independent PCG64 stream "
+                   f"(seed {args.audit_seed}, protocol_common.py:22-31)",
+            "min_c_y": min(cy) if cy else None, "mean_c_y": float(np.mean(cy)) if cy else None,
+            "max_rel_l2": max(rl) if rl else None, "mean_rel_l2": float(np.mean(rl)) if rl else None,
+            "all_c_y_ge_0.9999": all(c >= 0.9999 for c in cy), "all_rel_l2_lt_1e-5": all(x < 1e-5 for x in rl),
+            "straddles": straddles, "straddles_outside_margin": bad,
+            "complex128_seconds_per_block": float(np.mean(secs)) if secs else None, "complex128_setup_s": setup,
+            "complex64_seconds": a64["seconds"],
+            "rows_fields": ["sample id", "c_y", "rel L2", "index (complex64)", "index (complex128)"],
+            "rows": rows}
+
+
+def gpu_small_configs(args, local):
+    """The small workloads measured completely on the GPU: device-resident samples/s (inputs
+    prepared and uploaded first), end to end through sampling.sample_checked, and c_y of a few
+    samples against complex128 recontractions."""
+    import gc
+    import torch
+    from dcs245_classical_sampling_b200 import _lib
+    from dcs245_classical_sampling_b200.audit import audit_vector_pair
+    from dcs245_classical_sampling_b200.engine import InplaceConditionalBlockGPU
+    from dcs245_classical_sampling_b200.sampling import make_protocol, sample_checked
+    from dcs245_classical_sampling_b200.workloads import build_workload
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    out = {}
+    for name, cfg in SMALL_CONFIGS.items():
+        w = build_workload(name)
+        args6 = (w["graph"], w["unitaries"], w["n"], w["order"], w["parity_operations"], w["open_vertices"])
+        eng = InplaceConditionalBlockGPU(*args6)
+        eng.alloc(np.complex64, device=local, mode=cfg["mode"])
+        if cfg["mode"] == "fused":
+            eng.set_fused_config(variant=12, low=3, grouping="bytes", jit=True)
+        recs = make_protocol(args.seed, cfg["samples"], w["n"], w["open_vertices"])["records"]
+        xs = [np.array([int(c) for c in r["input_data_bits"]], np.uint8) for r in recs]
+        us = [r["draw_uniform"] for r in recs]
+        k = eng.k
+        preps = [eng.prepare([x]) for x in xs]
+        outs = torch.empty((len(xs), 1 << k), dtype=torch.complex128, device=dev)
+        d_us = torch.tensor(us, dtype=torch.float64, device=dev)
+        res = torch.empty((len(xs), _lib.DRAW_DTYPE.itemsize), dtype=torch.uint8, device=dev)
+        lib = _lib.load()
+        scratch = torch.empty(lib.dcs_draw_scratch_bytes(k, 1), dtype=torch.uint8, device=dev)
+        for i in range(min(3, len(xs))):
+            eng.enqueue(preps[i], outs[i:i + 1])
+        torch.cuda.synchronize(dev)
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for i in range(len(xs)):
+            eng.enqueue(preps[i], outs[i:i + 1])
+            _lib.check(lib.dcs_draw(_lib.ptr(outs[i]), k, 1, _lib.ptr(d_us[i:i + 1]), _lib.ptr(scratch),
+                                    _lib.ptr(res[i]), stream.cuda_stream))
+        b.record(stream)
+        torch.cuda.synchronize(dev)
+        value = len(xs) / (a.elapsed_time(b) / 1000.0)
+        sample_checked(eng, xs[:3], us[:3], hashes=True, exact_cdf=True)
+        torch.cuda.synchronize(dev)
+        a.record(stream)
+        e2e_recs = sample_checked(eng, xs, us, hashes=True, exact_cdf=True)
+        b.record(stream)
+        torch.cuda.synchronize(dev)
+        e2e = len(xs) / (a.elapsed_time(b) / 1000.0)
+        idx = [int(d["index"]) for d in res.cpu().numpy().view(_lib.DRAW_DTYPE).reshape(-1)]
+        same = idx == [r["A_index"] for r in e2e_recs]
+        ref = InplaceConditionalBlockGPU(*args6)
+        ref.alloc(np.complex128, device=local, mode="device")
+        cy = []
+        for i in range(4):
+            v128, _ = ref.block(xs[i])
+            cy.append(audit_vector_pair(v128, outs[i], i)["normalized_conditional_overlap_abs"])
+        out[name] = {"value": value, "unit": "samples/s", "samples": len(xs), "mode": cfg["mode"],
+                     "e2e": {"value": e2e, "unit": "samples/s", "h2d_bytes_per_step": preps[0]["h2d_bytes"] + 8,
+                             "d2h_bytes_per_step": (1 << k) * 16 + _lib.DRAW_DTYPE.itemsize + 8 * eng.items},
+                     "e2e_same_indices": same, "min_c_y_4_audits": min(cy), "indices_head": idx[:8]}
+        del eng, ref, preps, outs
+        gc.collect()
+        torch.cuda.empty_cache()
+    return out
 
 
 def eng_rmax(w):
@@ -495,7 +683,7 @@ def kernel_roofline(eng, prep, out, stream):
     tot_b = sum(x for _, _, x in evs)
     n = len(evs)
     return {"kernel": kernel, "launches": n, "avg_launch_s": tot_t / n, "alg_bytes_per_launch": tot_b / n,
-            "launch_ms": [round(a.elapsed_time(b), 3) for a, b, _ in evs]}
+            "launch_ms": [a.elapsed_time(b) for a, b, _ in evs], "launch_bytes": [x for _, _, x in evs]}
 
 
 def serve_arm(args):
@@ -554,7 +742,124 @@ def serve_arm(args):
     print(json.dumps(line), flush=True)
 
 
+def profile_case(argv):
+    """Small, self-contained profiling case for the contraction kernels (the cases the ncu
+    summaries under profiles/ capture).
+
+    Runs the first vertex steps of a workload's plan whose table stays within 2^max_slots
+    entries (default 2^28 complex64 = 2 GiB: larger than L2, small enough for a full ncu
+    capture), for one prefix and one slice, `iters` times, with either the fused kernels or the
+    per-step kernel.  Prints one JSON line with the per-launch CUDA-event timings.
+
+        python bench.py --profile-case [--mode fused|device] [--max-slots 28] [--storage float16] ..."""
+    import torch
+
+    from dcs245_classical_sampling_b200 import _lib
+    from dcs245_classical_sampling_b200 import plan as P
+    from dcs245_classical_sampling_b200.engine import SliceParams, device_steps
+    from dcs245_classical_sampling_b200.fused import build_fused_plan
+    from dcs245_classical_sampling_b200.sampling import make_protocol
+    from dcs245_classical_sampling_b200.workloads import build_workload
+
+    ap = argparse.ArgumentParser(prog="bench.py --profile-case")
+    ap.add_argument("--workload", default="ring64_d73_t314_k20")
+    ap.add_argument("--mode", default="fused", choices=["fused", "device"])
+    ap.add_argument("--max-slots", type=int, default=28)
+    ap.add_argument("--iters", type=int, default=3)
+    ap.add_argument("--max-dim", type=int, default=13)
+    ap.add_argument("--low", type=int, default=4)
+    ap.add_argument("--variant", type=int, default=0)
+    ap.add_argument("--pairs", action="store_true", help="two steps per shared-memory round trip")
+    ap.add_argument("--jit", action="store_true", help="plan-specialised group kernels (register-run variants)")
+    ap.add_argument("--grouping", default="greedy", choices=["greedy", "bytes"],
+                    help="fused groups: greedy spans or fewest table bytes")
+    ap.add_argument("--storage", default=None, choices=["float16"],
+                    help="binary16 tables with FP64 arithmetic (device mode)")
+    a = ap.parse_args(argv)
+    lib = _lib.load()
+    w = build_workload(a.workload)
+    bp = P.build_block_plan(w["graph"], w["unitaries"], w["n"], w["order"], w["parity_operations"],
+                            w["open_vertices"])
+    last = 0
+    for j, st in enumerate(bp.steps):
+        top = max(st.active_in + st.active_out + (0,)) + 1
+        if st.kind == "grow":
+            top = max(top, st.pivot + 1)
+        if top > a.max_slots:
+            break
+        last = j + 1
+    steps = bp.steps[:last]
+    proto = make_protocol(5, 1, w["n"], w["open_vertices"])
+    x = np.array([int(c) for c in proto["records"][0]["input_data_bits"]], np.uint8)
+    _, items = SliceParams(bp).items(x)
+    params = torch.from_numpy(items[0][1][:last].copy().view(np.int64)).cuda()
+    dev = torch.device("cuda", 0)
+    half = a.storage == "float16"
+    if half and a.mode != "device":
+        raise SystemExit("--storage float16 takes --mode device")
+    entry = 4 if half else 8
+    if half:
+        table = torch.empty(2 << a.max_slots, dtype=torch.float16, device=dev)
+    else:
+        table = torch.empty(1 << a.max_slots, dtype=torch.complex64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    sub = P.BlockPlan(**{**bp.__dict__, "steps": steps})
+    if a.mode == "fused":
+        fp = build_fused_plan(sub, max_dim=a.max_dim, low=a.low, variant=a.variant, pairs=a.pairs,
+                              grouping=a.grouping)
+        if a.jit:
+            from dcs245_classical_sampling_b200.jit import JitPlan
+            fp.jit = JitPlan(sub, fp, lib)
+        nmax = len(fp.groups)
+    else:
+        dsteps = device_steps(steps)
+        nmax = last
+    maxbits = torch.zeros(nmax + 1, dtype=torch.int64, device=dev)
+    scale = torch.zeros(_lib.SCALE_DTYPE.itemsize // 8, dtype=torch.int64, device=dev)
+    one = (int(np.array([1.0], np.float64).view(np.int64)[0]) if half
+           else int(np.array([1.0], np.float32).view(np.uint32)[0]))
+    per_launch = []
+    for it in range(a.iters):
+        maxbits.zero_()
+        maxbits[0] = one
+        scale.zero_()
+        if half:
+            table[0], table[1] = 1, 0
+        else:
+            table[0] = 1
+        evs = []
+        for g in range(nmax):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            if a.mode == "fused":
+                _lib.check(fp.launch(lib, _lib.ptr(table), _lib.ptr(params), g, 1, _lib.ptr(maxbits),
+                                     _lib.ptr(scale), stream.cuda_stream))
+                first, count = fp.spans[g]
+                alg = ((1 << len(steps[first].active_in)) + (1 << len(steps[first + count - 1].active_out))) * 8
+            else:
+                _lib.check(lib.dcs_slice_steps(_lib.H16 if half else _lib.C64, _lib.ptr(table), dsteps.ctypes.data,
+                                               _lib.ptr(params), last, g, 1, _lib.ptr(maxbits), _lib.ptr(scale),
+                                               stream.cuda_stream))
+                alg = ((1 << len(steps[g].active_in)) + (1 << len(steps[g].active_out))) * entry
+            e1.record(stream)
+            evs.append((e0, e1, alg))
+        torch.cuda.synchronize(dev)
+        if it == a.iters - 1:
+            per_launch = [(x0.elapsed_time(x1), alg) for x0, x1, alg in evs]
+    tot_ms = sum(t for t, _ in per_launch)
+    tot_b = sum(b for _, b in per_launch)
+    big = [(t, b) for t, b in per_launch if b >= (1 << 27) * entry]
+    print(json.dumps({"mode": a.mode, "storage": a.storage or "complex64", "steps": last, "launches": len(per_launch), "total_ms": tot_ms,
+                      "alg_gb": tot_b / 1e9, "alg_gbs": tot_b / tot_ms / 1e6,
+                      "big_launch_gbs": (sum(b for _, b in big) / sum(t for t, _ in big) / 1e6) if big else None,
+                      "per_launch_ms": [round(t, 3) for t, _ in per_launch]}))
+
+
 def main():
+    if "--profile-case" in sys.argv[1:]:
+        profile_case([x for x in sys.argv[1:] if x != "--profile-case"])
+        return
     args = parse()
     if args.impl == "reference":
         reference_arm(args)

@@ -17,6 +17,7 @@ LIB_PATH = PKG / "libdcs245.so"
 C64, C128, H16 = 0, 1, 2  # table storage: complex64, complex128, two binary16 components
 MAX_RUNS = 28
 E_ARG, E_CUDA, E_NONFINITE, E_CDF = -1, -2, -3, -4
+DRAW_SEQUENTIAL = 1  # dcs_draw_ex flag: numpy's sequential CDF pass for every block
 
 STEP_DTYPE = np.dtype([
     ("K", "<u8"), ("Ka", "<u8"), ("beta", "<u8"), ("pivot_bit", "<u8"), ("in_mask", "<u8"),
@@ -71,6 +72,7 @@ SIGNATURES = {
     "dcs_block_tail": (_I, [_P, _I, _P, _P, _I, _P]),
     "dcs_draw_scratch_bytes": (ctypes.c_size_t, [_I, _I]),
     "dcs_draw": (_I, [_P, _I, _I, _P, _P, _P, _P]),
+    "dcs_draw_ex": (_I, [_P, _I, _I, _P, ctypes.c_uint, _P, _P, _P]),
     "dcs_draw_static": (_I, [_P, _I, _P, _P, _P]),
     "dcs_overlap": (_I, [_P, _P, _U64, _P, _P, _P]),
     "dcs_philox_prefixes": (_I, [_P, _P, _I, _U64, _P, _I, _P, _P, _P]),

@@ -14,8 +14,11 @@
 //      |S_i - P_i| <= gamma_{i} P_i (Higham, Accuracy and Stability, Sec. 4.2), so if u lies
 //      outside the error intervals of both bin edges, numpy's index is the same index.
 //      Otherwise the block is flagged as a tie and an exact sequential FP64 pass (the same
-//      operation order as numpy's cumsum) decides — on the device, without host sync;
+//      operation order as numpy's cumsum) decides — on the device, without host sync.  On
+//      request (DCS_DRAW_SEQUENTIAL) that pass runs for every block, so that the reported CDF
+//      values are numpy's bit for bit (the production record rows derive a grid count from them);
 //   5. the 53-bit grid total-variation diagnostic of the reference.
+#include <cuda.h>
 #include <string.h>
 
 #include <mutex>
@@ -71,19 +74,24 @@ struct BlockState {  // per block scratch (device)
     int32_t nonfinite;
 };
 
+// sequential pass: one checkpoint (the running FP64 sum before the group) per 32 elements
+constexpr int kSeqLog = 5;
+__host__ __device__ constexpr size_t seq_groups(size_t n) { return (n + 31) >> kSeqLog; }
+
 // layout of the scratch area
 struct Layout {
-    size_t w, chunk_sum, state, tv_part, bytes;
+    size_t w, chunk_sum, state, tv_part, ckpt, bytes;
 };
-__host__ __device__ inline Layout layout(int k, int nblocks) {
+__host__ __device__ constexpr Layout layout(int k, int nblocks) {
     const size_t n = (size_t)1 << k;
     const size_t nch = n >= (size_t)kChunk ? n / kChunk : 1;
-    Layout L;
+    Layout L{};
     L.w = 0;
     L.chunk_sum = L.w + n * nblocks * sizeof(double);
     L.state = L.chunk_sum + nch * nblocks * sizeof(dd);
     L.tv_part = L.state + nblocks * sizeof(BlockState);
-    L.bytes = L.tv_part + nch * nblocks * sizeof(double);
+    L.ckpt = L.tv_part + nch * nblocks * sizeof(double);
+    L.bytes = L.ckpt + seq_groups(n) * nblocks * sizeof(double);
     L.bytes = (L.bytes + 255) & ~(size_t)255;
     return L;
 }
@@ -253,38 +261,94 @@ k_locate_elem(const double* __restrict__ w, int k, const dd* __restrict__ chunk_
     }
 }
 
-// 4. exact sequential FP64 CDF (numpy's operation order) for blocks flagged as ties
-__global__ void k_sequential(const double* __restrict__ w, int k, BlockState* __restrict__ state,
-                             dcs_draw_result* __restrict__ res, int nblocks) {
-    const int b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= nblocks) return;
+// 4. exact sequential FP64 CDF (numpy's operation order), one warp per block: for blocks
+//    flagged as ties, or for every block when `force`.  Every lane runs the same dependent
+//    chain S <- S + w_i (the 32 weights of a group are loaded by the 32 lanes and broadcast by
+//    shuffles, the next 128 prefetched), so the chain is numpy's cumsum exactly.  Pass 1 gives
+//    S_n and a checkpoint before every 32-element group; the selected group is the last one
+//    whose starting value satisfies fl(start / S_n) <= u (fl(x / S_n) is non-decreasing in x),
+//    and pass 2 replays that group only.  The compensated interval of the selected index is
+//    checked against u as the reference's independent check does (sampling_protocol.py:67-72).
+__global__ void __launch_bounds__(32)
+k_sequential(const double* __restrict__ w, int k, const dd* __restrict__ chunk_sum, int nch,
+             BlockState* __restrict__ state, dcs_draw_result* __restrict__ res, double* __restrict__ ckpt,
+             int force) {
+    const int b = blockIdx.x;
+    const int lane = threadIdx.x;
     dcs_draw_result& r = res[b];
-    if (state[b].status || !r.tie) return;
+    if (state[b].status || !(r.tie || force)) return;
     const uint64_t n = 1ull << k;
+    const uint64_t ng = seq_groups(n);
     const double* wb = w + ((uint64_t)b << k);
+    double* ck = ckpt + (uint64_t)b * ng;
+    // pass 1: S_n with checkpoints, four groups (128 weights) per iteration, the next four in flight
     double S = 0.0;
-    for (uint64_t i = 0; i < n; ++i) S = __dadd_rn(S, wb[i]);
-    if (!(S > 0.0) || !isfinite(S)) { r.status = DCS_E_CDF; return; }
+    double cur[4], nxt[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const uint64_t i = (uint64_t)q * 32 + lane;
+        cur[q] = i < n ? wb[i] : 0.0;
+    }
+    for (uint64_t g0 = 0; g0 < ng; g0 += 4) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const uint64_t i = (g0 + 4 + q) * 32 + lane;
+            nxt[q] = i < n ? wb[i] : 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            if (g0 + q < ng) {
+                if (lane == 0) ck[g0 + q] = S;
+                const uint64_t base = (g0 + q) * 32;
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                    const double v = __shfl_sync(0xffffffffu, cur[q], j);
+                    if (base + j < n) S = __dadd_rn(S, v);
+                }
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) cur[q] = nxt[q];
+    }
+    if (lane != 0) return;  // lane 0 wrote the checkpoints and finishes alone
+    if (!(S > 0.0) || !isfinite(S)) {
+        r.status = DCS_E_CDF;
+        return;
+    }
     const double u = r.uniform;
-    double run = 0.0, prev = 0.0;
-    dd exact{0.0, 0.0}, exact_prev{0.0, 0.0};
+    // last group whose starting value's quotient is <= u (group 0 starts at 0)
+    uint64_t lo = 0, hi = ng - 1;
+    while (lo < hi) {
+        const uint64_t mid = (lo + hi + 1) >> 1;
+        if (__ddiv_rn(ck[mid], S) <= u) lo = mid; else hi = mid - 1;
+    }
+    // pass 2: replay the group; the last element's value is forced to 1 (numpy: cumulative[-1] = 1)
+    double run = ck[lo], prev = __ddiv_rn(run, S);
     uint64_t idx = n - 1;
-    for (uint64_t i = 0; i < n; ++i) {
+    double upper = 1.0;
+    for (uint64_t i = lo * 32; i < n && i < (lo + 1) * 32; ++i) {
         run = __dadd_rn(run, wb[i]);
-        exact_prev = exact;
-        exact = dd_add(exact, wb[i]);
         const double ci = (i == n - 1) ? 1.0 : __ddiv_rn(run, S);
-        if (u < ci) { idx = i; r.cdf_upper = ci; break; }
+        if (u < ci) { idx = i; upper = ci; break; }
         prev = ci;
     }
+    // compensated prefix before idx: the scan's chunk prefix plus the chunk's elements before idx
+    const uint64_t c0 = idx / kChunk;
+    dd pre = chunk_sum[(uint64_t)b * nch + c0];
+    for (uint64_t i = c0 * kChunk; i < idx; ++i) pre = dd_add(pre, wb[i]);
+    const dd at = dd_add(pre, wb[idx]);
     const dd T = state[b].total;
     r.cdf_lower = idx ? prev : 0.0;
-    r.cdf_lower_exact = __ddiv_rn(exact_prev.hi, T.hi);
-    r.cdf_upper_exact = __ddiv_rn(exact.hi, T.hi);
+    r.cdf_upper = upper;
+    r.cdf_lower_exact = __ddiv_rn(pre.hi, T.hi);
+    r.cdf_upper_exact = __ddiv_rn(at.hi, T.hi);
     r.index = (int64_t)idx;
     r.total_cdf = S;
+    r.total_exact = T.hi;
     r.selected_weight = wb[idx];
     if (!(wb[idx] > 0.0)) r.status = DCS_E_CDF;
+    // the reference's independent check of the interval (a disagreement is an error, never a resample)
+    else if (!(r.cdf_lower_exact <= u && u < r.cdf_upper_exact)) r.status = DCS_E_CDF;
 }
 
 // 5. 53-bit grid TV, per chunk partial sums (deterministic final sum in k_tv_final)
@@ -384,21 +448,20 @@ extern "C" size_t dcs_draw_scratch_bytes(int k, int nblocks) {
     return layout(k, nblocks).bytes;
 }
 
-extern "C" int dcs_draw(const double* blocks, int k, int nblocks, const double* uniforms, void* scratch,
-                        dcs_draw_result* results, void* stream) {
-    if (!blocks || !uniforms || !scratch || !results || k < 0 || k > 30 || nblocks < 1 || nblocks > 65535) {
-        dcs_host::set_error("dcs_draw: invalid arguments");
-        return DCS_E_ARG;
-    }
+namespace {
+// the draw kernels on a scratch area laid out by layout(k, nblocks)
+int enqueue_draw(const double* blocks, int k, int nblocks, const double* uniforms, unsigned flags, void* scratch,
+                 dcs_draw_result* results, cudaStream_t s) {
     const Layout L = layout(k, nblocks);
     char* base = (char*)scratch;
     double* w = (double*)(base + L.w);
     dd* cs = (dd*)(base + L.chunk_sum);
     BlockState* st = (BlockState*)(base + L.state);
     double* part = (double*)(base + L.tv_part);
+    double* ck = (double*)(base + L.ckpt);
     const uint64_t n = 1ull << k;
     const int nch = (int)(n >= (uint64_t)kChunk ? n / kChunk : 1);
-    cudaStream_t s = (cudaStream_t)stream;
+    // the scratch keeps the previous call's contents: the per-block state must start at zero
     cudaError_t e = cudaMemsetAsync(st, 0, nblocks * sizeof(BlockState), s);
     if (e != cudaSuccess) return dcs_host::check_cuda(e, "dcs_draw memset");
     k_weights<<<dim3(nch, nblocks), kThreads, 0, s>>>((const double2*)blocks, k, w, cs, st);
@@ -407,13 +470,29 @@ extern "C" int dcs_draw(const double* blocks, int k, int nblocks, const double* 
     DCS_CHECK_LAUNCH("k_scan_locate");
     k_locate_elem<<<nblocks, kThreads, 0, s>>>(w, k, cs, nch, st, results);
     DCS_CHECK_LAUNCH("k_locate_elem");
-    k_sequential<<<(nblocks + 31) / 32, 32, 0, s>>>(w, k, st, results, nblocks);
+    k_sequential<<<nblocks, 32, 0, s>>>(w, k, cs, nch, st, results, ck, (flags & DCS_DRAW_SEQUENTIAL) ? 1 : 0);
     DCS_CHECK_LAUNCH("k_sequential");
     k_tv<<<dim3(nch, nblocks), kThreads, 0, s>>>(w, k, cs, nch, st, results, part);
     DCS_CHECK_LAUNCH("k_tv");
     k_tv_final<<<(nblocks + 31) / 32, 32, 0, s>>>(part, nch, st, results, nblocks);
     DCS_CHECK_LAUNCH("k_tv_final");
     return DCS_OK;
+}
+}  // namespace
+
+extern "C" int dcs_draw_ex(const double* blocks, int k, int nblocks, const double* uniforms, unsigned flags,
+                           void* scratch, dcs_draw_result* results, void* stream) {
+    if (!blocks || !uniforms || !scratch || !results || k < 0 || k > 30 || nblocks < 1 || nblocks > 65535 ||
+        (flags & ~(unsigned)DCS_DRAW_SEQUENTIAL)) {
+        dcs_host::set_error("dcs_draw: invalid arguments");
+        return DCS_E_ARG;
+    }
+    return enqueue_draw(blocks, k, nblocks, uniforms, flags, scratch, results, (cudaStream_t)stream);
+}
+
+extern "C" int dcs_draw(const double* blocks, int k, int nblocks, const double* uniforms, void* scratch,
+                        dcs_draw_result* results, void* stream) {
+    return dcs_draw_ex(blocks, k, nblocks, uniforms, 0u, scratch, results, stream);
 }
 
 extern "C" int dcs_overlap(const double* ref, const double* ap, uint64_t len, double* out, void* scratch,
@@ -440,16 +519,39 @@ extern "C" int dcs_overlap(const double* ref, const double* ap, uint64_t len, do
 // in a file-scope device array of fixed size, so this entry point allocates nothing.
 //
 // Limit: one block of up to 2^20 amplitudes per call (DCS_DRAW_STATIC_MAX_K); every GPU that
-// loads the library holds the array (about 8.1 MiB) until the process exits.
+// loads the library holds the array (about 8.4 MiB) until the process exits.
 namespace {
-constexpr size_t kStaticDrawBytes = ((size_t)1 << DCS_DRAW_STATIC_MAX_K) * sizeof(double) +
-                                    (((size_t)1 << DCS_DRAW_STATIC_MAX_K) / kChunk) * (sizeof(dd) + sizeof(double)) +
-                                    sizeof(BlockState) + 4096;
+constexpr size_t kStaticDrawBytes = layout(DCS_DRAW_STATIC_MAX_K, 1).bytes;
 static __device__ __align__(256) unsigned char g_draw_scratch[kStaticDrawBytes];
 
-// the device address of g_draw_scratch, looked up once per device with that device current
+// The device address of g_draw_scratch, looked up once per device with that device current,
+// and the context it was looked up in: a new context on the device (after cudaDeviceReset, or
+// a context torn down and created again) loads the module elsewhere, so the lookup is redone.
 std::mutex g_static_mutex;
 void* g_static_ptr[64] = {nullptr};
+void* g_static_ctx[64] = {nullptr};
+typedef CUresult (*ctx_get_current_fn)(CUcontext*);
+
+int current_context(void** ctx) {
+    static ctx_get_current_fn fn = nullptr;
+    if (!fn) {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        const cudaError_t e = cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q);
+        if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !f) {
+            dcs_host::set_error("dcs_draw_static: cuCtxGetCurrent is not available");
+            return DCS_E_CUDA;
+        }
+        fn = (ctx_get_current_fn)f;
+    }
+    CUcontext c = nullptr;
+    if (fn(&c) != CUDA_SUCCESS) {
+        dcs_host::set_error("dcs_draw_static: cuCtxGetCurrent failed");
+        return DCS_E_CUDA;
+    }
+    *ctx = (void*)c;
+    return DCS_OK;
+}
 }  // namespace
 
 extern "C" int dcs_draw_static(const double* blocks, int k, const double* uniform, dcs_draw_result* result,
@@ -474,36 +576,17 @@ extern "C" int dcs_draw_static(const double* blocks, int k, const double* unifor
     void* scratch = nullptr;
     {
         std::lock_guard<std::mutex> lock(g_static_mutex);
-        if (!g_static_ptr[dev]) {
+        void* ctx = nullptr;
+        const int rc = current_context(&ctx);
+        if (rc != DCS_OK) return rc;
+        if (!g_static_ptr[dev] || g_static_ctx[dev] != ctx) {
             void* p = nullptr;
             e = cudaGetSymbolAddress(&p, g_draw_scratch);
             if (e != cudaSuccess) return dcs_host::check_cuda(e, "dcs_draw_static: cudaGetSymbolAddress");
             g_static_ptr[dev] = p;
+            g_static_ctx[dev] = ctx;
         }
         scratch = g_static_ptr[dev];
     }
-    char* base = (char*)scratch;
-    double* w = (double*)(base + L.w);
-    dd* cs = (dd*)(base + L.chunk_sum);
-    BlockState* st = (BlockState*)(base + L.state);
-    double* part = (double*)(base + L.tv_part);
-    const uint64_t n = 1ull << k;
-    const int nch = (int)(n >= (uint64_t)kChunk ? n / kChunk : 1);
-    cudaStream_t s = (cudaStream_t)stream;
-    // the array keeps the previous call's contents: the per-block state must start at zero
-    e = cudaMemsetAsync(st, 0, sizeof(BlockState), s);
-    if (e != cudaSuccess) return dcs_host::check_cuda(e, "dcs_draw_static memset");
-    k_weights<<<dim3(nch, 1), kThreads, 0, s>>>((const double2*)blocks, k, w, cs, st);
-    DCS_CHECK_LAUNCH("k_weights");
-    k_scan_locate<<<1, 1, 0, s>>>(cs, nch, uniform, st, result);
-    DCS_CHECK_LAUNCH("k_scan_locate");
-    k_locate_elem<<<1, kThreads, 0, s>>>(w, k, cs, nch, st, result);
-    DCS_CHECK_LAUNCH("k_locate_elem");
-    k_sequential<<<1, 32, 0, s>>>(w, k, st, result, 1);
-    DCS_CHECK_LAUNCH("k_sequential");
-    k_tv<<<dim3(nch, 1), kThreads, 0, s>>>(w, k, cs, nch, st, result, part);
-    DCS_CHECK_LAUNCH("k_tv");
-    k_tv_final<<<1, 32, 0, s>>>(part, nch, st, result, 1);
-    DCS_CHECK_LAUNCH("k_tv_final");
-    return DCS_OK;
+    return enqueue_draw(blocks, k, 1, uniform, 0u, scratch, result, (cudaStream_t)stream);
 }

@@ -41,35 +41,61 @@ struct jit_scale {
 #define JK_SHRINK4 6
 #define JK_SHRINK2 7
 
+// Entry type of a translation unit: complex64 tables with FP32 arithmetic (default), or
+// complex128 tables with FP64 arithmetic when the unit defines DCS_JIT_FP64 (the audit
+// recontraction).  One unit holds kernels of one type only.
+#ifdef DCS_JIT_FP64
+typedef double real_t;
+typedef double2 cplx_t;
+typedef double4 wts_t;
+#else
+typedef float real_t;
+typedef float2 cplx_t;
+typedef float4 wts_t;
+#endif
+
 namespace jit {
 
 #ifndef DCS_JIT_THREADS
 #define DCS_JIT_THREADS 256
 #endif
 constexpr int kThreads = DCS_JIT_THREADS;  // threads per CTA of every kernel of the unit
-constexpr uint32_t kSign = 0x80000000u;
+constexpr uint32_t kSign = 0x80000000u;  // sign bit of an FP32 value, or of an FP64 value's high word
 
 __host__ __device__ constexpr int cpar(int x) { return x ? ((x & 1) ^ cpar(x >> 1)) : 0; }
 
 __device__ __forceinline__ float2 f2(float x, float y) { return make_float2(x, y); }
-__device__ __forceinline__ float2 sflip(float2 a, uint32_t m) {
-    return f2(__uint_as_float(__float_as_uint(a.x) ^ m), __uint_as_float(__float_as_uint(a.y) ^ m));
+__device__ __forceinline__ double2 f2(double x, double y) { return make_double2(x, y); }
+__device__ __forceinline__ float rfma(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ double rfma(double a, double b, double c) { return fma(a, b, c); }
+// sign flip by bit 31 of m
+__device__ __forceinline__ float sflip1(float a, uint32_t m) { return __uint_as_float(__float_as_uint(a) ^ m); }
+__device__ __forceinline__ double sflip1(double a, uint32_t m) {
+    return __hiloint2double(__double2hiint(a) ^ (int)m, __double2loint(a));
 }
+__device__ __forceinline__ cplx_t sflip(cplx_t a, uint32_t m) { return f2(sflip1(a.x, m), sflip1(a.y, m)); }
 // f * x
-__device__ __forceinline__ float2 zmul(float2 f, float2 x) {
-    return f2(fmaf(f.x, x.x, -f.y * x.y), fmaf(f.x, x.y, f.y * x.x));
+__device__ __forceinline__ cplx_t zmul(cplx_t f, cplx_t x) {
+    return f2(rfma(f.x, x.x, -f.y * x.y), rfma(f.x, x.y, f.y * x.x));
 }
 // acc + f * x
-__device__ __forceinline__ float2 zmadd(float2 f, float2 x, float2 acc) {
-    return f2(fmaf(f.x, x.x, fmaf(-f.y, x.y, acc.x)), fmaf(f.x, x.y, fmaf(f.y, x.x, acc.y)));
+__device__ __forceinline__ cplx_t zmadd(cplx_t f, cplx_t x, cplx_t acc) {
+    return f2(rfma(f.x, x.x, rfma(-f.y, x.y, acc.x)), rfma(f.x, x.y, rfma(f.y, x.x, acc.y)));
 }
-__device__ __forceinline__ float2 zadd(float2 a, float2 b) { return f2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ cplx_t zadd(cplx_t a, cplx_t b) { return f2(a.x + b.x, a.y + b.y); }
 // a + (-1)^NEG b
 template <int NEG>
-__device__ __forceinline__ float2 zaddg(float2 a, float2 b) {
+__device__ __forceinline__ cplx_t zaddg(cplx_t a, cplx_t b) {
     if constexpr (NEG) return f2(a.x - b.x, a.y - b.y);
     else return f2(a.x + b.x, a.y + b.y);
 }
+// |x|^2 of a stored entry, the running max, and the order-preserving key of a non-negative
+// value (maxbits)
+__device__ __forceinline__ real_t norm2(cplx_t q) { return q.x * q.x + q.y * q.y; }
+__device__ __forceinline__ float rmax(float a, float b) { return fmaxf(a, b); }
+__device__ __forceinline__ double rmax(double a, double b) { return fmax(a, b); }
+__device__ __forceinline__ unsigned long long max_key(float m) { return (unsigned long long)__float_as_uint(m); }
+__device__ __forceinline__ unsigned long long max_key(double m) { return (unsigned long long)__double_as_longlong(m); }
 
 // ---------------------------------------------------------------- orbit bodies
 // The weights are unit weights (prologue): f0 = 1 at every free step, and at a fixed step the
@@ -80,13 +106,13 @@ __device__ __forceinline__ float2 zaddg(float2 a, float2 b) {
 // odd.  SK / SKA: the partner signs (-1)^sK, (-1)^sKa.  Formulas: the per-step kernel's
 // (reference: source/kernel_opt/inplace_gpu.py:29-58) with f0 = 1.
 template <int KIND, int R, int K, int B, int DEAD, int SK, int SKA, int J = 0>
-__device__ __forceinline__ void orb1(float2 (&v)[1 << R], float2 F1p, float2 F1n, float2 Fap, float2 Fan, int y) {
+__device__ __forceinline__ void orb1(cplx_t (&v)[1 << R], cplx_t F1p, cplx_t F1n, cplx_t Fap, cplx_t Fan, int y) {
     if constexpr (J < (1 << R)) {
         if constexpr (!(J & (1 << K)) && !(J & DEAD)) {
             constexpr int D = J | (1 << K);
             constexpr bool N = cpar(J & B);
-            const float2 F1 = N ? F1n : F1p;
-            const float2 x = v[J], b = v[D];
+            const cplx_t F1 = N ? F1n : F1p;
+            const cplx_t x = v[J], b = v[D];
             if constexpr (KIND == JK_GROW) {  // v[J] = x stays
                 v[D] = zmul(F1, x);
             } else if constexpr (KIND == JK_MIX) {
@@ -105,27 +131,27 @@ __device__ __forceinline__ void orb1(float2 (&v)[1 << R], float2 F1p, float2 F1n
     }
 }
 template <int KIND, int R, int K, int B, int DEAD, int SK, int SKA>
-__device__ __forceinline__ void body1(float2 (&v)[1 << R], float4 f, int y, uint32_t m0) {
-    const float2 f1 = f2(f.z, f.w);
-    const float2 F1p = sflip(f1, m0), F1n = sflip(f1, m0 ^ kSign);
+__device__ __forceinline__ void body1(cplx_t (&v)[1 << R], wts_t f, int y, uint32_t m0) {
+    const cplx_t f1 = f2(f.z, f.w);
+    const cplx_t F1p = sflip(f1, m0), F1n = sflip(f1, m0 ^ kSign);
     constexpr uint32_t ka = SKA ? kSign : 0u;
     orb1<KIND, R, K, B, DEAD, SK, SKA>(v, F1p, F1n, sflip(F1p, ka), sflip(F1n, ka), y);
 }
 
 // One-entry kinds: every local entry without a DEAD bit.
 template <int R, int B, int DEAD, int J = 0>
-__device__ __forceinline__ void orb0(float2 (&v)[1 << R], float2 Fp, float2 Fn) {
+__device__ __forceinline__ void orb0(cplx_t (&v)[1 << R], cplx_t Fp, cplx_t Fn) {
     if constexpr (J < (1 << R)) {
         if constexpr (!(J & DEAD)) v[J] = zmul(cpar(J & B) ? Fn : Fp, v[J]);
         orb0<R, B, DEAD, J + 1>(v, Fp, Fn);
     }
 }
 template <int KIND, int R, int B, int DEAD>
-__device__ __forceinline__ void body0(float2 (&v)[1 << R], float4 f, int y, uint32_t m0) {
-    const float2 f1 = f2(f.z, f.w);
-    const float2 F1p = sflip(f1, m0), F1n = sflip(f1, m0 ^ kSign);
+__device__ __forceinline__ void body0(cplx_t (&v)[1 << R], wts_t f, int y, uint32_t m0) {
+    const cplx_t f1 = f2(f.z, f.w);
+    const cplx_t F1p = sflip(f1, m0), F1n = sflip(f1, m0 ^ kSign);
     if constexpr (KIND == JK_DIAG) {  // (1 + s f1) x
-        orb0<R, B, DEAD>(v, f2(1.f + F1p.x, F1p.y), f2(1.f + F1n.x, F1n.y));
+        orb0<R, B, DEAD>(v, f2((real_t)1 + F1p.x, F1p.y), f2((real_t)1 + F1n.x, F1n.y));
     } else {  // JK_FIXED: y ? s x : x (the selected weight is 1)
         if (y) orb0<R, B, DEAD>(v, F1p, F1n);
     }
@@ -135,13 +161,13 @@ __device__ __forceinline__ void body0(float2 (&v)[1 << R], float4 f, int y, uint
 // mask also has K2, bit 1: Ka's has K1.
 //   o_c = (x + b) + s_d f1 (g + gK h) ;  o_{c^Ka} = (g + h) + s_c f1 (x + gK b).
 template <int R, int K1, int K2, int MIX, int B, int DEAD, int SK, int J = 0>
-__device__ __forceinline__ void orb4(float2 (&v)[1 << R], float2 F1p, float2 F1n, float2 Fap, float2 Fan) {
+__device__ __forceinline__ void orb4(cplx_t (&v)[1 << R], cplx_t F1p, cplx_t F1n, cplx_t Fap, cplx_t Fan) {
     if constexpr (J < (1 << R)) {
         if constexpr (!(J & ((1 << K1) | (1 << K2))) && !(J & DEAD)) {
             constexpr int MK = (1 << K1) | ((MIX & 1) ? (1 << K2) : 0);
             constexpr int MKA = (1 << K2) | ((MIX & 2) ? (1 << K1) : 0);
             constexpr bool N = cpar(J & B);
-            const float2 x = v[J], b = v[J ^ MK], g = v[J ^ MKA], h = v[J ^ MK ^ MKA];
+            const cplx_t x = v[J], b = v[J ^ MK], g = v[J ^ MKA], h = v[J ^ MK ^ MKA];
             v[J] = zmadd(N ? Fan : Fap, zaddg<SK>(g, h), zadd(x, b));
             v[J ^ MKA] = zmadd(N ? F1n : F1p, zaddg<SK>(x, b), zadd(g, h));
         }
@@ -149,13 +175,14 @@ __device__ __forceinline__ void orb4(float2 (&v)[1 << R], float2 F1p, float2 F1n
     }
 }
 template <int R, int K1, int K2, int MIX, int B, int DEAD, int SK, int SKA>
-__device__ __forceinline__ void body4(float2 (&v)[1 << R], float4 f, int y, uint32_t m0) {
-    const float2 f1 = f2(f.z, f.w);
-    const float2 F1p = sflip(f1, m0), F1n = sflip(f1, m0 ^ kSign);
+__device__ __forceinline__ void body4(cplx_t (&v)[1 << R], wts_t f, int y, uint32_t m0) {
+    const cplx_t f1 = f2(f.z, f.w);
+    const cplx_t F1p = sflip(f1, m0), F1n = sflip(f1, m0 ^ kSign);
     constexpr uint32_t ka = SKA ? kSign : 0u;
     orb4<R, K1, K2, MIX, B, DEAD, SK>(v, F1p, F1n, sflip(F1p, ka), sflip(F1n, ka));
 }
 
+#ifndef DCS_JIT_FP64
 // ---------------------------------------------------------------- packed bodies
 // A thread holds the coset pair (t0, t0 | 1) (tile bit 0 outside the run's space): local entry
 // j of both cosets is one C2, lane 0 for t0, lane 1 for t0 | 1, and the FP32x2 instructions do
@@ -286,6 +313,8 @@ __device__ __forceinline__ void pbody4(C2 (&v)[1 << R], float4 f, int y, uint32_
     porb4<R, K1, K2, MIX, B, DEAD, SK>(v, F0, F1p, F1n, Fap, Fan);
 }
 
+#endif  // DCS_JIT_FP64
+
 // ---------------------------------------------------------------- group prologue, tiles, epilogue
 __device__ __forceinline__ int scale_exponent(double m2) {
     if (!(m2 > 0.0) || !isfinite(m2)) return 0;
@@ -302,21 +331,33 @@ __device__ __forceinline__ int scale_exponent(double m2) {
 __device__ __forceinline__ double2 step_factor(const jit_param& p, bool fixed) {
     return (fixed && (p.y & 1)) ? make_double2(p.f1r, p.f1i) : make_double2(p.f0r, p.f0i);
 }
-__device__ __forceinline__ float4 unit_weights(const jit_param& p, bool fixed) {
-    if (fixed) return (p.y & 1) ? make_float4(0.f, 0.f, 1.f, 0.f) : make_float4(1.f, 0.f, 0.f, 0.f);
+__device__ __forceinline__ wts_t unit_weights(const jit_param& p, bool fixed) {
+    wts_t w;
+    w.x = fixed && (p.y & 1) ? (real_t)0 : (real_t)1;
+    w.y = 0;
+    if (fixed) {
+        w.z = (p.y & 1) ? (real_t)1 : (real_t)0;
+        w.w = 0;
+        return w;
+    }
     const double n = p.f0r * p.f0r + p.f0i * p.f0i;  // f1 / f0
-    const double wr = (p.f1r * p.f0r + p.f1i * p.f0i) / n, wi = (p.f1i * p.f0r - p.f1r * p.f0i) / n;
-    return make_float4(1.f, 0.f, (float)wr, (float)wi);
+    w.z = (real_t)((p.f1r * p.f0r + p.f1i * p.f0i) / n);
+    w.w = (real_t)((p.f1i * p.f0r - p.f1r * p.f0i) / n);
+    return w;
 }
 
 // Pass scale 2^-e from the previous pass's max and the group's step factors (block 0 records
 // both), the unit step weights into shared memory, and the table of high tile-coordinate
 // addresses.  FIXMASK bit i: step FIRST + i is a fixed kind.
 template <int TD, int LOW, int COUNT, int FIRST, uint32_t FIXMASK>
-__device__ __forceinline__ float prologue(const jit_param* __restrict__ params, const uint64_t* basis,
-                                          const unsigned long long* maxbits, int group, jit_scale* scale,
-                                          float4* fw, int* ovy, uint64_t* hi_tab) {
+__device__ __forceinline__ real_t prologue(const jit_param* __restrict__ params, const uint64_t* basis,
+                                           const unsigned long long* maxbits, int group, jit_scale* scale,
+                                           wts_t* fw, int* ovy, uint64_t* hi_tab) {
+#ifdef DCS_JIT_FP64
+    const double m2prev = __longlong_as_double((long long)maxbits[group]);
+#else
     const double m2prev = (double)__uint_as_float((uint32_t)maxbits[group]);
+#endif
     const int e = scale_exponent(m2prev);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         double lg = 0.0, ph = 0.0;
@@ -344,9 +385,10 @@ __device__ __forceinline__ float prologue(const jit_param* __restrict__ params, 
         hi_tab[h] = a;
     }
     __syncthreads();
-    return (float)ldexp(1.0, -e);
+    return (real_t)ldexp(1.0, -e);
 }
 
+#ifndef DCS_JIT_FP64
 // Tile load: entries active before the group (as runs.cuh: 4-entry segments when slot 0 is
 // active and rows have 4 entries or more, else 16-byte pairs or single entries, zero-filled).
 template <int T, int LOW, bool PAIR_IN>
@@ -437,6 +479,8 @@ __device__ __forceinline__ float store_tile(float2* __restrict__ E, const float2
     return lm;
 }
 
+#endif  // DCS_JIT_FP64 (the FP64 units read and write the table directly in the first and last run)
+
 // Tile-constant sign parts parity(base & beta_s) ^ ov_s, one bit per step (warp 0).
 template <int COUNT>
 __device__ __forceinline__ void sign_bits(const uint64_t* beta, uint64_t base, const int* ovy, uint32_t* cs_sh) {
@@ -448,9 +492,9 @@ __device__ __forceinline__ void sign_bits(const uint64_t* beta, uint64_t base, c
     }
 }
 
-__device__ __forceinline__ void block_max(float lm, unsigned long long* maxbits, int slot) {
+__device__ __forceinline__ void block_max(real_t lm, unsigned long long* maxbits, int slot) {
     __shared__ unsigned long long red[32];
-    unsigned long long v = (unsigned long long)__float_as_uint(lm);
+    unsigned long long v = max_key(lm);
     for (int off = 16; off > 0; off >>= 1) {
         const unsigned long long o = __shfl_xor_sync(0xffffffffu, v, off);
         v = o > v ? o : v;

@@ -15,7 +15,8 @@ Execution modes (``alloc(..., mode=...)``):
   enqueued without host synchronisation, several slices (work items) per launch when the
   HBM budget allows (default);
 * ``"fused"``  — like ``device`` but several vertex steps per pass over the table
-  (coset-tiled fused kernel, complex64 only).
+  (coset-tiled fused kernels; complex128 tables run the plan-specialised register-run kernels
+  compiled in FP64, which is how the complex128 audit recontraction runs at full size).
 
 Host work per block is the reference's bookkeeping (local vectors, slice coefficients,
 offset bits), vectorised over slices; the device does every pass over the tables.
@@ -33,6 +34,12 @@ from . import _lib
 from .plan import (KIND_GROW, W_T, build_block_plan, deposit_runs, orbit_kind, slot_mask)
 
 LN2 = math.log(2.0)
+
+# Fused plan of complex128 tables (plan-specialised kernels in FP64): 2^12-entry tiles of 16-byte
+# entries (64 KB of shared memory, two CTAs per SM), 3 contiguous low bits (128-byte rows),
+# register runs of local dimension 4, groups of fewest table bytes.
+FP64_FUSED_CONFIG = {"max_dim": 12, "low": 3, "max_steps": 24, "variant": 12, "pairs": False, "grouping": "bytes",
+                     "group_cost": 1 << 30, "max_extra": 1}
 
 
 def device_steps(steps):
@@ -202,8 +209,10 @@ class InplaceConditionalBlockGPU:
                     else "device")
         if mode not in ("plain", "device", "fused"):
             raise ValueError(mode)
-        if mode == "fused" and (np.dtype(dtype) != np.dtype(np.complex64) or half):
-            raise ValueError("the fused executor stores complex64 tables")
+        if mode == "fused" and half:
+            raise ValueError("the fused executors store complex64 or complex128 tables")
+        if mode == "fused" and np.dtype(dtype) == np.dtype(np.complex128) and jit is False:
+            raise ValueError("complex128 fused tables run the plan-specialised kernels only (jit)")
         self.lib = _lib.load()
         if not torch.cuda.is_available():
             raise RuntimeError("InplaceConditionalBlockGPU needs a CUDA device")
@@ -232,7 +241,13 @@ class InplaceConditionalBlockGPU:
             budget = int((hbm_budget if hbm_budget is not None else 0.85 * free))
             items = max(1, min(nslice_items, budget // (table_entries * entry)))
         self.items = int(items)
-        if mode == "fused":
+        if mode == "fused" and self.use_fp64:
+            # complex128: 16-byte entries, so tiles of 2^12 entries (64 KB) and two CTAs per SM
+            self.fused_config = dict(FP64_FUSED_CONFIG)
+            self.jit, self.jit_minb, self.jit_threads = True, 2, 256
+            self.fplan = self._build_fplan()
+            self.items = 1
+        elif mode == "fused":
             from .autotune import cached
             cfg = cached(plan, torch.cuda.get_device_name(self.device)) or {}
             self.fused_config = {"max_dim": cfg.get("max_dim", 13), "low": cfg.get("low", 4),
@@ -281,7 +296,7 @@ class InplaceConditionalBlockGPU:
         """The fused plan of fused_config; with self.jit and register runs, its groups run as
         plan-specialised kernels (jit.py) compiled for this plan."""
         from .fused import build_fused_plan
-        fp = build_fused_plan(self.plan, **self.fused_config)
+        fp = build_fused_plan(self.plan, **self.fused_config, fp64=self.use_fp64)
         if getattr(self, "jit", False) and fp.tile_runs is not None:
             from .jit import JitPlan
             fp.jit = JitPlan(self.plan, fp, self.lib, minb=getattr(self, "jit_minb", None),
@@ -295,6 +310,8 @@ class InplaceConditionalBlockGPU:
         those kernels (default 256)."""
         if self.mode != "fused":
             raise ValueError("set_fused_config needs mode='fused'")
+        if self.use_fp64 and (jit is False or not cfg.get("variant", 4) & 4):
+            raise ValueError("complex128 fused tables run the plan-specialised register-run kernels only")
         if jit is not None:
             self.jit = bool(jit)
         if minb is not None:
@@ -311,6 +328,8 @@ class InplaceConditionalBlockGPU:
         from . import autotune as at
         if self.mode != "fused":
             return None
+        if self.use_fp64:
+            raise ValueError("the autotuner times complex64 tables")
         x = np.zeros(self.n, np.uint8) if x_bits is None else x_bits
         _, items = self.params.items(x)
         prm = torch.from_numpy(items[0][1].view(np.int64).copy()).to(self.device)
@@ -403,6 +422,8 @@ class InplaceConditionalBlockGPU:
         nm = self._nmax() + 1
         if self.mode == "fused":
             f = self.fplan
+            if not unit_ok and f.fp64:
+                raise ValueError("complex128 fused tables need step weights with f0 != 0 at every free step")
             if unit_ok:
                 _lib.check(f.launch(lib, _lib.ptr(self.table), params_ptr, 0, len(f.groups), _lib.ptr(self.maxbits),
                                     _lib.ptr(self.scale), st))
@@ -428,14 +449,16 @@ class InplaceConditionalBlockGPU:
             self.dcode, _lib.ptr(self.table), self.table_stride, self.dsteps.ctypes.data, params_ptr,
             self.nsteps, self.nsteps, 0, self.nsteps, _lib.ptr(self.maxbits), _lib.ptr(self.scale), n_items, st))
 
-    def enqueue(self, prep, out):
-        """Device work for a prepared batch into `out` ((nblocks, 2^k) complex128, zeroed):
-        contraction of every work item, accumulation, tail.  No host synchronisation
-        (except in "plain" mode).  Returns the number of library kernel launches."""
+    def enqueue(self, prep, out, flags=None):
+        """Device work for a prepared batch into `out` ((nblocks, 2^k) complex128): contraction of
+        every work item, accumulation, tail.  No host synchronisation (except in "plain" mode).
+        flags: optional (self.items,) int64 device tensor that collects the items' scale flags
+        (bit 0: a nonfinite table).  Returns the number of library kernel launches."""
         lib = self.lib
         nm = self._nmax() + 1
         entry = _lib.PARAM_DTYPE.itemsize
         launches = 0
+        out.zero_()
         for ci, (c0, cn, b0, nb, boff) in enumerate(prep["chunks"]):
             self._reset_items(cn)
             self._run_steps(_lib.ptr(prep["params"]) + c0 * self.nsteps * entry, cn, prep["unit_ok"][ci])
@@ -448,6 +471,8 @@ class InplaceConditionalBlockGPU:
                 _lib.ptr(prep["begin"]) + 4 * boff, nb, self.params.shift, _lib.ptr(self.scale),
                 _lib.ptr(self.maxbits[nm - 1:]), nm, _lib.ptr(flat), self.k, cn, self._stream()))
             launches += 2
+            if flags is not None:
+                flags[:cn] |= self.scale.view(self.items, -1)[:cn, 2]
         _lib.check(lib.dcs_block_tail(_lib.ptr(out), self.k, self.adj_hi.ctypes.data, self.u_open.ctypes.data,
                                       prep["nblocks"], self._stream()))
         launches += 2 if self.k <= 12 else 4
@@ -464,24 +489,9 @@ class InplaceConditionalBlockGPU:
 
     def _run(self, x_list, w=None, part=0, parts=1):
         prep = self.prepare(x_list, w, part, parts)
-        out = torch.zeros((len(x_list), 1 << self.k), dtype=torch.complex128, device=self.device)
+        out = torch.empty((len(x_list), 1 << self.k), dtype=torch.complex128, device=self.device)
         flags = self._flags_tensor()
-        lib = self.lib
-        nm = self._nmax() + 1
-        entry = _lib.PARAM_DTYPE.itemsize
-        for ci, (c0, cn, b0, nb, boff) in enumerate(prep["chunks"]):
-            self._reset_items(cn)
-            self._run_steps(_lib.ptr(prep["params"]) + c0 * self.nsteps * entry, cn, prep["unit_ok"][ci])
-            flat = out[b0:b0 + nb].view(torch.float64)
-            _lib.check(lib.dcs_accumulate_batched(
-                self.dcode, _lib.ptr(self.table), self.table_stride, self.plan.terminal_rank,
-                self.term_runs.ctypes.data, self.term_nruns, self.tbasis.ctypes.data,
-                _lib.ptr(prep["xors"]) + 8 * c0, _lib.ptr(prep["coefs"]) + 16 * c0,
-                _lib.ptr(prep["begin"]) + 4 * boff, nb, self.params.shift, _lib.ptr(self.scale),
-                _lib.ptr(self.maxbits[nm - 1:]), nm, _lib.ptr(flat), self.k, cn, self._stream()))
-            flags[:cn] |= self.scale.view(self.items, -1)[:cn, 2]
-        _lib.check(lib.dcs_block_tail(_lib.ptr(out), self.k, self.adj_hi.ctypes.data, self.u_open.ctypes.data,
-                                      len(x_list), self._stream()))
+        self.enqueue(prep, out, flags)
         if bool(((flags & 1) != 0).any()):  # one small device->host read per call
             raise ArithmeticError("Nonfinite in-place environment")
         return out, prep

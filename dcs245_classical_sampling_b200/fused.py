@@ -90,6 +90,8 @@ class FusedPlan:
     coset_pairs: bool = False
     # generated kernels: first and last run of a tile read and write the table directly
     direct_io: bool = True
+    # complex128 table, FP64 arithmetic (generated kernels only: the audit recontraction)
+    fp64: bool = False
     spans: list = field(default_factory=list)      # (first, count) per group
     universe: list = field(default_factory=list)   # |U| per group
     tiles: list = field(default_factory=list)      # tile count per group
@@ -103,6 +105,8 @@ class FusedPlan:
 
     def launch_library(self, lib, table, params, g0, ng, maxbits, scale, stream):
         """The library kernels (register runs where the groups have them)."""
+        if self.fp64:
+            raise ValueError("the library's fused kernels store complex64 tables")
         if self.tile_runs is not None:
             return lib.dcs_fused_runs(table, self.dsteps.ctypes.data, len(self.dsteps), self.groups.ctypes.data,
                                       len(self.groups), self.tile_steps.ctypes.data, self.tile_runs.ctypes.data,
@@ -111,7 +115,8 @@ class FusedPlan:
                                     len(self.groups), self.tile_steps.ctypes.data, params, g0, ng, maxbits, scale,
                                     stream)
 
-    def algorithmic_bytes(self, plan, elem=8):
+    def algorithmic_bytes(self, plan, elem=None):
+        elem = elem or (16 if self.fp64 else 8)
         tot = 0
         for first, count in self.spans:
             tot += ((1 << len(plan.steps[first].active_in)) + (1 << len(plan.steps[first + count - 1].active_out))) * elem
@@ -392,9 +397,10 @@ def _plan_runs(steps, first, count, tsteps, truns, dim, R, tbit, slot_of, keep_b
 
 
 def build_fused_plan(plan, max_dim=13, low=4, max_steps=MAX_GROUP_STEPS, max_extra=1, spans=None, variant=0,
-                     pairs=False, grouping="greedy", group_cost=1 << 30):
+                     pairs=False, grouping="greedy", group_cost=1 << 30, fp64=False):
     """grouping: "greedy" (group_steps) or "bytes" (group_steps_min_bytes, `group_cost` bytes
-    charged per group)."""
+    charged per group).  fp64: the plan runs on a complex128 table (plan-specialised register
+    runs only, see jit.py)."""
     steps = plan.steps
     if spans is None:
         if grouping == "bytes":
@@ -407,7 +413,7 @@ def build_fused_plan(plan, max_dim=13, low=4, max_steps=MAX_GROUP_STEPS, max_ext
     tsteps = np.zeros(len(steps), dtype=_lib.TILE_STEP_DTYPE)
     truns = np.zeros(len(steps), dtype=_lib.TILE_RUN_DTYPE) if variant & 4 else None
     fp = FusedPlan(groups=groups, tile_steps=tsteps, dsteps=device_steps(steps), spans=list(spans), tile_runs=truns,
-                   coset_pairs=bool(pairs and variant & 4))
+                   coset_pairs=bool(pairs and variant & 4), fp64=bool(fp64))
     for gi, (first, count) in enumerate(spans):
         U = 0
         vecs = []

@@ -23,7 +23,7 @@ from . import _lib
 HERE = Path(__file__).resolve().parent
 HEADER = HERE / "csrc" / "runs_jit.cuh"
 CACHE_DIR = HERE / "_jit_cache"
-KERNEL_VERSION = 8  # bump when the generated code changes meaning
+KERNEL_VERSION = 9  # bump when the generated code changes meaning
 
 ONE_VECTOR = (0, 1, 3, 5, 7)
 
@@ -101,11 +101,17 @@ def group_source(plan, fp, gi, minb=3, threads=256):
     Without it, the tile is staged in shared memory on load and store (the library kernel's
     scheme).  With ``fp.coset_pairs`` a thread takes two cosets per loop iteration where it has
     an even number of them.  `threads` per CTA: a power of two from 128 to 1024 (the packed form
-    takes 256 only)."""
+    takes 256 only).
+
+    With ``fp.fp64`` the group runs on a complex128 table with FP64 arithmetic (the unit defines
+    DCS_JIT_FP64): entries are 16 bytes, so every entry is one 16-byte access and coset pairs
+    along tile bit 0 are not merged; such groups need direct I/O."""
     if threads not in (128, 256, 512, 1024):
         raise ValueError(f"threads {threads}")
     lognt = threads.bit_length() - 1
     coset_pairs = bool(getattr(fp, "coset_pairs", False))
+    fp64 = bool(getattr(fp, "fp64", False))
+    esh = 4 if fp64 else 3  # log2 of the entry size in bytes
     g = fp.groups[gi]
     if not int(g["variant"]) & 4:
         return None
@@ -114,6 +120,8 @@ def group_source(plan, fp, gi, minb=3, threads=256):
             raise ValueError("the packed group kernels run 256 threads per CTA")
         return _packed_source(fp, gi, minb)
     direct = bool(getattr(fp, "direct_io", True)) and _direct_ok(fp, gi)
+    if fp64 and not direct:
+        raise ValueError(f"group {gi}: the complex128 group kernels read and write the table directly")
     R = 4 if int(g["variant"]) & 8 else 3
     first, count = int(g["first"]), int(g["count"])
     TD, LOW = int(g["tile_dim"]), int(g["low_bits"])
@@ -141,24 +149,24 @@ def group_source(plan, fp, gi, minb=3, threads=256):
     L.append(f"__constant__ uint64_t g{gi}_beta[{count}] = "
              f"{{{', '.join(_u64(fp.dsteps[first + s]['beta']) for s in range(count))}}};")
     L.append(f'extern "C" __global__ void __launch_bounds__({threads}, {minb})')
-    L.append(f"dcs_g{gi}(float2* __restrict__ E, const jit_param* __restrict__ params, "
+    L.append(f"dcs_g{gi}(cplx_t* __restrict__ E, const jit_param* __restrict__ params, "
              "unsigned long long* __restrict__ maxbits, jit_scale* __restrict__ scale) {")
     L.append(f"    constexpr int TD = {TD}, LOW = {LOW}, T = 1 << TD, COUNT = {count}, FIRST = {first};")
     L.append("    extern __shared__ __align__(16) unsigned char smem[];")
     if uses_tile_buffer(fp, gi):
-        L.append("    float2* sh = reinterpret_cast<float2*>(smem);")
-        L.append("    uint64_t* hi_tab = reinterpret_cast<uint64_t*>(smem + sizeof(float2) * T);")
+        L.append("    cplx_t* sh = reinterpret_cast<cplx_t*>(smem);")
+        L.append("    uint64_t* hi_tab = reinterpret_cast<uint64_t*>(smem + sizeof(cplx_t) * T);")
     else:
         L.append("    uint64_t* hi_tab = reinterpret_cast<uint64_t*>(smem);")
-    L.append("    __shared__ float4 fw[COUNT];")
+    L.append("    __shared__ wts_t fw[COUNT];")
     L.append("    __shared__ int ovy[COUNT];")
     # Direct I/O: the sign bits alternate between two words, so the barrier after a tile's sign
     # bits is the only one between tiles (the next tile's first shared-memory writes come after
     # it, and warp 0 cannot pass it before every warp has read the previous word).
     L.append("    __shared__ uint32_t cs_sh[2];")
-    L.append(f"    const float sc = jit::prologue<TD, LOW, COUNT, FIRST, {_fixmask(fp, first, count)}u>(params, "
+    L.append(f"    const real_t sc = jit::prologue<TD, LOW, COUNT, FIRST, {_fixmask(fp, first, count)}u>(params, "
              f"g{gi}_basis, maxbits, {gi}, scale, fw, ovy, hi_tab);")
-    L.append("    float lm = 0.f;")
+    L.append("    real_t lm = 0;")
     L.append("    uint32_t par = 0;")
     L.append(f"    for (uint64_t tile = blockIdx.x; tile < {_u64(1 << int(g['coset_m']))}; tile += gridDim.x) {{")
     L.append(f"        const uint64_t base = {_deposit_expr(g)};")
@@ -187,14 +195,14 @@ def group_source(plan, fp, gi, minb=3, threads=256):
         NB = T >> nins
         niter = NB >> lognt if NB > threads else 1
         free = [b for b in range(TD) if b not in ins]  # thread index bits fill free[:lognt]
-        mhi3 = sum(1 << b for b in free[lognt:]) << 3
-        free3 = sum(1 << b for b in free) << 3  # bits a representative's byte offset can have
+        mhi3 = sum(1 << b for b in free[lognt:]) << esh
+        free3 = sum(1 << b for b in free) << esh  # bits a representative's byte offset can have
 
         def sh_off(c, o, free3=free3):
             """Byte offset of a local entry: t0 ^ o, written t0 + o when o has no bit that t0 can
             have (then the offset is an immediate of the shared-memory access)."""
             return f"(t0{c} + {o}u)" if not (o & free3) else f"(t0{c} ^ {o}u)"
-        offs = [int(tr["off"][j]) << 3 for j in range(1 << R)]
+        offs = [int(tr["off"][j]) << esh for j in range(1 << R)]
         G = [gaddr(int(tr["off"][j])) for j in range(1 << R)]
         L.append(f"        // run: steps {first + s}..{first + s + n - 1}, {NB} cosets of {1 << R} entries"
                  f"{', from the table' if src_g else ''}{', to the table' if dst_g else ''}")
@@ -204,10 +212,11 @@ def group_source(plan, fp, gi, minb=3, threads=256):
         L.append("                uint32_t tp = threadIdx.x;")
         for p in ins:
             L.append(f"                tp = jit::ins0(tp, {p});")
-        L.append("                tp <<= 3;")
+        L.append(f"                tp <<= {esh};")
         L.append("                uint32_t tu = 0;")
         # local bit k0 with basis vector e_0: entries j and j | 2^k0 are one aligned 16-byte word
-        k0 = next((k for k in range(R) if int(tr["off"][1 << k]) == 1), None)
+        # (complex64 entries only)
+        k0 = None if fp64 else next((k for k in range(R) if int(tr["off"][1 << k]) == 1), None)
         pairs = [(j, j | (1 << k0)) for j in range(1 << R) if not (j >> k0) & 1] if k0 is not None else None
         cos = ["a", "b"] if coset_pairs and niter % 2 == 0 else ["a"]
         L.append("#pragma unroll 1")
@@ -215,10 +224,10 @@ def group_source(plan, fp, gi, minb=3, threads=256):
         for c in cos:
             L.append(f"                    const uint32_t t0{c} = tp | tu;")
             L.append(f"                    tu = ((tu | ~{mhi3}u) + 1u) & {mhi3}u;")
-            L.append(f"                    float2 v{c}[{1 << R}];")
+            L.append(f"                    cplx_t v{c}[{1 << R}];")
             if src_g or dst_g:
-                L.append(f"                    const uint64_t a0{c} = base ^ hi_tab[t0{c} >> {3 + LOW}] ^ "
-                         f"(uint64_t)((t0{c} >> 3) & {lowmask}u);")
+                L.append(f"                    const uint64_t a0{c} = base ^ hi_tab[t0{c} >> {esh + LOW}] ^ "
+                         f"(uint64_t)((t0{c} >> {esh}) & {lowmask}u);")
         for c in cos:
             if src_g:
                 if pairs and pair_in:
@@ -230,7 +239,7 @@ def group_source(plan, fp, gi, minb=3, threads=256):
                 else:
                     for j in range(1 << R):
                         L.append(f"                    {{ const uint64_t a = a0{c} ^ {_u64(G[j])}; "
-                                 f"v{c}[{j}] = (a & {_u64(in_inact)}) ? make_float2(0.f, 0.f) : __ldcg(E + a); }}")
+                                 f"v{c}[{j}] = (a & {_u64(in_inact)}) ? jit::f2((real_t)0, (real_t)0) : __ldcg(E + a); }}")
             elif pairs:
                 for j, j1 in pairs:
                     L.append(f"                    {{ const float4 q = *reinterpret_cast<const float4*>(shb + "
@@ -238,7 +247,7 @@ def group_source(plan, fp, gi, minb=3, threads=256):
                              f"v{c}[{j1}] = make_float2(q.z, q.w); }}")
             else:
                 for j, o in enumerate(offs):
-                    L.append(f"                    v{c}[{j}] = *reinterpret_cast<const float2*>(shb + {sh_off(c, o)});")
+                    L.append(f"                    v{c}[{j}] = *reinterpret_cast<const cplx_t*>(shb + {sh_off(c, o)});")
         for i in range(n):
             si = s + i
             st = fp.tile_steps[first + si]
@@ -247,7 +256,7 @@ def group_source(plan, fp, gi, minb=3, threads=256):
             dead = int(st["rdead"])
             sk, ska = int(st["sK"]) & 1, int(st["sKa"]) & 1
             k1, k2, mix = int(st["rk1"]), int(st["rk2"]), int(st["rmix"])
-            tb3 = (int(st["tbeta"]) << 3) & 0xFFFFFFFF
+            tb3 = (int(st["tbeta"]) << esh) & 0xFFFFFFFF
             for c in cos:
                 m0 = f"(((uint32_t)__popc(t0{c} & {tb3}u) ^ (csm >> {si})) & 1u) << 31"
                 args = f"(v{c}, fw[{si}], ovy[{si}] >> 1, {m0})"
@@ -270,15 +279,15 @@ def group_source(plan, fp, gi, minb=3, threads=256):
                 else:
                     for j in range(1 << R):
                         L.append(f"                    {{ const uint64_t a = a0{c} ^ {_u64(G[j])}; "
-                                 f"if (!(a & {_u64(out_inact)})) {{ const float2 q = make_float2(v{c}[{j}].x * sc, "
-                                 f"v{c}[{j}].y * sc); lm = fmaxf(lm, q.x * q.x + q.y * q.y); E[a] = q; }} }}")
+                                 f"if (!(a & {_u64(out_inact)})) {{ const cplx_t q = jit::f2(v{c}[{j}].x * sc, "
+                                 f"v{c}[{j}].y * sc); lm = jit::rmax(lm, jit::norm2(q)); E[a] = q; }} }}")
             elif pairs:
                 for j, j1 in pairs:
                     L.append(f"                    *reinterpret_cast<float4*>(shb + {sh_off(c, offs[j])}) = "
                              f"make_float4(v{c}[{j}].x, v{c}[{j}].y, v{c}[{j1}].x, v{c}[{j1}].y);")
             else:
                 for j, o in enumerate(offs):
-                    L.append(f"                    *reinterpret_cast<float2*>(shb + {sh_off(c, o)}) = v{c}[{j}];")
+                    L.append(f"                    *reinterpret_cast<cplx_t*>(shb + {sh_off(c, o)}) = v{c}[{j}];")
         L.append("                }")
         L.append("            }")
         if not direct:
@@ -303,6 +312,8 @@ def packable(fp, gi):
     run of the group has tile bit 0 in its space or among its coset zero bits."""
     g = fp.groups[gi]
     v = int(g["variant"])
+    if getattr(fp, "fp64", False):  # the packed bodies are FP32x2
+        return False
     if not (v & 2 and v & 4) or not getattr(fp, "direct_io", True) or not _direct_ok(fp, gi):
         return False
     R = 4 if v & 8 else 3
@@ -382,7 +393,7 @@ def _packed_source(fp, gi, minb):
         niter = NB2 >> 8 if NB2 > 256 else 1
         mhi = int(tr["mhi"])
         mhi3 = (mhi & (mhi - 1)) << 3  # tile bit 0 is the lane bit
-        offs = [int(tr["off"][j]) << 3 for j in range(1 << R)]
+        offs = [int(tr["off"][j]) << esh for j in range(1 << R)]
         G = [gaddr(int(tr["off"][j])) for j in range(1 << R)]
         L.append(f"        // run: steps {first + s}..{first + s + n - 1}, {NB2} coset pairs of {1 << R} entries"
                  f"{', from the table' if src_g else ''}{', to the table' if dst_g else ''}")
@@ -474,8 +485,9 @@ def plan_sources(plan, fp, minb=3, parts=8, threads=256):
     for gis, _ in units:
         if not gis:
             continue
-        src = (f"#define DCS_JIT_THREADS {threads}\n" '#include "runs_jit.cuh"\n\n' +
-               "\n".join(bodies[gi] for gi in sorted(gis)))
+        src = (f"#define DCS_JIT_THREADS {threads}\n" +
+               ("#define DCS_JIT_FP64 1\n" if getattr(fp, "fp64", False) else "") +
+               '#include "runs_jit.cuh"\n\n' + "\n".join(bodies[gi] for gi in sorted(gis)))
         out.append((src, sorted(gis)))
     return out
 
@@ -531,6 +543,11 @@ class JitPlan:
         self.minb = int(minb)
         self.threads = int(threads)
         sms = self.lib.dcs_sm_count()
+        entry = 16 if getattr(fp, "fp64", False) else 8
+        if getattr(fp, "fp64", False):
+            missing = [gi for gi in range(len(fp.groups)) if not int(fp.groups[gi]["variant"]) & 4]
+            if missing:  # the library's fused kernels store complex64 only
+                raise ValueError(f"complex128 fused plan: groups {missing} have no register runs")
         for img, gis in compile_plan(plan, fp, self.lib, minb, parts, self.threads):
             buf = ctypes.create_string_buffer(img, len(img))
             self._images.append(buf)
@@ -540,7 +557,7 @@ class JitPlan:
             for gi in gis:
                 g = fp.groups[gi]
                 td, low = int(g["tile_dim"]), int(g["low_bits"])
-                smem = 8 * (1 << (td - low)) + (8 * (1 << td) if uses_tile_buffer(fp, gi) else 0)
+                smem = 8 * (1 << (td - low)) + (entry * (1 << td) if uses_tile_buffer(fp, gi) else 0)
                 k = ctypes.c_void_p()
                 per_sm = ctypes.c_int()
                 _lib.check(self.lib.dcs_jit_kernel(handle, f"dcs_g{gi}".encode(), smem, self.threads, ctypes.byref(k),

@@ -293,16 +293,26 @@ int dcs_block_tail(double *total, int k, const uint32_t *adj_hi, const double *u
 size_t dcs_draw_scratch_bytes(int k, int nblocks);
 int dcs_draw(const double *blocks, int k, int nblocks, const double *uniforms, void *scratch,
              dcs_draw_result *results, void *stream);
+/* dcs_draw with flags.  DCS_DRAW_SEQUENTIAL: run the exact sequential FP64 CDF pass (numpy's
+ * cumsum order, otherwise run only for ties) for every block, so that cdf_lower, cdf_upper and
+ * total_cdf are numpy's values bit for bit (the reference's record rows derive
+ * actual_53bit_conditional_probability from them, production/worker.py:116).  In every mode a
+ * selected index whose compensated interval does not contain u gives DCS_E_CDF (reference:
+ * sampling_protocol.py:67-72). */
+#define DCS_DRAW_SEQUENTIAL 1u
+int dcs_draw_ex(const double *blocks, int k, int nblocks, const double *uniforms, unsigned flags, void *scratch,
+                dcs_draw_result *results, void *stream);
 
 /* Draw that allocates nothing (no counterpart in the reference; this library's addition).
  * For callers that cannot allocate device memory where they sample: code running while a
  * stream is captured, host runtimes that lend the library only their own buffers, loops where
  * an allocation would synchronise the device.  Same computation and result as dcs_draw for
- * one block, with the scratch in a fixed device array inside the library (about 8.1 MiB per
+ * one block, with the scratch in a fixed device array inside the library (about 8.4 MiB per
  * GPU that loads the library, held until the process exits).  Limit: one block of at most
  * 2^DCS_DRAW_STATIC_MAX_K amplitudes per call; larger blocks are rejected with DCS_E_ARG.
  * The first call on each device looks the array up (cudaGetSymbolAddress) with that device
- * current; make that first call before any stream capture.  All calls share the array:
+ * current; make that first call before any stream capture.  A new context on the device (after
+ * cudaDeviceReset) is noticed and the lookup redone on the next call.  All calls share the array:
  * calls that overlap on the GPU (other streams, other threads) race and must be serialised
  * by the caller.  blocks, uniform (1 double) and result are device memory. */
 #define DCS_DRAW_STATIC_MAX_K 20

@@ -1,8 +1,8 @@
 """Generate the golden fixtures under tests/golden/ by running the REFERENCE itself.
 
-Run in a container that has the reference checkout (read-only) at REFERENCE_ROOT
-(default /root/reference); the GPU machines do not, which is why the outputs
-are committed.  The reference is imported unmodified:
+Run in a container that has the reference checkout (read-only); its location is
+given by the environment variable REFERENCE_ROOT (required).  The GPU machines do
+not have it, which is why the outputs are committed.  The reference is imported unmodified:
 
 * ``qiskit`` and ``stim`` are stubbed (they are used only by circuit
   preparation, which the fixtures replace with this project's seeded ring
@@ -18,7 +18,7 @@ are committed.  The reference is imported unmodified:
 Outputs: ``<case>.json`` (inputs, reference plan, draws, meta) and
 ``<case>.npz`` (graph, unitaries, reference blocks).
 
-    python tests/golden/make_golden.py [--cases c1 small c2 c64plan]
+    REFERENCE_ROOT=<checkout> python tests/golden/make_golden.py [--cases c1 small c2 c64plan ...]
 """
 import argparse
 import json
@@ -32,7 +32,9 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 REPO = HERE.parents[1]
-REF = Path(os.environ.get("REFERENCE_ROOT", "/root/reference")) / "source"
+if not os.environ.get("REFERENCE_ROOT"):
+    raise SystemExit("set REFERENCE_ROOT to the reference checkout")
+REF = Path(os.environ["REFERENCE_ROOT"]) / "source"
 
 
 def install_reference():
@@ -62,7 +64,7 @@ install_reference()
 from conditional_block_inplace_gpu import InplaceConditionalBlockGPU  # noqa: E402
 from inplace_plan import compile_inplace, execute_inplace  # noqa: E402
 from sampling_protocol import draw_checked, make_protocol, assemble_output  # noqa: E402
-from protocol_common import actual_cdf_law_vector  # noqa: E402
+from protocol_common import actual_cdf_law_vector, make_run_protocol  # noqa: E402
 from full_vector_audit_certificate import audit_vector_pair  # noqa: E402
 from dcs_rankwidth.parity_slicing import choose_parity_slices, prefix_ranks_matrix  # noqa: E402
 from dcs_rankwidth import scan_plan  # noqa: E402
@@ -126,7 +128,9 @@ def jsonable(d):
     return out
 
 
-def make_case(name, workload, n_prefixes, n_uniforms, blocks=True, proto_seed=None):
+def make_case(name, workload, n_prefixes, n_uniforms, blocks=True, proto_seed=None, store_blocks=True):
+    """store_blocks=False keeps the reference's draws and a per-block summary (mass, selected
+    weight, weights hash) but not the blocks themselves (large blocks, many prefixes)."""
     w = build_workload(workload)
     n, openv, order, ops = w["n"], w["open_vertices"], w["order"], w["parity_operations"]
     A = w["graph"]
@@ -154,7 +158,8 @@ def make_case(name, workload, n_prefixes, n_uniforms, blocks=True, proto_seed=No
             x = np.asarray(list(map(int, r["input_data_bits"])), np.uint8)
             v, meta = eng.block(x)
             v = np.asarray(v)
-            arrays[f"block_{r['sample_id']}"] = v
+            if store_blocks:
+                arrays[f"block_{r['sample_id']}"] = v
             us = [r["draw_uniform"]] + [float(u) for u in rng.random(n_uniforms - 1)]
             for u in us:
                 d = draw_checked(v, u)
@@ -205,6 +210,27 @@ def sampler_cases():
                                "branch_uniform": r["branch_uniform"], "draw_uniform": r["draw_uniform"],
                                "input_data_bits": r["input_data_bits"]} for r in proto["records"]]
     out["assemble"] = [list(assemble_output("000000", [5, 1, 3], i, [5, 0, 4, 1, 3, 2])) for i in range(8)]
+    # a 64-qubit record with 20 free bits and a non-identity ring (a seeded permutation standing
+    # in for a device's ring order), several indices
+    p64 = make_protocol(24520, 3, 64, list(range(44, 64)))
+    ring64 = [int(q) for q in np.random.default_rng(64).permutation(64)]
+    out["assemble64"] = {"ring": ring64, "free": list(range(44, 64)), "cases": [
+        {"input_data_bits": r["input_data_bits"], "A_index": int(a),
+         "out": list(assemble_output(r["input_data_bits"], list(range(44, 64)), int(a), ring64))}
+        for r in p64["records"] for a in (0, 1, 123456, (1 << 20) - 1)]}
+    # the generation protocol records themselves (config-3 seeds, 64 qubits, 20 free bits)
+    out["protocol64"] = [{k: r[k] for k in ("sample_id", "conditional_branch", "branch_uniform", "draw_uniform",
+                                            "input_data_bits")} for r in p64["records"]]
+    # audit ids chosen before generation (production/protocol_common.py:22-31): the reference's
+    # own make_run_protocol on a small two-worker case and on the 2048-sample, 64-audit case
+    audit = []
+    for seed, aseed, count, workers, per, n_, free_ in ((7324501, 7324502, 24, 2, 2, 6, [5, 1, 3]),
+                                                       (24520, 24521, 2048, 1, 64, 64, list(range(44, 64)))):
+        rp = make_run_protocol(seed, aseed, count, workers, per, n_, free_, "fp32")
+        audit.append({"seed": seed, "audit_seed": aseed, "count": count, "workers": workers, "per_worker": per,
+                      "n": n_, "free": free_, "ids_by_worker": rp["audit"]["ids_by_worker"],
+                      "ids": rp["audit"]["ids"]})
+    out["audit_ids"] = audit
     return out
 
 
@@ -228,6 +254,11 @@ CASES = {
     "small": dict(workload="ring24_d24_t60_k10", n_prefixes=3, n_uniforms=3),
     # 40-qubit ring, depth 45, 190 T, 16 open bits (one prefix; ~2^22 tables)
     "c2": dict(workload="ring40_d45_t190_k16", n_prefixes=1, n_uniforms=4),
+    # all 256 samples of the 16-qubit workload (same protocol seed as c1: records 0-3 are c1's),
+    # one draw per sample with its own protocol uniform
+    "c1full": dict(workload="ring16_d20_t24_k8", n_prefixes=256, n_uniforms=1),
+    # 8 prefixes of the 40-qubit workload (record 0 is c2's); draws only, blocks not stored
+    "c2draws": dict(workload="ring40_d45_t190_k16", n_prefixes=8, n_uniforms=2, store_blocks=False),
     # plan only: 64-qubit ring, depth 73, 314 T, 20 open bits, two parity slices
     "c64plan": dict(workload="ring64_d73_t314_k20", n_prefixes=2, n_uniforms=0, blocks=False),
 }

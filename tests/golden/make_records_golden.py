@@ -1,7 +1,7 @@
 """Golden fixture for the production record rows, checked by the REFERENCE's own verifier.
 
-Run in a container that has the reference checkout (read-only) at REFERENCE_ROOT (default
-/root/reference).  It
+Run in a container that has the reference checkout (read-only); the environment variable
+REFERENCE_ROOT (required) gives its location.  It
 
 1. makes a synthetic production protocol for the 16-qubit ring case ``c1`` with the reference's
    ``make_run_protocol`` (source/production/protocol_common.py:18-45): 8 samples, one worker,
@@ -17,8 +17,8 @@ Run in a container that has the reference checkout (read-only) at REFERENCE_ROOT
 Outputs ``records.json`` (the protocol, the rows without their timing fields, the verdict) and
 ``records.npz`` (the sampled and reference vectors).
 
-    python tests/golden/make_records_golden.py
-    python tests/golden/make_records_golden.py --verify-artifacts DIR [--engine half]   # rows from a GPU
+    REFERENCE_ROOT=<checkout> python tests/golden/make_records_golden.py
+    REFERENCE_ROOT=<checkout> python tests/golden/make_records_golden.py --verify-artifacts DIR [--engine half]
 
 With ``--verify-artifacts``, DIR holds samples.jsonl, audits.jsonl and the vectors that
 ``records.write_rows`` wrote for the same protocol on a GPU; the script completes the

@@ -1,0 +1,146 @@
+"""Draw parity on the GPU: indices drawn from blocks this build contracts (complex64 and
+complex128) against the reference's draws from its own complex128 blocks, given the same
+uniforms; the exact sequential CDF mode; the pipelined per-sample loop."""
+import numpy as np
+import pytest
+import torch
+
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def _engine(case, arrays, dtype, mode, jit_shape=False):
+    from dcs245_classical_sampling_b200.engine import InplaceConditionalBlockGPU
+    eng = InplaceConditionalBlockGPU(arrays["graph"], arrays["unitaries"], case["n"], case["order"],
+                                     case["parity_operations"], case["open_vertices"])
+    eng.alloc(dtype=dtype, mode=mode)
+    if jit_shape:  # the bench's executor: plan-specialised register runs
+        low = 4 if eng.plan.maxslots < 16 else 3
+        grouping = "greedy" if eng.plan.maxslots < 16 else "bytes"
+        eng.set_fused_config(variant=12, low=low, grouping=grouping, jit=True)
+        assert eng.fplan.jit is not None and eng.fplan.jit.kernels
+    return eng
+
+
+def _x(rec):
+    return np.array([int(c) for c in rec["input_data_bits"]], np.uint8)
+
+
+@pytest.mark.parametrize("mode", ["device", "fused-jit"])
+@pytest.mark.parametrize("name", ["c1full", "c2draws"])
+def test_complex64_draws_match_reference_indices(golden, name, mode):
+    """Every draw of the widened fixtures (all 256 samples of the 16-qubit workload; 8 prefixes
+    of the 40-qubit one): the index drawn from this build's complex64 block equals the
+    reference's index from its complex128 block for the same uniform.  The only allowed
+    difference is a straddle: the uniform lies within the complex64 error margin of an edge of
+    the reference's CDF bin, which the draw reports as cdf_straddle."""
+    from dcs245_classical_sampling_b200.sampling import STRADDLE_MARGIN, draw_checked
+    case, arrays = golden(name)
+    eng = _engine(case, arrays, np.complex64, "fused" if mode == "fused-jit" else "device",
+                  jit_shape=mode == "fused-jit")
+    recs = {r["sample_id"]: r for r in case["protocol"]["records"]}
+    blocks = {}
+    straddles, flagged = 0, 0
+    for d in case["draws"]:
+        sid = d["sample_id"]
+        if sid not in blocks:
+            blocks[sid], _ = eng.block(_x(recs[sid]))
+            if f"block_{sid}" in arrays:
+                assert rel_l2(blocks[sid].cpu().numpy(), arrays[f"block_{sid}"]) < 1e-5
+        got = draw_checked(blocks[sid], d["uniform"], hashes=False)
+        flagged += got["cdf_straddle"]
+        if got["A_index"] != d["A_index"]:
+            assert d["uniform_to_nearest_boundary"] < STRADDLE_MARGIN, (sid, got["A_index"], d["A_index"])
+            assert got["cdf_straddle"]
+            straddles += 1
+        else:
+            assert got["cdf_lower_fsum"] == pytest.approx(d["cdf_lower_fsum"], rel=1e-4, abs=2 * STRADDLE_MARGIN)
+    print(f"{name} {mode}: {len(case['draws'])} draws, {straddles} straddles, {flagged} near a bin edge")
+
+
+@pytest.mark.parametrize("name", ["c1", "small", "c2"])
+def test_complex128_fused_blocks_match_reference(golden, name):
+    """The plan-specialised kernels compiled in FP64 (the complex128 audit executor) against the
+    reference's complex128 blocks, and their draws against the reference's draws."""
+    from dcs245_classical_sampling_b200.sampling import draw_checked
+    case, arrays = golden(name)
+    eng = _engine(case, arrays, np.complex128, "fused")
+    assert eng.fplan.fp64 and eng.fplan.jit is not None and eng.fplan.jit.kernels
+    for rec in case["protocol"]["records"]:
+        v, meta = eng.block(_x(rec))
+        assert meta["prefix_dtype"] == "complex128"
+        assert rel_l2(v.cpu().numpy(), arrays[f"block_{rec['sample_id']}"]) < 1e-13
+        for d in case["draws"]:
+            if d["sample_id"] == rec["sample_id"]:
+                assert draw_checked(v, d["uniform"], hashes=False)["A_index"] == d["A_index"]
+
+
+def test_complex128_fused_rejects_library_kernels(golden):
+    case, arrays = golden("c1")
+    eng = _engine(case, arrays, np.complex128, "fused")
+    with pytest.raises(ValueError):
+        eng.set_fused_config(jit=False)
+
+
+@pytest.mark.parametrize("name", ["c1full", "small", "c2"])
+def test_exact_cdf_mode_is_numpy_bit_for_bit(golden, name):
+    """exact_cdf=True: NumPy's sequential CDF values, bit for bit, for every golden draw (the
+    default mode reports the compensated values where it certified the index)."""
+    from dcs245_classical_sampling_b200.sampling import draw_checked
+    case, arrays = golden(name)
+    for d in case["draws"]:
+        v = torch.from_numpy(arrays[f"block_{d['sample_id']}"]).cuda()
+        got = draw_checked(v, d["uniform"], hashes=False, exact_cdf=True)
+        assert got["A_index"] == d["A_index"]
+        for key in ("cdf_lower_numpy", "cdf_upper_numpy", "scaled_mass_cdf", "selected_scaled_weight"):
+            assert got[key] == d[key], key
+        for key in ("cdf_lower_fsum", "cdf_upper_fsum", "scaled_mass_fsum"):
+            assert got[key] == pytest.approx(d[key], rel=4e-16, abs=1e-300), key
+
+
+def test_exact_cdf_mode_on_ties_and_edges():
+    """Uniforms on and next to float64 CDF edges of a 2^12 block: the exact mode gives NumPy's
+    index and values where the reference accepts the draw, and the reference's error where its
+    independent interval check rejects it."""
+    from dcs245_classical_sampling_b200.sampling import draw_checked
+    from oracle import sampler_ref
+    rng = np.random.default_rng(11)
+    v = rng.normal(size=1 << 12) + 1j * rng.normal(size=1 << 12)
+    w = v.real * v.real + v.imag * v.imag
+    cdf = np.cumsum(w) / np.cumsum(w)[-1]
+    for i in (0, 31, 32, 33, 2047, 4094):
+        for u in (float(cdf[i]), float(np.nextafter(cdf[i], 0)), float(np.nextafter(cdf[i], 1))):
+            if not 0 <= u < 1:
+                continue
+            try:
+                want = sampler_ref.draw(v, u)
+            except ArithmeticError:
+                with pytest.raises(ArithmeticError):
+                    draw_checked(v, u, exact_cdf=True)
+                continue
+            got = draw_checked(v, u, exact_cdf=True)
+            assert got["A_index"] == want["A_index"]
+            for key in ("cdf_lower_numpy", "cdf_upper_numpy", "scaled_mass_cdf"):
+                assert got[key] == want[key], key
+
+
+def test_sample_checked_equals_block_and_draw(golden):
+    """The pipelined per-sample loop gives, sample by sample, the records of engine.block +
+    draw_checked (hashes included), and the same host blocks."""
+    from dcs245_classical_sampling_b200.sampling import draw_checked, sample_checked
+    case, arrays = golden("c1full")
+    eng = _engine(case, arrays, np.complex64, "fused", jit_shape=True)
+    recs = case["protocol"]["records"][:12]
+    xs = [_x(r) for r in recs]
+    us = [r["draw_uniform"] for r in recs]
+    got, host = sample_checked(eng, xs, us, hashes=True, exact_cdf=True, keep_host_blocks=True)
+    assert len(got) == len(xs) == len(host)
+    for x, u, g, h in zip(xs, us, got, host):
+        v, _ = eng.block(x)
+        want = draw_checked(v, u, hashes=True, exact_cdf=True)
+        assert g == want
+        assert np.array_equal(h, v.cpu().numpy())
+    assert sample_checked(eng, [], []) == []
+    with pytest.raises(ValueError):
+        sample_checked(eng, xs[:1], [1.0])

@@ -32,3 +32,22 @@ def test_c_port_matches_numpy_oracle(golden, name):
             assert not np.any(E[term])
         else:
             assert rel_l2(E[term] * math.exp(ls), want * math.exp(wls)) < 1e-13
+
+
+@pytest.mark.parametrize("name", ["c1", "small"])
+def test_cpu_sampler_blocks_and_draws_match_reference(golden, name):
+    """The CPU comparator of the small workloads (complete samples with the C executor) against
+    the reference's complex128 blocks and draws."""
+    from oracle import block_ref
+    from oracle.c import CpuSampler
+    case, arrays = golden(name)
+    eng = block_ref.OracleEngine(arrays["graph"], arrays["unitaries"], case["n"], case["order"],
+                                 case["parity_operations"], case["open_vertices"])
+    cs = CpuSampler(eng)
+    recs = {r["sample_id"]: r for r in case["protocol"]["records"]}
+    for sid, rec in recs.items():
+        x = np.array([int(c) for c in rec["input_data_bits"]], np.uint8)
+        assert rel_l2(cs.block(x), arrays[f"block_{sid}"]) < 1e-13
+    for d in case["draws"]:
+        x = np.array([int(c) for c in recs[d["sample_id"]]["input_data_bits"]], np.uint8)
+        assert cs.sample(x, d["uniform"])["A_index"] == d["A_index"]

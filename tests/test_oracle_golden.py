@@ -65,6 +65,41 @@ def test_oracle_draws_match_reference(golden, name):
         assert qiskit == d["bitstring_qiskit"]
 
 
+def test_oracle_matches_reference_on_all_config1_samples(golden):
+    """All 256 samples of the 16-qubit workload (c1full): the oracle's complex128 blocks and its
+    draws equal the reference's, with every CDF field bit for bit."""
+    case, arrays = golden("c1full")
+    eng = _engine(case, arrays)
+    recs = case["protocol"]["records"]
+    assert len(recs) == 256 and len(case["draws"]) == 256
+    for rec, d in zip(recs, case["draws"]):
+        x = np.array([int(c) for c in rec["input_data_bits"]], np.uint8)
+        got, _ = eng.block(x)
+        assert rel_l2(got, arrays[f"block_{rec['sample_id']}"]) < 1e-13
+        dr = sampler_ref.draw(arrays[f"block_{rec['sample_id']}"], d["uniform"])
+        assert d["uniform"] == rec["draw_uniform"]
+        for key in ("A_index", "cdf_lower_numpy", "cdf_upper_numpy", "cdf_lower_fsum", "cdf_upper_fsum",
+                    "uniform_to_nearest_boundary"):
+            assert dr[key] == d[key], key
+
+
+def test_widened_fixtures_share_the_smaller_cases_prefixes(golden):
+    """c1full and c2draws extend c1 and c2 with the same protocol seed: their first records are the
+    smaller cases' records, and their draws of those prefixes are the same."""
+    for small, big in (("c1", "c1full"), ("c2", "c2draws")):
+        a, _ = golden(small)
+        b, _ = golden(big)
+        ra, rb = a["protocol"]["records"], b["protocol"]["records"]
+        assert rb[: len(ra)] == ra
+        first = {d["sample_id"]: d for d in a["draws"] if d["uniform"] == ra[d["sample_id"]]["draw_uniform"]}
+        for d in b["draws"]:
+            if d["sample_id"] in first and d["uniform"] == first[d["sample_id"]]["uniform"]:
+                assert d["A_index"] == first[d["sample_id"]]["A_index"]
+                assert d["weights_sha256"] == first[d["sample_id"]]["weights_sha256"]
+    c2d, _ = golden("c2draws")
+    assert len(c2d["protocol"]["records"]) == 8
+
+
 def test_oracle_sampler_known_answers(golden):
     s, _ = golden("sampler")
     for c in s["selftest"]:
