@@ -65,9 +65,15 @@ def parse():
     ap.add_argument("--tune", action="store_true", help="autotune the fused tile shape before timing")
     ap.add_argument("--no-jit", action="store_true",
                     help="run the library's register-run kernel instead of the plan-specialised group kernels")
+    ap.add_argument("--prefetch-kb", type=int, default=None,
+                    help="generated kernels: KiB per CTA staging the next tile's first-run entries "
+                         "(default: the tuned configuration)")
     ap.add_argument("--serve", action="store_true", help="run the serving mix (32q/48q/64q) instead")
-    ap.add_argument("--serve-seconds", type=float, default=20.0, help="arrival window of the serving run")
+    ap.add_argument("--serve-seconds", type=float, default=12.0, help="arrival window of the serving run")
     ap.add_argument("--serve-rate", type=float, default=1.0, help="Poisson request rate (1/s)")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving mix in the default run")
+    ap.add_argument("--plain-64q-seconds", type=float, default=None,
+                    help="serving comparator: per-sample plain-path time of the 64q circuit (default: measured)")
     ap.add_argument("--serve-max-samples", type=int, default=64)
     ap.add_argument("--hbm-budget-gib", type=float, default=170.0)
     ap.add_argument("--graphs", action="store_true",
@@ -285,8 +291,8 @@ def gpu_arm(args):
 
     from dcs245_classical_sampling_b200 import _lib
     from dcs245_classical_sampling_b200.engine import InplaceConditionalBlockGPU
-    from dcs245_classical_sampling_b200.sampling import (STRADDLE_MARGIN, draw_many, make_audit_ids, make_protocol,
-                                                         sample_checked)
+    from dcs245_classical_sampling_b200.sampling import (draw_many, make_audit_ids, make_protocol, sample_checked,
+                                                         straddle_margin)
     from dcs245_classical_sampling_b200.workloads import build_workload
 
     w = build_workload(args.workload)
@@ -299,6 +305,8 @@ def gpu_arm(args):
         tune_report = eng.autotune(jit=not args.no_jit)
     if args.mode == "fused" and eng.fplan.tile_runs is not None and eng.jit == args.no_jit:
         eng.set_fused_config(jit=not args.no_jit)  # plan-specialised group kernels (NVRTC, cached cubins)
+    if args.mode == "fused" and args.prefetch_kb is not None:
+        eng.set_fused_config(prefetch_kb=args.prefetch_kb)
     setup_s = time.perf_counter() - t0
     k = eng.k
     total = args.warmup + args.steps
@@ -441,6 +449,12 @@ def gpu_arm(args):
     if rank == 0 and world == 1 and not args.no_configs:
         configs = gpu_small_configs(args, local)
 
+    serve = None
+    if rank == 0 and world == 1 and not args.no_serve and args.workload == "ring64_d73_t314_k20":
+        if plain is not None:
+            args.plain_64q_seconds = 1.0 / plain["value"]
+        serve = run_serving(args, local)
+
     if rank == 0:
         peak, how = peaks()
         cb = None
@@ -453,8 +467,8 @@ def gpu_arm(args):
                     configs[name]["gpu_over_cpu"] = configs[name]["value"] / c["value"]
                     configs[name]["e2e_over_cpu"] = configs[name]["e2e"]["value"] / c["value"]
         ach = dom["alg_bytes_per_launch"] / dom["avg_launch_s"] / 1e9
-        near = [bool(min(d["uniform"] - d["cdf_lower_exact"], d["cdf_upper_exact"] - d["uniform"]) < STRADDLE_MARGIN)
-                for d in draws[args.warmup:total]]
+        near = [bool(min(d["uniform"] - d["cdf_lower_exact"], d["cdf_upper_exact"] - d["uniform"])
+                     < straddle_margin(float(d["weight_l2"]))) for d in draws[args.warmup:total]]
         line = {"metric": METRIC, "value": value, "unit": "samples/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": 1000.0 * elapsed / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f16 storage, f64 arithmetic" if args.storage else "c64",
@@ -489,10 +503,11 @@ def gpu_arm(args):
                 "draws": {"indices": [int(d["index"]) for d in draws[args.warmup:total]],
                           "ties": int(sum(int(d["tie"]) for d in draws[args.warmup:total])),
                           "near_cdf_edge": int(sum(near)),
-                          "near_cdf_edge_margin": STRADDLE_MARGIN,
+                          "near_cdf_edge_margin": "sampling.straddle_margin: 6 sigma of the CDF shift of a block "
+                                                  "at relative L2 1e-5 with independent per-entry errors",
                           "straddles_audited": audit["straddles"] if audit else None},
                 "clocks": clk, "setup_s": setup_s, "cpu_baseline": cb, "audit": audit,
-                "configs": configs,
+                "configs": configs, "serve": serve,
                 "fused_config": fused_cfg,
                 "autotune": tune_report}
         print(json.dumps(line), flush=True)
@@ -513,7 +528,7 @@ def run_audit(args, a64, local):
     import torch
     from dcs245_classical_sampling_b200.audit import audit_vector_pair, relative_l2
     from dcs245_classical_sampling_b200.engine import InplaceConditionalBlockGPU
-    from dcs245_classical_sampling_b200.sampling import STRADDLE_MARGIN, draw_many
+    from dcs245_classical_sampling_b200.sampling import CDF_SHIFT_BOUND, draw_many
     from dcs245_classical_sampling_b200.workloads import WORKLOADS, build_workload
     gc.collect()
     torch.cuda.empty_cache()
@@ -538,7 +553,7 @@ def run_audit(args, a64, local):
         if i64 != i128:
             straddles += 1
             near = min(d64["uniform"] - d64["cdf_lower_exact"], d64["cdf_upper_exact"] - d64["uniform"])
-            bad += int(not near < STRADDLE_MARGIN)
+            bad += int(not near < CDF_SHIFT_BOUND)
         rows.append([int(sid), rec["normalized_conditional_overlap_abs"], relative_l2(v, ap), i64, i128])
     rmax = ref.inplace_rmax
     del ref
@@ -686,36 +701,48 @@ def kernel_roofline(eng, prep, out, stream):
             "launch_ms": [a.elapsed_time(b) for a, b, _ in evs], "launch_bytes": [x for _, _, x in evs]}
 
 
-def serve_arm(args):
-    """Serving mix: Poisson requests against three circuits, continuous batching, p50/p99."""
+SERVE_MIX = {"ring32_d37_t79_k14": 50, "ring48_d55_t177_k17": 30, "ring64_d73_t314_k20": 20}
+
+
+def run_serving(args, local):
+    """Serving mix: Poisson requests against the three circuits (32q 2^14, 48q 2^17, 64q 2^20 blocks;
+    50/30/20 by request count, 1-64 samples each), continuous batching with round-robin batches,
+    and admission by HBM budget (one table pool granted per batch; graphs=True keeps fixed
+    per-runner tables instead, captured as CUDA graphs).  Compared with plain per-request
+    execution: every request alone, in arrival order, one sample at a time on the plain path (one
+    launch and one host read per vertex step), whose per-sample times are measured here."""
+    import gc
     import torch
-    from dcs245_classical_sampling_b200.serve import CircuitRunner, Server, latency_stats, poisson_requests
+    from dcs245_classical_sampling_b200.engine import InplaceConditionalBlockGPU
+    from dcs245_classical_sampling_b200.sampling import draw_checked, make_protocol
+    from dcs245_classical_sampling_b200.serve import (CircuitRunner, Request, Server, TablePool, latency_stats,
+                                                      poisson_requests)
     from dcs245_classical_sampling_b200.workloads import build_workload
-    rank, world, local = dist_init()
-    torch.cuda.set_device(local)
-    mix = {"ring32_d37_t79_k14": 50, "ring48_d55_t177_k17": 30, "ring64_d73_t314_k20": 20}
-    budget = args.hbm_budget_gib * 2 ** 30
+    dev = torch.device("cuda", local)
+    gc.collect()
+    torch.cuda.empty_cache()
+    budget = int(args.hbm_budget_gib * 2 ** 30)
     t0 = time.perf_counter()
+    pool = None if args.graphs else TablePool(budget, dev)
     runners = {}
-    big = CircuitRunner("ring64_d73_t314_k20", build_workload("ring64_d73_t314_k20"), key=args.seed + 64,
-                        max_samples=1, device=local)
-    runners[big.name] = big
-    left = budget - big.table_bytes()
-    for name, share in (("ring48_d55_t177_k17", 0.8), ("ring32_d37_t79_k14", 0.2)):
-        runners[name] = CircuitRunner(name, build_workload(name), key=args.seed + len(runners), max_samples=64,
-                                      device=local, hbm_budget=left * share, graphs=args.graphs)
+    for i, name in enumerate(SERVE_MIX):
+        w = build_workload(name)
+        big = name.startswith("ring64")
+        kw = {"pool": pool} if pool is not None else (
+            {} if big else {"hbm_budget": (budget - (8 << 34)) * (0.8 if name.startswith("ring48") else 0.2),
+                            "graphs": True})
+        runners[name] = CircuitRunner(name, w, key=args.seed + 64 + i, max_samples=1 if big else 64,
+                                      device=local, **kw)
     for r in runners.values():  # every batch size captured before the arrivals start
         r.precapture(range(1, r.max_samples + 1))
     setup = time.perf_counter() - t0
-    # warm every runner once
-    from dcs245_classical_sampling_b200.serve import Request
-    Server(runners).run([Request(10 ** 6 + i, c, 1, 0.0) for i, c in enumerate(runners)], realtime=False)
-    reqs = poisson_requests(args.serve_rate, args.serve_seconds, mix, seed=args.seed,
+    Server(runners, pool).run([Request(10 ** 6 + i, c, 1, 0.0) for i, c in enumerate(runners)], realtime=False)
+    reqs = poisson_requests(args.serve_rate, args.serve_seconds, SERVE_MIX, seed=args.seed,
                             max_samples=args.serve_max_samples)
     clocks = ClockSampler(local)
     clocks.start()
     ta = time.perf_counter()
-    done = Server(runners).run(reqs, realtime=True)
+    done = Server(runners, pool).run(reqs, realtime=True)
     span = time.perf_counter() - ta
     clk = clocks.stop()
     per = {}
@@ -730,15 +757,71 @@ def serve_arm(args):
     tot = sum(r.nsamples for r in done)
     ties = sum(int(rec["tie"]) for r in done for rec, _ in r.records.values())
     bad = sum(int(rec["status"] != 0) for r in done for rec, _ in r.records.values())
-    line = {"metric": "serving mix: samples/s and request p50/p99 ms (32q 2^14, 48q 2^17, 64q 2^20; 50/30/20)",
-            "value": tot / span, "unit": "samples/s", "n_gpus": 1, "higher_is_better": True,
+    slots = {c: {"samples_per_launch": r.max_samples, "table_item_gib": r.item_bytes / 2 ** 30, "mode": r.mode}
+             for c, r in runners.items()}
+    pool_free_after = None if pool is None else pool.free == [(0, pool.nbytes)]
+    del runners, pool
+    gc.collect()
+    torch.cuda.empty_cache()
+    # plain per-request execution: measured per-sample times of the plain path per circuit
+    plain_s = {}
+    for name in SERVE_MIX:
+        if name.startswith("ring64") and args.plain_64q_seconds:
+            plain_s[name] = args.plain_64q_seconds
+            continue
+        w = build_workload(name)
+        eng = InplaceConditionalBlockGPU(w["graph"], w["unitaries"], w["n"], w["order"], w["parity_operations"],
+                                         w["open_vertices"])
+        eng.alloc(np.complex64, device=local, mode="plain")
+        recs = make_protocol(args.seed, 4, w["n"], w["open_vertices"])["records"]
+        xs = [np.array([int(c) for c in r["input_data_bits"]], np.uint8) for r in recs]
+        v, _ = eng.block(xs[0])
+        n = 1 if name.startswith("ring64") else 3
+        tp = time.perf_counter()
+        for i in range(n):
+            v, _ = eng.block(xs[1 + i])
+            draw_checked(v, recs[1 + i]["draw_uniform"], hashes=False)
+        plain_s[name] = (time.perf_counter() - tp) / n
+        del eng
+        gc.collect()
+        torch.cuda.empty_cache()
+    # the same arrivals served one request at a time, first come first served (a single queue)
+    tfree, plain_lat = 0.0, []
+    for r in sorted(reqs, key=lambda q: q.arrival):
+        start = max(tfree, r.arrival)
+        tfree = start + r.nsamples * plain_s[r.circuit]
+        plain_lat.append((tfree - r.arrival) * 1e3)
+    plain_span = tfree - min(r.arrival for r in reqs) if reqs else 0.0
+    plain_busy = sum(r.nsamples * plain_s[r.circuit] for r in reqs)
+    return {"metric": "serving mix: samples/s and request p50/p99 ms (32q 2^14, 48q 2^17, 64q 2^20; 50/30/20)",
+            "value": tot / span, "unit": "samples/s", "higher_is_better": True,
             "latency": latency_stats(done), "per_circuit": per, "requests": len(done), "samples": tot,
             "span_s": span, "arrival_window_s": args.serve_seconds, "rate_hz": args.serve_rate,
             "hbm_budget_gib": args.hbm_budget_gib,
-            "slots": {c: {"samples_per_launch": r.max_samples, "table_items": r.engine.items,
-                          "table_gib": r.table_bytes() / 2 ** 30, "mode": r.mode} for c, r in runners.items()},
-            "ties": ties, "failed_draws": bad, "cuda_graphs": bool(args.graphs), "setup_s": setup, "clocks": clk,
+            "admission": "per-batch table grants from one HBM pool" if not args.graphs else
+                         "fixed per-runner tables (CUDA graphs)",
+            "pool_returned_every_region": pool_free_after,
+            "slots": slots, "ties": ties, "failed_draws": bad, "cuda_graphs": bool(args.graphs), "setup_s": setup,
+            "clocks": clk,
+            "plain_per_request": {
+                "seconds_per_sample": plain_s,
+                "value": tot / plain_busy if plain_busy else None, "unit": "samples/s",
+                "p50_ms": float(np.percentile(plain_lat, 50)) if plain_lat else None,
+                "p99_ms": float(np.percentile(plain_lat, 99)) if plain_lat else None,
+                "span_s": plain_span,
+                "how": "measured per-sample plain-path times; requests served alone in arrival order "
+                       "(single FIFO queue computed from those times)"},
+            "speedup_vs_plain": (tot / span) / (tot / plain_busy) if plain_busy else None,
             "data": "synthetic (seeded ring circuits, Philox4x32-10 prefixes and uniforms on the device)"}
+
+
+def serve_arm(args):
+    """`bench.py --serve`: the serving mix alone, as its own JSON line."""
+    import torch
+    rank, world, local = dist_init()
+    torch.cuda.set_device(local)
+    line = run_serving(args, local)
+    line["n_gpus"] = 1
     print(json.dumps(line), flush=True)
 
 
@@ -773,6 +856,10 @@ def profile_case(argv):
     ap.add_argument("--jit", action="store_true", help="plan-specialised group kernels (register-run variants)")
     ap.add_argument("--grouping", default="greedy", choices=["greedy", "bytes"],
                     help="fused groups: greedy spans or fewest table bytes")
+    ap.add_argument("--prefetch-kb", type=int, default=0,
+                    help="generated kernels: KiB per CTA staging the next tile's first-run entries")
+    ap.add_argument("--minb", type=int, default=None, help="generated kernels: CTAs per SM for the registers")
+    ap.add_argument("--fp64", action="store_true", help="complex128 table, FP64 generated kernels (the audits)")
     ap.add_argument("--storage", default=None, choices=["float16"],
                     help="binary16 tables with FP64 arithmetic (device mode)")
     a = ap.parse_args(argv)
@@ -797,26 +884,28 @@ def profile_case(argv):
     half = a.storage == "float16"
     if half and a.mode != "device":
         raise SystemExit("--storage float16 takes --mode device")
-    entry = 4 if half else 8
+    if a.fp64 and (a.mode != "fused" or not a.jit or half):
+        raise SystemExit("--fp64 takes --mode fused --jit (the complex128 generated kernels)")
+    entry = 4 if half else (16 if a.fp64 else 8)
     if half:
-        table = torch.empty(2 << a.max_slots, dtype=torch.float16, device=dev)
+        table = torch.zeros(2 << a.max_slots, dtype=torch.float16, device=dev)
     else:
-        table = torch.empty(1 << a.max_slots, dtype=torch.complex64, device=dev)
+        table = torch.zeros(1 << a.max_slots, dtype=torch.complex128 if a.fp64 else torch.complex64, device=dev)
     stream = torch.cuda.current_stream(dev)
     sub = P.BlockPlan(**{**bp.__dict__, "steps": steps})
     if a.mode == "fused":
         fp = build_fused_plan(sub, max_dim=a.max_dim, low=a.low, variant=a.variant, pairs=a.pairs,
-                              grouping=a.grouping)
+                              grouping=a.grouping, fp64=a.fp64, prefetch_kb=a.prefetch_kb)
         if a.jit:
             from dcs245_classical_sampling_b200.jit import JitPlan
-            fp.jit = JitPlan(sub, fp, lib)
+            fp.jit = JitPlan(sub, fp, lib, minb=a.minb)
         nmax = len(fp.groups)
     else:
         dsteps = device_steps(steps)
         nmax = last
     maxbits = torch.zeros(nmax + 1, dtype=torch.int64, device=dev)
     scale = torch.zeros(_lib.SCALE_DTYPE.itemsize // 8, dtype=torch.int64, device=dev)
-    one = (int(np.array([1.0], np.float64).view(np.int64)[0]) if half
+    one = (int(np.array([1.0], np.float64).view(np.int64)[0]) if half or a.fp64
            else int(np.array([1.0], np.float32).view(np.uint32)[0]))
     per_launch = []
     for it in range(a.iters):
@@ -836,7 +925,7 @@ def profile_case(argv):
                 _lib.check(fp.launch(lib, _lib.ptr(table), _lib.ptr(params), g, 1, _lib.ptr(maxbits),
                                      _lib.ptr(scale), stream.cuda_stream))
                 first, count = fp.spans[g]
-                alg = ((1 << len(steps[first].active_in)) + (1 << len(steps[first + count - 1].active_out))) * 8
+                alg = ((1 << len(steps[first].active_in)) + (1 << len(steps[first + count - 1].active_out))) * entry
             else:
                 _lib.check(lib.dcs_slice_steps(_lib.H16 if half else _lib.C64, _lib.ptr(table), dsteps.ctypes.data,
                                                _lib.ptr(params), last, g, 1, _lib.ptr(maxbits), _lib.ptr(scale),
@@ -850,7 +939,10 @@ def profile_case(argv):
     tot_ms = sum(t for t, _ in per_launch)
     tot_b = sum(b for _, b in per_launch)
     big = [(t, b) for t, b in per_launch if b >= (1 << 27) * entry]
-    print(json.dumps({"mode": a.mode, "storage": a.storage or "complex64", "steps": last, "launches": len(per_launch), "total_ms": tot_ms,
+    # integer sum of the table's words: equal for variants that compute the same values bit for bit
+    checksum = int(torch.sum(table.view(torch.int32), dtype=torch.int64).item())
+    print(json.dumps({"mode": a.mode, "storage": a.storage or ("complex128" if a.fp64 else "complex64"),
+                      "prefetch_kb": a.prefetch_kb, "checksum": checksum, "steps": last, "launches": len(per_launch), "total_ms": tot_ms,
                       "alg_gb": tot_b / 1e9, "alg_gbs": tot_b / tot_ms / 1e6,
                       "big_launch_gbs": (sum(b for _, b in big) / sum(t for t, _ in big) / 1e6) if big else None,
                       "per_launch_ms": [round(t, 3) for t, _ in per_launch]}))

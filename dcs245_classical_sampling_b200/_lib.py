@@ -45,7 +45,7 @@ TILE_RUN_DTYPE = np.dtype([("nins", "<u1"), ("count", "<u1"), ("r", "<u1"), ("pa
 DRAW_DTYPE = np.dtype([
     ("index", "<i8"), ("tie", "<i4"), ("status", "<i4"), ("total_cdf", "<f8"), ("total_exact", "<f8"),
     ("selected_weight", "<f8"), ("cdf_lower", "<f8"), ("cdf_upper", "<f8"), ("cdf_lower_exact", "<f8"),
-    ("cdf_upper_exact", "<f8"), ("uniform", "<f8"), ("tv53", "<f8"),
+    ("cdf_upper_exact", "<f8"), ("uniform", "<f8"), ("tv53", "<f8"), ("weight_l2", "<f8"),
 ])
 STRUCTS = [STEP_DTYPE, PARAM_DTYPE, SCALE_DTYPE, GROUP_DTYPE, TILE_STEP_DTYPE, DRAW_DTYPE, TILE_RUN_DTYPE]
 

@@ -80,7 +80,7 @@ __host__ __device__ constexpr size_t seq_groups(size_t n) { return (n + 31) >> k
 
 // layout of the scratch area
 struct Layout {
-    size_t w, chunk_sum, state, tv_part, ckpt, bytes;
+    size_t w, chunk_sum, state, tv_part, sq_part, ckpt, bytes;
 };
 __host__ __device__ constexpr Layout layout(int k, int nblocks) {
     const size_t n = (size_t)1 << k;
@@ -90,7 +90,8 @@ __host__ __device__ constexpr Layout layout(int k, int nblocks) {
     L.chunk_sum = L.w + n * nblocks * sizeof(double);
     L.state = L.chunk_sum + nch * nblocks * sizeof(dd);
     L.tv_part = L.state + nblocks * sizeof(BlockState);
-    L.ckpt = L.tv_part + nch * nblocks * sizeof(double);
+    L.sq_part = L.tv_part + nch * nblocks * sizeof(double);
+    L.ckpt = L.sq_part + nch * nblocks * sizeof(double);
     L.bytes = L.ckpt + seq_groups(n) * nblocks * sizeof(double);
     L.bytes = (L.bytes + 255) & ~(size_t)255;
     return L;
@@ -351,10 +352,12 @@ k_sequential(const double* __restrict__ w, int k, const dd* __restrict__ chunk_s
     else if (!(r.cdf_lower_exact <= u && u < r.cdf_upper_exact)) r.status = DCS_E_CDF;
 }
 
-// 5. 53-bit grid TV, per chunk partial sums (deterministic final sum in k_tv_final)
+// 5. 53-bit grid TV and the sum of squared weights, per chunk partial sums (deterministic final
+//    sums in k_tv_final)
 __global__ void __launch_bounds__(kThreads)
 k_tv(const double* __restrict__ w, int k, const dd* __restrict__ chunk_sum, int nch,
-     const BlockState* __restrict__ state, const dcs_draw_result* __restrict__ res, double* __restrict__ part) {
+     const BlockState* __restrict__ state, const dcs_draw_result* __restrict__ res, double* __restrict__ part,
+     double* __restrict__ sq_part) {
     const int b = blockIdx.y;
     const int c = blockIdx.x;
     const uint64_t n = 1ull << k;
@@ -386,7 +389,7 @@ k_tv(const double* __restrict__ w, int k, const dd* __restrict__ chunk_sum, int 
     const double two53 = 9007199254740992.0;
     double prev_end = ceil(dd_div(run, T) * two53);
     if (start + (uint64_t)threadIdx.x * kPer == 0) prev_end = 0.0;
-    double s = 0.0;
+    double s = 0.0, q = 0.0;
     for (int j = 0; j < kPer; ++j) {
         const uint64_t i = start + (uint64_t)threadIdx.x * kPer + j;
         if (i >= n) break;
@@ -394,20 +397,30 @@ k_tv(const double* __restrict__ w, int k, const dd* __restrict__ chunk_sum, int 
         const double ci = (i == n - 1) ? 1.0 : dd_div(run, T);
         const double end = ceil(ci * two53);
         s += fabs((end - prev_end) / two53 - loc[j] / mass);
+        const double p = loc[j] / mass;
+        q = fma(p, p, q);
         prev_end = end;
     }
     const dd tot = block_sum_dd(dd{s, 0.0});
-    if (threadIdx.x == 0) part[(uint64_t)b * nch + c] = tot.hi + tot.lo;
+    const dd sq = block_sum_dd(dd{q, 0.0});
+    if (threadIdx.x == 0) {
+        part[(uint64_t)b * nch + c] = tot.hi + tot.lo;
+        sq_part[(uint64_t)b * nch + c] = sq.hi + sq.lo;
+    }
 }
 
-__global__ void k_tv_final(const double* __restrict__ part, int nch, const BlockState* __restrict__ state,
-                           dcs_draw_result* __restrict__ res, int nblocks) {
+__global__ void k_tv_final(const double* __restrict__ part, const double* __restrict__ sq_part, int nch,
+                           const BlockState* __restrict__ state, dcs_draw_result* __restrict__ res, int nblocks) {
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= nblocks) return;
     if (state[b].status) { res[b].status = state[b].status; return; }
-    double s = 0.0;
-    for (int c = 0; c < nch; ++c) s += part[(uint64_t)b * nch + c];
+    double s = 0.0, q = 0.0;
+    for (int c = 0; c < nch; ++c) {
+        s += part[(uint64_t)b * nch + c];
+        q += sq_part[(uint64_t)b * nch + c];
+    }
     res[b].tv53 = 0.5 * s;
+    res[b].weight_l2 = q;
 }
 
 // ---------------------------------------------------------------- audit overlap
@@ -458,6 +471,7 @@ int enqueue_draw(const double* blocks, int k, int nblocks, const double* uniform
     dd* cs = (dd*)(base + L.chunk_sum);
     BlockState* st = (BlockState*)(base + L.state);
     double* part = (double*)(base + L.tv_part);
+    double* sq = (double*)(base + L.sq_part);
     double* ck = (double*)(base + L.ckpt);
     const uint64_t n = 1ull << k;
     const int nch = (int)(n >= (uint64_t)kChunk ? n / kChunk : 1);
@@ -472,9 +486,9 @@ int enqueue_draw(const double* blocks, int k, int nblocks, const double* uniform
     DCS_CHECK_LAUNCH("k_locate_elem");
     k_sequential<<<nblocks, 32, 0, s>>>(w, k, cs, nch, st, results, ck, (flags & DCS_DRAW_SEQUENTIAL) ? 1 : 0);
     DCS_CHECK_LAUNCH("k_sequential");
-    k_tv<<<dim3(nch, nblocks), kThreads, 0, s>>>(w, k, cs, nch, st, results, part);
+    k_tv<<<dim3(nch, nblocks), kThreads, 0, s>>>(w, k, cs, nch, st, results, part, sq);
     DCS_CHECK_LAUNCH("k_tv");
-    k_tv_final<<<(nblocks + 31) / 32, 32, 0, s>>>(part, nch, st, results, nblocks);
+    k_tv_final<<<(nblocks + 31) / 32, 32, 0, s>>>(part, sq, nch, st, results, nblocks);
     DCS_CHECK_LAUNCH("k_tv_final");
     return DCS_OK;
 }

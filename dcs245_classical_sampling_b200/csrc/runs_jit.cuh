@@ -349,7 +349,8 @@ __device__ __forceinline__ wts_t unit_weights(const jit_param& p, bool fixed) {
 // Pass scale 2^-e from the previous pass's max and the group's step factors (block 0 records
 // both), the unit step weights into shared memory, and the table of high tile-coordinate
 // addresses.  FIXMASK bit i: step FIRST + i is a fixed kind.
-template <int TD, int LOW, int COUNT, int FIRST, uint32_t FIXMASK>
+// FILL_HI: fill hi_tab (false when the kernel keeps the split tables of fill_hi_split instead).
+template <int TD, int LOW, int COUNT, int FIRST, uint32_t FIXMASK, bool FILL_HI = true>
 __device__ __forceinline__ real_t prologue(const jit_param* __restrict__ params, const uint64_t* basis,
                                            const unsigned long long* maxbits, int group, jit_scale* scale,
                                            wts_t* fw, int* ovy, uint64_t* hi_tab) {
@@ -377,16 +378,46 @@ __device__ __forceinline__ real_t prologue(const jit_param* __restrict__ params,
         fw[threadIdx.x] = unit_weights(p, (FIXMASK >> threadIdx.x) & 1u);
         ovy[threadIdx.x] = (p.ov & 1) | ((p.y & 1) << 1);
     }
-    for (int h = threadIdx.x; h < (1 << (TD - LOW)); h += kThreads) {
-        uint64_t a = 0;
+    if constexpr (FILL_HI) {
+        for (int h = threadIdx.x; h < (1 << (TD - LOW)); h += kThreads) {
+            uint64_t a = 0;
 #pragma unroll
-        for (int i = 0; i < TD - LOW; ++i)
-            if ((h >> i) & 1) a ^= basis[i];
-        hi_tab[h] = a;
+            for (int i = 0; i < TD - LOW; ++i)
+                if ((h >> i) & 1) a ^= basis[i];
+            hi_tab[h] = a;
+        }
     }
     __syncthreads();
     return (real_t)ldexp(1.0, -e);
 }
+
+// The table of high tile-coordinate addresses split in two (2^A + 2^(NBITS - A) words instead of
+// 2^NBITS): addr of high index h = hA[h & (2^A - 1)] ^ hB[h >> A].  Filled before the prologue,
+// whose barrier publishes it.
+template <int NBITS, int A>
+__device__ __forceinline__ void fill_hi_split(const uint64_t* basis, uint64_t* hA, uint64_t* hB) {
+    for (int h = threadIdx.x; h < (1 << A) + (1 << (NBITS - A)); h += kThreads) {
+        const bool lo = h < (1 << A);
+        const int v = lo ? h : h - (1 << A);
+        const int o = lo ? 0 : A;
+        const int nb = lo ? A : NBITS - A;
+        uint64_t a = 0;
+        for (int i = 0; i < nb; ++i)
+            if ((v >> i) & 1) a ^= basis[o + i];
+        if (lo) hA[v] = a; else hB[v] = a;
+    }
+}
+
+// Asynchronous global -> shared copies (LDGSTS) of the next tile's first-run entries into a
+// thread's own staging slots; the thread waits for its own copies only (no barrier needed).
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async8(uint32_t dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 #ifndef DCS_JIT_FP64
 // Tile load: entries active before the group (as runs.cuh: 4-entry segments when slot 0 is

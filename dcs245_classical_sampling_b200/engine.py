@@ -40,6 +40,9 @@ LN2 = math.log(2.0)
 # register runs of local dimension 4, groups of fewest table bytes.
 FP64_FUSED_CONFIG = {"max_dim": 12, "low": 3, "max_steps": 24, "variant": 12, "pairs": False, "grouping": "bytes",
                      "group_cost": 1 << 30, "max_extra": 1}
+# shapes tried in order when a group of the plan fits no run of that shape (small plans)
+FP64_FALLBACK_CONFIGS = ({"low": 4, "grouping": "greedy"}, {"variant": 4}, {"variant": 4, "low": 4, "grouping": "greedy"},
+                         {"variant": 4, "low": 2}, {"variant": 4, "low": 1, "grouping": "greedy"})
 
 
 def device_steps(steps):
@@ -182,7 +185,7 @@ class InplaceConditionalBlockGPU:
 
     # ------------------------------------------------------------------ allocation
     def alloc(self, dtype=np.complex64, device=0, fp64_kernel_path=None, mode=None, items=None,
-              hbm_budget=None, jit=None, storage=None):
+              hbm_budget=None, jit=None, storage=None, external_table=False):
         """Allocate device buffers (conditional_block_inplace_gpu.py:18-34).
 
         dtype: complex64 (FP32 arithmetic) or complex128 (FP64 arithmetic).
@@ -196,7 +199,9 @@ class InplaceConditionalBlockGPU:
         storage: "float16" stores each entry as two IEEE binary16 components (4 bytes), combines
         them in FP64 and rounds every stored value FP64 -> FP32 -> binary16: the reference's
         approximate half-storage tier (kernel_opt/inplace_half_gpu.py:37-78), which halves the
-        table of complex64; complex64 dtype and the "device" / "plain" executors only."""
+        table of complex64; complex64 dtype and the "device" / "plain" executors only.
+        external_table: allocate no table; the caller lends one per batch with bind_table (up to
+        `items` work items), e.g. from a device-memory pool shared by several engines."""
         if np.dtype(dtype) not in (np.dtype(np.complex64), np.dtype(np.complex128)):
             raise ValueError(dtype)
         if storage not in (None, "float16"):
@@ -253,13 +258,19 @@ class InplaceConditionalBlockGPU:
             self.fused_config = {"max_dim": cfg.get("max_dim", 13), "low": cfg.get("low", 4),
                                  "max_steps": cfg.get("max_steps", 24), "variant": cfg.get("variant", 0),
                                  "pairs": cfg.get("pairs", False), "grouping": cfg.get("grouping", "greedy"),
-                                 "group_cost": cfg.get("group_cost", 1 << 30), "max_extra": cfg.get("max_extra", 1)}
+                                 "group_cost": cfg.get("group_cost", 1 << 30), "max_extra": cfg.get("max_extra", 1),
+                                 "prefetch_kb": cfg.get("prefetch_kb", 0)}
             self.jit = bool(cfg.get("jit", False) if jit is None else jit)
             self.jit_minb = cfg.get("minb")
             self.jit_threads = cfg.get("threads") or 256
             self.fplan = self._build_fplan()
             self.items = 1
-        if half:  # (re, im) binary16 pairs
+        self.entry_bytes = entry
+        self.table_dtype = torch.float16 if half else tdtype
+        self.items_cap = self.items
+        if external_table:
+            self.table = None
+        elif half:  # (re, im) binary16 pairs
             self.table = torch.empty(self.items * table_entries * 2, dtype=torch.float16, device=self.device)
         else:
             self.table = torch.empty(self.items * table_entries, dtype=tdtype, device=self.device)
@@ -289,6 +300,31 @@ class InplaceConditionalBlockGPU:
         self._alloc = True
         self.buf = True
 
+    def table_item_bytes(self):
+        """Device bytes of one work item's table."""
+        return self.table_stride * self.entry_bytes
+
+    def bind_table(self, buf, items):
+        """Run the next batches on `items` work items' tables in `buf` (a device uint8 tensor of at
+        least items * table_item_bytes() bytes, 256-byte aligned), at most the capacity given
+        to alloc.  The engine keeps no other reference to the memory."""
+        items = int(items)
+        if not 0 < items <= self.items_cap:
+            raise ValueError(f"{items} work items outside 1..{self.items_cap}")
+        need = items * self.table_item_bytes()
+        if buf.dtype != torch.uint8 or buf.numel() < need or buf.data_ptr() % 256 or buf.device != self.device:
+            raise ValueError("bind_table needs a 256-byte aligned uint8 device buffer of items x table bytes")
+        self.table = buf[:need].view(self.table_dtype)
+        self.items = items
+
+    def _mb(self):
+        nm = self._nmax() + 1
+        return self.maxbits[: self.items * nm].view(self.items, nm)
+
+    def _sc(self):
+        w = _lib.SCALE_DTYPE.itemsize // 8
+        return self.scale[: self.items * w].view(self.items, w)
+
     def _nmax(self):
         return len(self.fplan.groups) if self.mode == "fused" else self.nsteps
 
@@ -297,6 +333,17 @@ class InplaceConditionalBlockGPU:
         plan-specialised kernels (jit.py) compiled for this plan."""
         from .fused import build_fused_plan
         fp = build_fused_plan(self.plan, **self.fused_config, fp64=self.use_fp64)
+        if self.use_fp64 and not all(int(v) & 4 for v in fp.groups["variant"]):
+            # small tiles may not fit register runs of dimension 4: the next shapes that do
+            for alt in FP64_FALLBACK_CONFIGS:
+                cfg = {**self.fused_config, **alt}
+                fp = build_fused_plan(self.plan, **cfg, fp64=True)
+                if all(int(v) & 4 for v in fp.groups["variant"]):
+                    self.fused_config = cfg
+                    break
+            else:
+                raise ValueError("complex128 fused tables: this plan has groups that fit no register run; "
+                                 "use mode='device'")
         if getattr(self, "jit", False) and fp.tile_runs is not None:
             from .jit import JitPlan
             fp.jit = JitPlan(self.plan, fp, self.lib, minb=getattr(self, "jit_minb", None),
@@ -350,11 +397,10 @@ class InplaceConditionalBlockGPU:
         return torch.cuda.current_stream(self.device).cuda_stream
 
     def _reset_items(self, n_items):
-        nm = self._nmax() + 1
-        mb = self.maxbits.view(self.items, nm)
+        mb = self._mb()
         mb[:n_items].zero_()
         mb[:n_items, 0] = self.one_bits
-        self.scale.view(self.items, -1)[:n_items].zero_()
+        self._sc()[:n_items].zero_()
         # empty environment = 1 at address 0 of every item (inplace_gpu.py:108)
         if getattr(self, "half", False):
             t = self.table.view(self.items, self.table_stride, 2)
@@ -432,7 +478,7 @@ class InplaceConditionalBlockGPU:
                                             _lib.ptr(self.maxbits), _lib.ptr(self.scale), st))
             return
         if self.mode == "plain":
-            mb = self.maxbits.view(self.items, nm)
+            mb = self._mb()
             for s in range(self.nsteps):
                 _lib.check(lib.dcs_slice_steps_batched(
                     self.dcode, _lib.ptr(self.table), self.table_stride, self.dsteps.ctypes.data, params_ptr,
@@ -472,7 +518,7 @@ class InplaceConditionalBlockGPU:
                 _lib.ptr(self.maxbits[nm - 1:]), nm, _lib.ptr(flat), self.k, cn, self._stream()))
             launches += 2
             if flags is not None:
-                flags[:cn] |= self.scale.view(self.items, -1)[:cn, 2]
+                flags[:cn] |= self._sc()[:cn, 2]
         _lib.check(lib.dcs_block_tail(_lib.ptr(out), self.k, self.adj_hi.ctypes.data, self.u_open.ctypes.data,
                                       prep["nblocks"], self._stream()))
         launches += 2 if self.k <= 12 else 4
@@ -483,7 +529,7 @@ class InplaceConditionalBlockGPU:
 
     def check_scale_flags(self, n_items=None):
         """Raise the reference's ArithmeticError if the last chunk saw a nonfinite table."""
-        sc = self.scale.view(self.items, -1)[: n_items or self.items, 2].cpu().numpy()
+        sc = self._sc()[: n_items or self.items, 2].cpu().numpy()
         if np.any(sc & 1):
             raise ArithmeticError("Nonfinite in-place environment")
 

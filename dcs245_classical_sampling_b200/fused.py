@@ -92,6 +92,9 @@ class FusedPlan:
     direct_io: bool = True
     # complex128 table, FP64 arithmetic (generated kernels only: the audit recontraction)
     fp64: bool = False
+    # generated kernels: KiB of shared memory per CTA for staging the next tile's first-run
+    # entries with asynchronous copies (0: the first run loads from the table; jit.prefetch_layout)
+    prefetch_kb: int = 0
     spans: list = field(default_factory=list)      # (first, count) per group
     universe: list = field(default_factory=list)   # |U| per group
     tiles: list = field(default_factory=list)      # tile count per group
@@ -397,10 +400,11 @@ def _plan_runs(steps, first, count, tsteps, truns, dim, R, tbit, slot_of, keep_b
 
 
 def build_fused_plan(plan, max_dim=13, low=4, max_steps=MAX_GROUP_STEPS, max_extra=1, spans=None, variant=0,
-                     pairs=False, grouping="greedy", group_cost=1 << 30, fp64=False):
+                     pairs=False, grouping="greedy", group_cost=1 << 30, fp64=False, prefetch_kb=0):
     """grouping: "greedy" (group_steps) or "bytes" (group_steps_min_bytes, `group_cost` bytes
     charged per group).  fp64: the plan runs on a complex128 table (plan-specialised register
-    runs only, see jit.py)."""
+    runs only, see jit.py).  prefetch_kb: staging of the next tile's first-run entries in the
+    generated kernels (jit.prefetch_layout)."""
     steps = plan.steps
     if spans is None:
         if grouping == "bytes":
@@ -413,7 +417,7 @@ def build_fused_plan(plan, max_dim=13, low=4, max_steps=MAX_GROUP_STEPS, max_ext
     tsteps = np.zeros(len(steps), dtype=_lib.TILE_STEP_DTYPE)
     truns = np.zeros(len(steps), dtype=_lib.TILE_RUN_DTYPE) if variant & 4 else None
     fp = FusedPlan(groups=groups, tile_steps=tsteps, dsteps=device_steps(steps), spans=list(spans), tile_runs=truns,
-                   coset_pairs=bool(pairs and variant & 4), fp64=bool(fp64))
+                   coset_pairs=bool(pairs and variant & 4), fp64=bool(fp64), prefetch_kb=int(prefetch_kb))
     for gi, (first, count) in enumerate(spans):
         U = 0
         vecs = []

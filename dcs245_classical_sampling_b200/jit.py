@@ -43,13 +43,13 @@ def _beff(kind, ts, R):
     return bl & ~own
 
 
-def _deposit_expr(g):
+def _deposit_expr(g, var="tile"):
     terms = []
     for r in range(int(g["ncoset_runs"])):
         w = int(g["coset_runs"][r])
         src, dst, ln = w & 255, (w >> 8) & 255, (w >> 16) & 255
         mask = (1 << 64) - 1 if ln >= 64 else (1 << ln) - 1
-        terms.append(f"(((tile >> {src}) & {_u64(mask)}) << {dst})")
+        terms.append(f"((({var} >> {src}) & {_u64(mask)}) << {dst})")
     return " | ".join(terms) if terms else "0ull"
 
 
@@ -79,6 +79,96 @@ def _direct_ok(fp, gi):
     g = fp.groups[gi]
     first, count = int(g["first"]), int(g["count"])
     return len({int(fp.tile_steps[first + s]["cskip"]) for s in range(count)}) == 1
+
+
+def _gaddr_fn(g):
+    TD, LOW = int(g["tile_dim"]), int(g["low_bits"])
+    lowmask = (1 << LOW) - 1
+    basis = [int(g["basis"][i]) for i in range(16)]
+
+    def gaddr(t):
+        a = t & lowmask
+        for i in range(TD - LOW):
+            if (t >> (LOW + i)) & 1:
+                a ^= basis[i]
+        return a
+    return gaddr
+
+
+def prefetch_layout(fp, gi, threads=256):
+    """Staging of the next tile's first-run entries (``fp.prefetch_kb`` > 0): every thread copies
+    the entries its own cosets of the next tile will load, asynchronously, into its own slots of
+    a staging buffer while the current tile runs; the first run then reads them from shared
+    memory.  Applies to multi-run groups with direct I/O whose first-run entries are live at the
+    same local indices in every coset (the address of every free tile coordinate avoids the
+    inactive slots).  Returns None, or the layout: KPF staged loop iterations (as many as fit
+    in prefetch_kb), the staged units (16-byte pairs (j, j1) or single entries (j, None)), the
+    unit size UB, the slot stride NBT (threads of the first run) and the staging bytes."""
+    kb = int(getattr(fp, "prefetch_kb", 0) or 0)
+    if kb <= 0 or not getattr(fp, "direct_io", True) or not _direct_ok(fp, gi) or not uses_tile_buffer(fp, gi):
+        return None
+    if getattr(fp, "coset_pairs", False):
+        return None
+    g = fp.groups[gi]
+    if not int(g["variant"]) & 4 or packable(fp, gi):
+        return None
+    fp64 = bool(getattr(fp, "fp64", False))
+    R = 4 if int(g["variant"]) & 8 else 3
+    first = int(g["first"])
+    TD, LOW = int(g["tile_dim"]), int(g["low_bits"])
+    T = 1 << TD
+    lognt = threads.bit_length() - 1
+    in_mask = int(fp.dsteps[first]["in_mask"])
+    in_inact = ~in_mask & 0xFFFFFFFFFFFFFFFF
+    gaddr = _gaddr_fn(g)
+    s, _ = _group_runs(fp, gi)[0]
+    tr = fp.tile_runs[first + s]
+    nins = int(tr["nins"])
+    ins = [int(x) for x in tr["ins"][:nins]]
+    NB = T >> nins
+    niter = NB >> lognt if NB > threads else 1
+    free = [b for b in range(TD) if b not in ins]
+    if any(gaddr(1 << f) & in_inact for f in free):
+        return None
+    G = [gaddr(int(tr["off"][j])) for j in range(1 << R)]
+    live = [j for j in range(1 << R) if not G[j] & in_inact]
+    if not live:
+        return None
+    k0 = None if fp64 else next((k for k in range(R) if int(tr["off"][1 << k]) == 1), None)
+    pair_in = LOW >= 1 and (in_mask & 1)
+    if k0 is not None and pair_in:
+        units = [(j, j | (1 << k0)) for j in live if not (j >> k0) & 1]
+        UB = 16
+    else:
+        units = [(j, None) for j in live]
+        UB = 16 if fp64 else 8
+    NBT = min(NB, threads)
+    per_iter = len(units) * UB * NBT
+    KPF = min(niter, (kb * 1024) // per_iter)
+    if KPF < 1:
+        return None
+    return {"KPF": KPF, "niter": niter, "units": units, "UB": UB, "NBT": NBT, "NB": NB, "ins": ins,
+            "G": G, "stg_bytes": KPF * per_iter}
+
+
+def _split_bits(TD, LOW):
+    nbits = max(1, TD - LOW)
+    return nbits, nbits // 2
+
+
+def group_smem(fp, gi, threads=256):
+    """Dynamic shared memory of the kernel of group gi: the tile buffer (if the kernel keeps one),
+    the table(s) of high tile-coordinate addresses and the staging buffer (prefetch_layout)."""
+    g = fp.groups[gi]
+    TD, LOW = int(g["tile_dim"]), int(g["low_bits"])
+    entry = 16 if getattr(fp, "fp64", False) else 8
+    tile = entry * (1 << TD) if uses_tile_buffer(fp, gi) else 0
+    lay = prefetch_layout(fp, gi, threads)
+    if lay is None:
+        return tile + 8 * (1 << (TD - LOW))
+    nbits, A = _split_bits(TD, LOW)
+    hi = 8 * ((1 << A) + (1 << (nbits - A)))
+    return tile + ((hi + 15) // 16) * 16 + lay["stg_bytes"]
 
 
 def _fixmask(fp, first, count):
@@ -144,6 +234,9 @@ def group_source(plan, fp, gi, minb=3, threads=256):
         return a
 
     runs = _group_runs(fp, gi)
+    lay = prefetch_layout(fp, gi, threads) if direct else None
+    cskip0 = _u64(fp.tile_steps[first]["cskip"])
+    ntiles = _u64(1 << int(g["coset_m"]))
     L = []
     L.append(f"__constant__ uint64_t g{gi}_basis[{nb}] = {{{', '.join(_u64(basis[i]) for i in range(nb))}}};")
     L.append(f"__constant__ uint64_t g{gi}_beta[{count}] = "
@@ -153,22 +246,79 @@ def group_source(plan, fp, gi, minb=3, threads=256):
              "unsigned long long* __restrict__ maxbits, jit_scale* __restrict__ scale) {")
     L.append(f"    constexpr int TD = {TD}, LOW = {LOW}, T = 1 << TD, COUNT = {count}, FIRST = {first};")
     L.append("    extern __shared__ __align__(16) unsigned char smem[];")
-    if uses_tile_buffer(fp, gi):
+    if lay is not None:
+        nbits, A = _split_bits(TD, LOW)
+        hbytes = ((8 * ((1 << A) + (1 << (nbits - A))) + 15) // 16) * 16
+        stg_off = (16 if fp64 else 8) * T + hbytes
         L.append("    cplx_t* sh = reinterpret_cast<cplx_t*>(smem);")
-        L.append("    uint64_t* hi_tab = reinterpret_cast<uint64_t*>(smem + sizeof(cplx_t) * T);")
+        L.append("    uint64_t* hA = reinterpret_cast<uint64_t*>(smem + sizeof(cplx_t) * T);")
+        L.append(f"    uint64_t* hB = hA + {1 << A};")
+        L.append("    uint64_t* hi_tab = nullptr;")
+        L.append(f"    const uint32_t stg_s = (uint32_t)__cvta_generic_to_shared(smem + {stg_off});")
+        L.append(f"    jit::fill_hi_split<{nbits}, {A}>(g{gi}_basis, hA, hB);")
+
+        def hexpr(t0):
+            sh_ = esh + LOW
+            return f"(hA[({t0} >> {sh_}) & {(1 << A) - 1}u] ^ hB[{t0} >> {sh_ + A}])"
     else:
-        L.append("    uint64_t* hi_tab = reinterpret_cast<uint64_t*>(smem);")
+        if uses_tile_buffer(fp, gi):
+            L.append("    cplx_t* sh = reinterpret_cast<cplx_t*>(smem);")
+            L.append("    uint64_t* hi_tab = reinterpret_cast<uint64_t*>(smem + sizeof(cplx_t) * T);")
+        else:
+            L.append("    uint64_t* hi_tab = reinterpret_cast<uint64_t*>(smem);")
+
+        def hexpr(t0):
+            return f"hi_tab[{t0} >> {esh + LOW}]"
     L.append("    __shared__ wts_t fw[COUNT];")
     L.append("    __shared__ int ovy[COUNT];")
     # Direct I/O: the sign bits alternate between two words, so the barrier after a tile's sign
     # bits is the only one between tiles (the next tile's first shared-memory writes come after
     # it, and warp 0 cannot pass it before every warp has read the previous word).
     L.append("    __shared__ uint32_t cs_sh[2];")
-    L.append(f"    const real_t sc = jit::prologue<TD, LOW, COUNT, FIRST, {_fixmask(fp, first, count)}u>(params, "
-             f"g{gi}_basis, maxbits, {gi}, scale, fw, ovy, hi_tab);")
+    L.append(f"    const real_t sc = jit::prologue<TD, LOW, COUNT, FIRST, {_fixmask(fp, first, count)}u, "
+             f"{'false' if lay is not None else 'true'}>(params, g{gi}_basis, maxbits, {gi}, scale, fw, ovy, hi_tab);")
     L.append("    real_t lm = 0;")
     L.append("    uint32_t par = 0;")
-    L.append(f"    for (uint64_t tile = blockIdx.x; tile < {_u64(1 << int(g['coset_m']))}; tile += gridDim.x) {{")
+    if lay is not None:
+        # the first run's thread representative, and the copies of a tile's staged entries
+        NBT = lay["NBT"]
+        lognbt = NBT.bit_length() - 1
+        ub_sh = lay["UB"].bit_length() - 1
+        nu = len(lay["units"])
+        free0 = [b for b in range(TD) if b not in lay["ins"]]
+        mhi0 = sum(1 << b for b in free0[lognt:]) << esh
+        L.append(f"    const bool pf_thread = (int)threadIdx.x < {lay['NB']};")
+        L.append("    uint32_t tp0 = threadIdx.x;")
+        for p in lay["ins"]:
+            L.append(f"    tp0 = jit::ins0(tp0, {p});")
+        L.append(f"    tp0 <<= {esh};")
+
+        def prefetch(tile_expr, ind):
+            out = [f"{ind}if (pf_thread) {{",
+                   f"{ind}    const uint64_t pt = {tile_expr};",
+                   f"{ind}    if (pt < {ntiles}) {{",
+                   f"{ind}        const uint64_t pbase = {_deposit_expr(g, 'pt')};",
+                   f"{ind}        if (!(pbase & {cskip0})) {{",
+                   f"{ind}            uint32_t ptu = 0;",
+                   "#pragma unroll"]
+            out.append(f"{ind}            for (int pk = 0; pk < {lay['KPF']}; ++pk) {{")
+            out.append(f"{ind}                const uint32_t pt0 = tp0 | ptu;")
+            out.append(f"{ind}                ptu = ((ptu | ~{mhi0}u) + 1u) & {mhi0}u;")
+            out.append(f"{ind}                const uint64_t pa0 = pbase ^ {hexpr('pt0')} ^ (uint64_t)((pt0 >> {esh}) & "
+                       f"{lowmask}u);")
+            out.append(f"{ind}                const uint32_t pd = stg_s + ((uint32_t)(pk * {nu}) << {lognbt + ub_sh}) + "
+                       f"((uint32_t)threadIdx.x << {ub_sh});")
+            for u, (j, _) in enumerate(lay["units"]):
+                fn = "cp_async16" if lay["UB"] == 16 else "cp_async8"
+                out.append(f"{ind}                jit::{fn}(pd + {u << (lognbt + ub_sh)}u, E + (pa0 ^ {_u64(lay['G'][j])}));")
+            out.append(f"{ind}            }}")
+            out.append(f"{ind}            jit::cp_async_commit();")
+            out.append(f"{ind}        }}")
+            out.append(f"{ind}    }}")
+            out.append(f"{ind}}}")
+            return out
+        L.extend(prefetch("(uint64_t)blockIdx.x", "    "))
+    L.append(f"    for (uint64_t tile = blockIdx.x; tile < {ntiles}; tile += gridDim.x) {{")
     L.append(f"        const uint64_t base = {_deposit_expr(g)};")
     if direct:
         L.append(f"        jit::sign_bits<COUNT>(g{gi}_beta, base, ovy, &cs_sh[par]);")
@@ -214,6 +364,8 @@ def group_source(plan, fp, gi, minb=3, threads=256):
             L.append(f"                tp = jit::ins0(tp, {p});")
         L.append(f"                tp <<= {esh};")
         L.append("                uint32_t tu = 0;")
+        if src_g and lay is not None:
+            L.append("                jit::cp_async_wait_all();  // this thread's staged entries of this tile")
         # local bit k0 with basis vector e_0: entries j and j | 2^k0 are one aligned 16-byte word
         # (complex64 entries only)
         k0 = None if fp64 else next((k for k in range(R) if int(tr["off"][1 << k]) == 1), None)
@@ -226,20 +378,45 @@ def group_source(plan, fp, gi, minb=3, threads=256):
             L.append(f"                    tu = ((tu | ~{mhi3}u) + 1u) & {mhi3}u;")
             L.append(f"                    cplx_t v{c}[{1 << R}];")
             if src_g or dst_g:
-                L.append(f"                    const uint64_t a0{c} = base ^ hi_tab[t0{c} >> {esh + LOW}] ^ "
+                L.append(f"                    const uint64_t a0{c} = base ^ {hexpr('t0' + c)} ^ "
                          f"(uint64_t)((t0{c} >> {esh}) & {lowmask}u);")
+        staged = src_g and lay is not None
         for c in cos:
+            if staged:  # entries staged by this thread's copies (iterations < KPF), else from the table
+                if lay["KPF"] < niter:
+                    L.append(f"                    if (k < {lay['KPF']}) {{")
+                L.append(f"                    const unsigned char* sk = smem + ({stg_off}u + ((uint32_t)(k * {nu}) << "
+                         f"{lognbt + ub_sh}) + ((uint32_t)threadIdx.x << {ub_sh}));")
+                liveset = set()
+                for u, (j, j1) in enumerate(lay["units"]):
+                    off = u << (lognbt + ub_sh)
+                    if j1 is not None:
+                        L.append(f"                    {{ const float4 q = *reinterpret_cast<const float4*>(sk + {off}u); "
+                                 f"v{c}[{j}] = make_float2(q.x, q.y); v{c}[{j1}] = make_float2(q.z, q.w); }}")
+                        liveset |= {j, j1}
+                    else:
+                        L.append(f"                    v{c}[{j}] = *reinterpret_cast<const cplx_t*>(sk + {off}u);")
+                        liveset.add(j)
+                for j in range(1 << R):
+                    if j not in liveset:
+                        L.append(f"                    v{c}[{j}] = jit::f2((real_t)0, (real_t)0);")
+                if lay["KPF"] < niter:
+                    L.append("                    } else {")
             if src_g:
-                if pairs and pair_in:
-                    for j, j1 in pairs:
-                        L.append(f"                    {{ const uint64_t a = a0{c} ^ {_u64(G[j])}; "
-                                 f"if (a & {_u64(in_inact)}) {{ v{c}[{j}] = v{c}[{j1}] = make_float2(0.f, 0.f); }} "
-                                 f"else {{ const float4 q = __ldcg(reinterpret_cast<const float4*>(E + a)); "
-                                 f"v{c}[{j}] = make_float2(q.x, q.y); v{c}[{j1}] = make_float2(q.z, q.w); }} }}")
-                else:
-                    for j in range(1 << R):
-                        L.append(f"                    {{ const uint64_t a = a0{c} ^ {_u64(G[j])}; "
-                                 f"v{c}[{j}] = (a & {_u64(in_inact)}) ? jit::f2((real_t)0, (real_t)0) : __ldcg(E + a); }}")
+                if not staged or lay["KPF"] < niter:
+                    if pairs and pair_in:
+                        for j, j1 in pairs:
+                            L.append(f"                    {{ const uint64_t a = a0{c} ^ {_u64(G[j])}; "
+                                     f"if (a & {_u64(in_inact)}) {{ v{c}[{j}] = v{c}[{j1}] = make_float2(0.f, 0.f); }} "
+                                     f"else {{ const float4 q = __ldcg(reinterpret_cast<const float4*>(E + a)); "
+                                     f"v{c}[{j}] = make_float2(q.x, q.y); v{c}[{j1}] = make_float2(q.z, q.w); }} }}")
+                    else:
+                        for j in range(1 << R):
+                            L.append(f"                    {{ const uint64_t a = a0{c} ^ {_u64(G[j])}; "
+                                     f"v{c}[{j}] = (a & {_u64(in_inact)}) ? jit::f2((real_t)0, (real_t)0) : "
+                                     "__ldcg(E + a); }")
+                if staged and lay["KPF"] < niter:
+                    L.append("                    }")
             elif pairs:
                 for j, j1 in pairs:
                     L.append(f"                    {{ const float4 q = *reinterpret_cast<const float4*>(shb + "
@@ -290,11 +467,16 @@ def group_source(plan, fp, gi, minb=3, threads=256):
                     L.append(f"                    *reinterpret_cast<cplx_t*>(shb + {sh_off(c, o)}) = v{c}[{j}];")
         L.append("                }")
         L.append("            }")
+        if src_g and lay is not None:  # every staged entry is in registers: stage the next tile
+            L.extend(prefetch("tile + gridDim.x", "            "))
         if not direct:
             L.append("        }")
         if not dst_g:
             L.append("        __syncthreads();")
     if direct:
+        if lay is not None:
+            L.append("        } else {")
+            L.extend(prefetch("tile + gridDim.x", "            "))
         L.append("        }")
         L.append("        par ^= 1u;")
     else:
@@ -557,7 +739,7 @@ class JitPlan:
             for gi in gis:
                 g = fp.groups[gi]
                 td, low = int(g["tile_dim"]), int(g["low_bits"])
-                smem = 8 * (1 << (td - low)) + (entry * (1 << td) if uses_tile_buffer(fp, gi) else 0)
+                smem = group_smem(fp, gi, self.threads)
                 k = ctypes.c_void_p()
                 per_sm = ctypes.c_int()
                 _lib.check(self.lib.dcs_jit_kernel(handle, f"dcs_g{gi}".encode(), smem, self.threads, ctypes.byref(k),

@@ -5,10 +5,11 @@
   the weights and amplitudes are taken on the host from one device-to-host copy, as the
   reference's record requires.  Extra keys: ``cdf_tie`` (the parallel FP64 CDF could not
   certify that NumPy's sequential CDF selects the same index, so the device ran the exact
-  sequential pass instead; the index is NumPy's either way) and ``cdf_straddle`` (the uniform
-  lies within ``straddle_margin`` of an edge of its CDF bin, so a block of the stated relative
-  error could select a neighbouring index: for complex64 blocks, the bound of a complex128
-  contraction of the same prefix).  ``exact_cdf=True`` runs NumPy's sequential CDF for the
+  sequential pass instead; the index is NumPy's either way) and ``cdf_straddle`` with
+  ``cdf_straddle_margin`` (the uniform lies within that margin of an edge of its CDF bin, so a
+  block of relative L2 error ``straddle_rel_l2`` could select a neighbouring index: by default
+  the complex64 tolerance against the complex128 contraction of the same prefix; see
+  ``straddle_margin``).  ``exact_cdf=True`` runs NumPy's sequential CDF for the
   block, so that ``cdf_lower_numpy``, ``cdf_upper_numpy`` and ``scaled_mass_cdf`` are NumPy's
   values bit for bit (otherwise they are the compensated values when no tie was found).
 * ``draw_many(blocks, uniforms)`` — the device-only fast path for a batch of blocks: returns
@@ -36,8 +37,20 @@ REPLAY_SCOPE = ("Full CDF checked in memory; hashes/interval retained. Independe
 COMPLEX64_REL_L2 = 1e-5
 # A block within relative L2 error r of another has normalised CDF values within 2r of the
 # other's: ||a/|a| - b/|b| || <= 2r, the probability vectors differ by at most twice that in L1,
-# and partial sums of two distributions differ by at most half their L1 distance.
-STRADDLE_MARGIN = 2 * COMPLEX64_REL_L2
+# and partial sums of two distributions differ by at most half their L1 distance.  At 2^20
+# outcomes a CDF bin is ~1e-6 wide, so this worst case covers every draw.
+CDF_SHIFT_BOUND = 2 * COMPLEX64_REL_L2
+# Standard deviations of the CDF shift that the straddle margin covers (see straddle_margin).
+STRADDLE_SIGMAS = 6.0
+
+
+def straddle_margin(weight_l2, rel_l2=COMPLEX64_REL_L2):
+    """Distance to a CDF edge within which another contraction of relative L2 error rel_l2 could
+    select a neighbouring index.  With independent per-entry relative errors of rms rel_l2, the
+    shift of a partial sum of the probabilities p_j has standard deviation <= 2 rel_l2
+    sqrt(sum p_j^2) (each p_j moves by about 2 p_j times its amplitude's relative error); the
+    margin is STRADDLE_SIGMAS of that, and never more than the worst case 2 rel_l2."""
+    return min(2.0 * rel_l2, STRADDLE_SIGMAS * 2.0 * rel_l2 * float(np.sqrt(max(weight_l2, 0.0))))
 
 
 class _Scratch:
@@ -101,13 +114,14 @@ def check_record(r):
         raise ArithmeticError("Independent accurately summed CDF interval disagrees; do not resample")
 
 
-def record_dict(r, straddle_margin=STRADDLE_MARGIN):
+def record_dict(r, straddle_rel_l2=COMPLEX64_REL_L2):
     """draw_checked's result keys (without the hashes) from a checked device record."""
     check_record(r)
     uniform = float(r["uniform"])
     lo, hi = float(r["cdf_lower_exact"]), float(r["cdf_upper_exact"])
     mass = float(r["total_exact"])
     near = min(uniform - lo, hi - uniform)
+    margin = straddle_margin(float(r["weight_l2"]), straddle_rel_l2) if straddle_rel_l2 is not None else 0.0
     return {"A_index": int(r["index"]), "uniform": uniform, "scaled_mass_cdf": float(r["total_cdf"]),
             "scaled_mass_fsum": mass, "selected_scaled_weight": float(r["selected_weight"]),
             "selected_conditional_probability": float(r["selected_weight"] / mass),
@@ -117,7 +131,7 @@ def record_dict(r, straddle_margin=STRADDLE_MARGIN):
             "independent_cdf_check_passed": True,
             "finite_53bit_draw_TV_against_computed_normalized_weights": float(r["tv53"]),
             "cdf_tie": bool(r["tie"]),
-            "cdf_straddle": bool(straddle_margin is not None and near < straddle_margin)}
+            "cdf_straddle": bool(near < margin), "cdf_straddle_margin": margin}
 
 
 def block_hashes(host):
@@ -127,7 +141,7 @@ def block_hashes(host):
             "amplitudes_sha256": hashlib.sha256(host.astype("<c16", copy=False).tobytes()).hexdigest()}
 
 
-def draw_checked(amplitudes, uniform, hashes=True, exact_cdf=False, straddle_margin=STRADDLE_MARGIN):
+def draw_checked(amplitudes, uniform, hashes=True, exact_cdf=False, straddle_rel_l2=COMPLEX64_REL_L2):
     """Reference-compatible checked draw (sampling_protocol.py:44-88)."""
     if isinstance(amplitudes, torch.Tensor):
         if amplitudes.dim() != 1:
@@ -144,14 +158,14 @@ def draw_checked(amplitudes, uniform, hashes=True, exact_cdf=False, straddle_mar
         raise ValueError("Nonfinite vector or invalid uniform")
     v = _as_device_blocks(amplitudes)
     r = draw_many(v.unsqueeze(0), [uniform], device=v.device, exact_cdf=exact_cdf)[0]
-    out = record_dict(r, straddle_margin)
+    out = record_dict(r, straddle_rel_l2)
     if hashes:
         out.update(block_hashes(v.cpu().numpy()))
     out["replay_scope"] = REPLAY_SCOPE
     return out
 
 
-def sample_checked(engine, x_list, uniforms, hashes=True, exact_cdf=False, straddle_margin=STRADDLE_MARGIN,
+def sample_checked(engine, x_list, uniforms, hashes=True, exact_cdf=False, straddle_rel_l2=COMPLEX64_REL_L2,
                    keep_host_blocks=False):
     """Blocks and checked draws of many prefixes, one sample at a time, as the reference's worker
     loop does (production/worker.py:105-113: block, host copy, draw_checked): the same records
@@ -189,7 +203,7 @@ def sample_checked(engine, x_list, uniforms, hashes=True, exact_cdf=False, strad
         copied[slot].synchronize()
         if bool((host_flags[slot] & 1).any()):
             raise ArithmeticError("Nonfinite in-place environment")
-        rec = record_dict(host_res[slot].numpy().view(_lib.DRAW_DTYPE)[0], straddle_margin)
+        rec = record_dict(host_res[slot].numpy().view(_lib.DRAW_DTYPE)[0], straddle_rel_l2)
         if hashes:
             rec.update(block_hashes(host_blk[slot].numpy()))
         rec["replay_scope"] = REPLAY_SCOPE

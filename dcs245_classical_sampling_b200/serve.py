@@ -8,12 +8,22 @@ static parameter tables on the device.  A batch of samples runs entirely on the 
   -> contraction (per-step batched kernels, or the fused kernel for large tables)
   -> slice accumulation -> Walsh-Hadamard/phase/U_open tail -> FP64 CDF draw
 
-and only the draw records (88 bytes per sample) come back.  The ``Server`` does continuous
-batching: arriving requests are admitted into their circuit's queue; whenever a runner's
-previous batch has finished it takes the next samples from every admitted request of its
-circuit (up to its slot count), so work of different requests shares launches and the runners
-of different circuits overlap on the device through their streams.  A sample's result depends
-only on (circuit, request id, sample index, key), never on what it was batched with.
+and only the draw records (96 bytes per sample) come back.  The ``Server`` does continuous
+batching: arriving requests are admitted into their circuit's active set; whenever a runner's
+previous batch has finished it takes the next samples round-robin over the active requests of
+its circuit (one sample of each in turn, up to its slot count), so work of different requests
+shares launches, a large request is split over many batches instead of holding the runner, and
+the runners of different circuits overlap on the device through their streams.  A sample's
+result depends only on (circuit, request id, sample index, key), never on what it was batched
+with.
+
+Admission by HBM budget: with a ``TablePool`` the contraction tables are not owned by the
+runners.  The pool holds the budget's device memory; a batch is launched only when the pool
+grants it a region for at least one work item (slice) of its circuit, and the region returns
+to the pool when the batch's records are back, so memory that one circuit frees admits the
+work of another (the 64-qubit circuit's 128 GiB table is granted per batch, not held).  Large
+regions are granted from the front of the pool and small ones from the back, and while a
+large request waits no small batch takes memory from the front.
 
 Latency of a request = completion time - arrival time (host clock); p50/p99 over requests.
 """
@@ -105,6 +115,68 @@ class DeviceCircuit:
             self.nslices, _lib.ptr(xbits), nsamples, _lib.ptr(params), _lib.ptr(coefs), _lib.ptr(xors), stream))
 
 
+class TablePool:
+    """One device buffer of `nbytes` (the HBM budget for contraction tables), granted to batches
+    as byte regions.  Regions of `large` bytes or more are granted first-fit from the front,
+    smaller ones from the back; freed regions merge with their neighbours.  `front_reserved`
+    bytes at the front are kept from small grants (set while a large request waits)."""
+
+    ALIGN = 256
+
+    def __init__(self, nbytes, device, large=1 << 34):
+        self.nbytes = int(nbytes) // self.ALIGN * self.ALIGN
+        self.device = torch.device(device) if not isinstance(device, torch.device) else device
+        self.buf = torch.empty(self.nbytes, dtype=torch.uint8, device=self.device)
+        self.free = [(0, self.nbytes)]  # sorted, disjoint (start, end)
+        self.large = int(large)
+        self.front_reserved = 0
+
+    def size(self, nbytes):
+        return -(-int(nbytes) // self.ALIGN) * self.ALIGN
+
+    def alloc(self, nbytes):
+        """A region (start, end) of at least `nbytes`, or None if no free run is large enough."""
+        size = self.size(nbytes)
+        if size <= 0 or size > self.nbytes:
+            return None
+        if size >= self.large:
+            for i, (s, e) in enumerate(self.free):
+                if e - s >= size:
+                    if s + size == e:
+                        del self.free[i]
+                    else:
+                        self.free[i] = (s + size, e)
+                    return (s, s + size)
+            return None
+        for i in range(len(self.free) - 1, -1, -1):
+            s, e = self.free[i]
+            if e - max(s, self.front_reserved) >= size:
+                if e - size == s:
+                    del self.free[i]
+                else:
+                    self.free[i] = (s, e - size)
+                return (e - size, e)
+        return None
+
+    def release(self, region):
+        self.free.append(tuple(region))
+        self.free.sort()
+        merged = []
+        for a, b in self.free:
+            if merged and merged[-1][1] == a:
+                merged[-1] = (merged[-1][0], b)
+            else:
+                merged.append((a, b))
+        self.free = merged
+
+    def free_bytes(self):
+        return sum(e - s for s, e in self.free)
+
+    def view(self, region):
+        s, e = region
+        return self.buf[s:e]
+
+
 @dataclass
 class Batch:
     samples: list            # (request id, sample index)
@@ -112,17 +184,24 @@ class Batch:
     host: torch.Tensor       # pinned draw records
     xbits: torch.Tensor      # pinned prefix masks
     launched: float
+    region: tuple = None     # pool region holding the batch's tables
 
 
 class CircuitRunner:
     """One circuit: engine, stream, device tables, in-flight batch buffers."""
 
-    def __init__(self, name, workload, key, max_samples, device=0, mode=None, hbm_budget=None, graphs=False):
+    def __init__(self, name, workload, key, max_samples, device=0, mode=None, hbm_budget=None, graphs=False,
+                 pool=None):
         """graphs=True: the device work of a batch (prefixes, parameters, contraction, accumulation,
-        tail, draw) is captured once per batch size as a CUDA graph and replayed."""
+        tail, draw) is captured once per batch size as a CUDA graph and replayed.
+        pool: a TablePool that grants the batch's tables per batch (admission by HBM budget);
+        without one the runner owns tables of `hbm_budget` bytes at most (default: one batch)."""
         self.name, self.key = name, int(key)
         self.graphs = bool(graphs)
         self._graph = {}
+        self.pool = pool
+        if pool is not None and self.graphs:
+            raise ValueError("CUDA graphs capture fixed table addresses: use runner-owned tables (no pool)")
         w = workload
         self.device = torch.device("cuda", device)
         self.engine = InplaceConditionalBlockGPU(w["graph"], w["unitaries"], w["n"], w["order"],
@@ -133,10 +212,20 @@ class CircuitRunner:
         entry = 8 << self.engine.plan.maxslots
         if self.mode == "fused":
             items = 1
+        elif pool is not None:
+            items = max_samples * L
         else:
             fit = int(hbm_budget // entry) if hbm_budget is not None else max_samples * L
             items = max(1, min(max_samples * L, fit))
-        self.engine.alloc(np.complex64, device=device, mode=self.mode, items=items)
+        if pool is not None and pool.size(entry) > pool.nbytes:
+            raise ValueError(f"{name}: one work item's table ({entry / 2**30:.3g} GiB) exceeds the HBM budget "
+                             f"({pool.nbytes / 2**30:.3g} GiB)")
+        if pool is None and hbm_budget is not None and entry > hbm_budget:
+            raise ValueError(f"{name}: one work item's table ({entry / 2**30:.3g} GiB) exceeds the HBM budget "
+                             f"({hbm_budget / 2**30:.3g} GiB)")
+        self.engine.alloc(np.complex64, device=device, mode=self.mode, items=items,
+                          external_table=pool is not None)
+        self.item_bytes = self.engine.table_item_bytes()
         self.lib = _lib.load()
         self.dc = DeviceCircuit(self.engine, self.device)
         assert self.dc.nslices == L
@@ -160,7 +249,26 @@ class CircuitRunner:
         self.d_scratch = torch.empty(self.lib.dcs_draw_scratch_bytes(self.k, M), dtype=torch.uint8, device=dev)
 
     def table_bytes(self):
-        return self.engine.table.numel() * self.engine.table.element_size()
+        """Device bytes of the tables the runner owns (0 with a pool: tables are granted per batch)."""
+        t = self.engine.table
+        return 0 if self.pool is not None or t is None else t.numel() * t.element_size()
+
+    def grant(self, n):
+        """Tables for a batch of n samples: with a pool, the largest region of up to n x slices work
+        items it grants now, bound to the engine (None if not even one item fits); without a pool,
+        the runner's own tables."""
+        if self.pool is None:
+            return ()
+        L = self.dc.nslices
+        want = n * L if self.mode != "fused" else 1
+        items = want
+        while items >= 1:
+            region = self.pool.alloc(items * self.item_bytes)
+            if region is not None:
+                self.engine.bind_table(self.pool.view(region), items)
+                return region
+            items //= 2
+        return None
 
     def _chunks(self, n):
         """Launch chunks of engine.items work items and, per chunk, the item ranges of its blocks."""
@@ -227,8 +335,9 @@ class CircuitRunner:
                 self._replay(n, chunks)
         self.stream.synchronize()
 
-    def launch(self, samples):
-        """Enqueue one batch (list of (request id, sample index)); returns a Batch."""
+    def launch(self, samples, region=()):
+        """Enqueue one batch (list of (request id, sample index)) on the tables of `region` (from
+        grant); returns a Batch."""
         n = len(samples)
         assert 0 < n <= self.max_samples
         chunks, begins = self._chunks(n)
@@ -248,7 +357,7 @@ class CircuitRunner:
             ev = torch.cuda.Event()
             ev.record(self.stream)
             self._hold = ids  # the pinned upload must outlive its copy
-        return Batch(list(samples), ev, host, hx, time.perf_counter())
+        return Batch(list(samples), ev, host, hx, time.perf_counter(), region or None)
 
 
 @dataclass
@@ -263,10 +372,30 @@ class Request:
 
 
 class Server:
-    """Continuous batching over several CircuitRunners."""
+    """Continuous batching over several CircuitRunners (see the module docstring).
 
-    def __init__(self, runners):
+    pool: the TablePool the runners were built with, if any (batches then launch only when it
+    grants their tables, and give them back when their records are in)."""
+
+    def __init__(self, runners, pool=None):
         self.runners = dict(runners)
+        self.pool = pool
+
+    @staticmethod
+    def _pick(active, m):
+        """Up to m samples round-robin over the active requests [request, next index] (one of each
+        in turn); returns the samples and the new next indices, without changing `active`."""
+        take, nxt = [], {id(a): a[1] for a in active}
+        progress = True
+        while len(take) < m and progress:
+            progress = False
+            for a in active:
+                r = a[0]
+                if nxt[id(a)] < r.nsamples and len(take) < m:
+                    take.append((r.rid, nxt[id(a)]))
+                    nxt[id(a)] += 1
+                    progress = True
+        return take, nxt
 
     def run(self, requests, realtime=True, poll_sleep=0.0005):
         """Serve `requests` (arrival times in seconds from start).  Returns the requests with
@@ -274,7 +403,7 @@ class Server:
         reqs = sorted(requests, key=lambda r: r.arrival)
         by_id = {r.rid: r for r in reqs}
         pending = collections.deque(reqs)
-        queues = {c: collections.deque() for c in self.runners}
+        active = {c: [] for c in self.runners}
         inflight = {c: None for c in self.runners}
         t0 = time.perf_counter()
         remaining = len(reqs)
@@ -282,7 +411,7 @@ class Server:
             now = time.perf_counter() - t0
             while pending and (pending[0].arrival <= now or not realtime):
                 r = pending.popleft()
-                queues[r.circuit].extend((r.rid, i) for i in range(r.nsamples))
+                active[r.circuit].append([r, 0])
             progressed = False
             for c, run in self.runners.items():
                 b = inflight[c]
@@ -297,12 +426,30 @@ class Server:
                         if r.done == r.nsamples:
                             r.finish = tnow
                             remaining -= 1
+                    if b.region is not None:
+                        self.pool.release(b.region)
                     inflight[c] = None
                     progressed = True
-                if inflight[c] is None and queues[c]:
-                    take = [queues[c].popleft() for _ in range(min(run.max_samples, len(queues[c])))]
-                    inflight[c] = run.launch(take)
-                    progressed = True
+            for c, run in self.runners.items():
+                if inflight[c] is not None or not active[c]:
+                    continue
+                take, nxt = self._pick(active[c], run.max_samples)
+                region = run.grant(len(take))
+                if region is None:  # no HBM for this circuit now: wait for a batch to give some back
+                    if self.pool is not None and run.item_bytes >= self.pool.large:
+                        self.pool.front_reserved = self.pool.size(run.item_bytes)
+                    continue
+                if self.pool is not None and run.item_bytes >= self.pool.large:
+                    self.pool.front_reserved = 0
+                if run.pool is not None and run.mode != "fused":  # the granted items bound the batch
+                    cap = max(1, run.engine.items // run.dc.nslices)
+                    if cap < len(take):
+                        take, nxt = self._pick(active[c], cap)
+                for a in active[c]:
+                    a[1] = nxt[id(a)]
+                active[c] = [a for a in active[c] if a[1] < a[0].nsamples]
+                inflight[c] = run.launch(take, region)
+                progressed = True
             if not progressed:
                 if pending and realtime:
                     time.sleep(min(poll_sleep, max(0.0, pending[0].arrival - (time.perf_counter() - t0))))

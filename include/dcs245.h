@@ -191,6 +191,7 @@ typedef struct dcs_draw_result {
     double cdf_lower_exact, cdf_upper_exact;/* compensated prefix / total */
     double uniform;
     double tv53;               /* 53-bit grid TV against the normalised weights */
+    double weight_l2;          /* sum of the squared normalised weights (sum p_i^2) */
 } dcs_draw_result;
 
 int dcs_abi_version(void);

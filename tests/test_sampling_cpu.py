@@ -78,4 +78,4 @@ def test_straddle_margin_bounds_the_cdf_shift():
             pa, pb = np.abs(a) ** 2, np.abs(b) ** 2
             shift = np.max(np.abs(np.cumsum(pa) / pa.sum() - np.cumsum(pb) / pb.sum()))
             assert shift <= 2 * r
-    assert sampling.STRADDLE_MARGIN == 2 * sampling.COMPLEX64_REL_L2
+    assert sampling.CDF_SHIFT_BOUND == 2 * sampling.COMPLEX64_REL_L2

@@ -128,3 +128,42 @@ def test_graph_replay_equals_direct_launches():
     assert a.keys() == b.keys()
     for key in a:
         assert a[key] == b[key], key
+
+
+def test_pool_admission_alone_and_in_the_mix():
+    """The 32- and 48-qubit serving circuits (2^14 and 2^17 blocks) share one table pool that holds
+    at most 9 of the 48-qubit circuit's 128 MiB work items, so its batches are admitted with as
+    many items as the pool grants at launch.  Every request's records are the same alone and in
+    the mix, and every granted region returns to the pool."""
+    from dcs245_classical_sampling_b200.serve import CircuitRunner, Request, Server, TablePool
+    from dcs245_classical_sampling_b200.workloads import build_workload
+    pool = TablePool(int(1.2 * 2 ** 30), "cuda")
+    runners = {"c32": CircuitRunner("c32", build_workload("ring32_d37_t79_k14"), key=0x5EED0201, max_samples=16,
+                                    pool=pool),
+               "c48": CircuitRunner("c48", build_workload("ring48_d55_t177_k17"), key=0x5EED0202, max_samples=16,
+                                    pool=pool)}
+    assert runners["c48"].item_bytes == 8 << 24 and runners["c48"].table_bytes() == 0
+    rng = np.random.default_rng(8)
+    reqs = [Request(rid, ("c32", "c48")[rid % 2], int(rng.integers(1, 13)), 0.0) for rid in range(8)]
+    mixed = Server(runners, pool).run([Request(r.rid, r.circuit, r.nsamples, 0.0) for r in reqs], realtime=False)
+    assert pool.free == [(0, pool.nbytes)]
+    mix = _records(mixed)
+    for r in reqs:
+        alone = _records(Server(runners, pool).run([Request(r.rid, r.circuit, r.nsamples, 0.0)], realtime=False))
+        for i in range(r.nsamples):
+            a, m = alone[(r.rid, i)], mix[(r.rid, i)]
+            assert a["status"] == 0 and m["status"] == 0
+            assert a["index"] == m["index"]
+            for f in ("cdf_lower", "cdf_upper", "selected_weight", "total_exact"):
+                assert a[f] == pytest.approx(m[f], rel=1e-12, abs=1e-300), f
+    assert pool.free == [(0, pool.nbytes)]
+
+
+def test_pool_refuses_a_circuit_larger_than_the_budget():
+    from dcs245_classical_sampling_b200.serve import CircuitRunner, TablePool
+    from dcs245_classical_sampling_b200.workloads import build_workload
+    pool = TablePool(64 << 20, "cuda")
+    with pytest.raises(ValueError, match="exceeds the HBM budget"):
+        CircuitRunner("c48", build_workload("ring48_d55_t177_k17"), key=1, max_samples=4, pool=pool)
+    with pytest.raises(ValueError, match="exceeds the HBM budget"):
+        CircuitRunner("c48", build_workload("ring48_d55_t177_k17"), key=1, max_samples=4, hbm_budget=64 << 20)
