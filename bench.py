@@ -68,6 +68,8 @@ def parse():
     ap.add_argument("--prefetch-kb", type=int, default=None,
                     help="generated kernels: KiB per CTA staging the next tile's first-run entries "
                          "(default: the tuned configuration)")
+    ap.add_argument("--tune-groups", action="store_true",
+                    help="choose the generated kernel variant per group (autotune.tune_groups) before timing")
     ap.add_argument("--serve", action="store_true", help="run the serving mix (32q/48q/64q) instead")
     ap.add_argument("--serve-seconds", type=float, default=12.0, help="arrival window of the serving run")
     ap.add_argument("--serve-rate", type=float, default=1.0, help="Poisson request rate (1/s)")
@@ -307,6 +309,9 @@ def gpu_arm(args):
         eng.set_fused_config(jit=not args.no_jit)  # plan-specialised group kernels (NVRTC, cached cubins)
     if args.mode == "fused" and args.prefetch_kb is not None:
         eng.set_fused_config(prefetch_kb=args.prefetch_kb)
+    group_report = None
+    if args.mode == "fused" and args.tune_groups:
+        group_report = eng.tune_groups()
     setup_s = time.perf_counter() - t0
     k = eng.k
     total = args.warmup + args.steps
@@ -410,7 +415,8 @@ def gpu_arm(args):
 
     fused_cfg = getattr(eng, "fused_config", None)
     if fused_cfg is not None:
-        fused_cfg = {**fused_cfg, "jit": bool(getattr(eng.fplan, "jit", None))}
+        fused_cfg = {**fused_cfg, "jit": bool(getattr(eng.fplan, "jit", None)),
+                     "group_cfg": {str(g): list(c) for g, c in (getattr(eng, "jit_group_cfg", None) or {}).items()}}
     del eng, preps, outs  # release the 128 GiB table before the other engines allocate theirs
     import gc
     gc.collect()
@@ -509,7 +515,7 @@ def gpu_arm(args):
                 "clocks": clk, "setup_s": setup_s, "cpu_baseline": cb, "audit": audit,
                 "configs": configs, "serve": serve,
                 "fused_config": fused_cfg,
-                "autotune": tune_report}
+                "autotune": tune_report, "tune_groups": group_report}
         print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.barrier()
@@ -760,7 +766,7 @@ def run_serving(args, local):
     slots = {c: {"samples_per_launch": r.max_samples, "table_item_gib": r.item_bytes / 2 ** 30, "mode": r.mode}
              for c, r in runners.items()}
     pool_free_after = None if pool is None else pool.free == [(0, pool.nbytes)]
-    del runners, pool
+    del runners, pool, kw
     gc.collect()
     torch.cuda.empty_cache()
     # plain per-request execution: measured per-sample times of the plain path per circuit

@@ -51,9 +51,11 @@ JIT_CANDIDATES = [(13, 3, 24, 12, False, None, 256, "bytes"), (13, 4, 24, 12, Fa
                   (13, 4, 24, 6, False), (13, 4, 24, 14, False), (13, 4, 24, 15, False)]
 
 
-KEYS = ("max_dim", "low", "max_steps", "variant", "pairs", "minb", "threads", "grouping", "group_cost", "max_extra")
-PLAN_KEYS = ("max_dim", "low", "max_steps", "variant", "pairs", "grouping", "group_cost", "max_extra")
-DEFAULTS = {"minb": None, "threads": 256, "grouping": "greedy", "group_cost": 1 << 30, "max_extra": 1}
+KEYS = ("max_dim", "low", "max_steps", "variant", "pairs", "minb", "threads", "grouping", "group_cost", "max_extra",
+        "prefetch_kb")
+PLAN_KEYS = ("max_dim", "low", "max_steps", "variant", "pairs", "grouping", "group_cost", "max_extra", "prefetch_kb")
+DEFAULTS = {"minb": None, "threads": 256, "grouping": "greedy", "group_cost": 1 << 30, "max_extra": 1,
+            "prefetch_kb": 0}
 
 
 def candidate(c):
@@ -124,3 +126,80 @@ def tune(engine, params_dev, candidates=None, repeats=1, save=True, jit=False):
         except OSError:
             pass
     return {"best": chosen, "candidates": report}
+
+
+# per-group kernel choices: (CTAs per SM the registers are sized for, KiB staging the next
+# tile's first-run entries; jit.prefetch_layout)
+GROUP_CANDIDATES = ((3, 0), (3, 8), (2, 0), (2, 16), (2, 32))
+
+
+def _time_groups(engine, fp, jp, params_dev, repeats):
+    """Per-group CUDA-event times (min over repeats) of one slice with the kernels of `jp`."""
+    import torch
+    lib = engine.lib
+    stream = torch.cuda.current_stream(engine.device)
+    ng = len(fp.groups)
+    best = [float("inf")] * ng
+    for _ in range(repeats + 1):
+        mb = engine.maxbits
+        mb.zero_()
+        mb[0] = engine.one_bits
+        engine.scale.zero_()
+        engine.table.view(engine.items, engine.table_stride)[:1, 0] = 1
+        evs = []
+        for gi in range(ng):
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            _lib.check(jp.launch(_lib.ptr(engine.table), _lib.ptr(params_dev), gi, 1, _lib.ptr(mb),
+                                 _lib.ptr(engine.scale), stream.cuda_stream))
+            b.record(stream)
+            evs.append((a, b))
+        torch.cuda.synchronize(engine.device)
+        for gi, (a, b) in enumerate(evs):
+            best[gi] = min(best[gi], a.elapsed_time(b) / 1000.0)
+    return best
+
+
+def tune_groups(engine, params_dev, candidates=GROUP_CANDIDATES, repeats=2, save=True):
+    """Choose, per group of the engine's fused plan (plan-specialised kernels), the kernel variant
+    of `candidates` with the shortest launch, timed with CUDA events on the engine's own table;
+    install the mix and return the report.  Every variant computes the same values bit for bit,
+    so groups can mix them."""
+    import torch
+    from .jit import JitPlan
+    fp = engine.fplan
+    if fp.jit is None:
+        raise ValueError("tune_groups needs the plan-specialised kernels (jit)")
+    lib = engine.lib
+    threads = fp.jit.threads
+    ng = len(fp.groups)
+    times = {}
+    for cand in candidates:
+        cand = (int(cand[0]), int(cand[1]))
+        jp = JitPlan(engine.plan, fp, lib, minb=cand[0], threads=threads, group_cfg={gi: cand for gi in range(ng)})
+        times[cand] = _time_groups(engine, fp, jp, params_dev, repeats)
+        jp.close()
+    choice = {gi: min(times, key=lambda c: times[c][gi]) for gi in range(ng)}
+    fp.jit.close()
+    fp.jit = JitPlan(engine.plan, fp, lib, minb=engine.jit_minb, threads=threads, group_cfg=choice)
+    engine.jit_group_cfg = choice
+    total = sum(_time_groups(engine, fp, fp.jit, params_dev, repeats))
+    report = {"group_cfg": {str(g): list(c) for g, c in choice.items()}, "seconds": total,
+              "per_candidate_seconds": {f"{c[0]}/{c[1]}": sum(t) for c, t in times.items()},
+              "per_group_ms": {str(g): {f"{c[0]}/{c[1]}": round(times[c][g] * 1e3, 4) for c in times}
+                               for g in range(ng)}}
+    if save:
+        key = f"{fingerprint(engine.plan)}|{torch.cuda.get_device_name(engine.device)}"
+        data = _load()
+        entry = dict(data.get(key) or {})
+        if entry and all(entry.get(k) == engine.fused_config.get(k) for k in PLAN_KEYS if k in entry):
+            entry["group_cfg"] = report["group_cfg"]
+            entry["seconds"] = round(total, 4)
+            entry["source"] = (entry.get("source", "") + "; per-group kernels chosen by autotune.tune_groups").lstrip("; ")
+            data[key] = entry
+            try:
+                CACHE.write_text(json.dumps(data, indent=1) + "\n")
+            except OSError:
+                pass
+    return report

@@ -4,8 +4,9 @@
 
 Same constructor ``(graph, unitaries, n, order, parity_operations, open_vertices)``, same
 ``alloc(dtype, device)`` and ``block(x_bits, w=None, part=0, parts=1) -> (vector, meta)``,
-same errors.  The returned vector is a complex128 torch tensor on the engine's device,
-scaled by sqrt(2^(n-k)), index bit j <-> ``open_vertices[j]``.
+same errors.  The returned vector is a complex128 torch tensor on the engine's device
+(``DeviceBlock``: ``np.asarray`` and ``cupy.asnumpy`` copy it to the host, as the reference's
+worker does), scaled by sqrt(2^(n-k)), index bit j <-> ``open_vertices[j]``.
 
 Execution modes (``alloc(..., mode=...)``):
 
@@ -165,6 +166,20 @@ class SliceParams:
         return count, out
 
 
+class DeviceBlock(torch.Tensor):
+    """What ``block`` returns: the complex128 block as a CUDA tensor that host code can copy the
+    way the reference's worker copies CuPy arrays (``host = cp.asnumpy(v)``,
+    production/worker.py:109): ``np.asarray(v)`` returns a host copy (so does ``cupy.asnumpy``,
+    through ``__cuda_array_interface__``, or a NumPy-backed stand-in of it).  Operations on it
+    return plain tensors."""
+
+    __torch_function__ = torch._C._disabled_torch_function_impl
+
+    def __array__(self, dtype=None, copy=None):
+        host = torch.Tensor.cpu(self).numpy()
+        return host if dtype is None else host.astype(dtype, copy=False)
+
+
 class InplaceConditionalBlockGPU:
     """Drop-in for the reference engine of the same name (see module docstring)."""
 
@@ -263,6 +278,7 @@ class InplaceConditionalBlockGPU:
             self.jit = bool(cfg.get("jit", False) if jit is None else jit)
             self.jit_minb = cfg.get("minb")
             self.jit_threads = cfg.get("threads") or 256
+            self.jit_group_cfg = {int(g): tuple(c) for g, c in (cfg.get("group_cfg") or {}).items()}
             self.fplan = self._build_fplan()
             self.items = 1
         self.entry_bytes = entry
@@ -347,14 +363,16 @@ class InplaceConditionalBlockGPU:
         if getattr(self, "jit", False) and fp.tile_runs is not None:
             from .jit import JitPlan
             fp.jit = JitPlan(self.plan, fp, self.lib, minb=getattr(self, "jit_minb", None),
-                             threads=getattr(self, "jit_threads", 256))
+                             threads=getattr(self, "jit_threads", 256),
+                             group_cfg=getattr(self, "jit_group_cfg", None))
         return fp
 
-    def set_fused_config(self, jit=None, minb=None, threads=None, **cfg):
-        """Rebuild the fused plan with another tile shape (max_dim, low, max_steps, variant, pairs);
-        jit=True/False switches the plan-specialised group kernels on or off; minb: CTAs per SM
-        their registers are sized for (default: 2 with variant bit 0, else 3); threads: per CTA of
-        those kernels (default 256)."""
+    def set_fused_config(self, jit=None, minb=None, threads=None, group_cfg=None, **cfg):
+        """Rebuild the fused plan with another tile shape (max_dim, low, max_steps, variant, pairs,
+        prefetch_kb); jit=True/False switches the plan-specialised group kernels on or off; minb:
+        CTAs per SM their registers are sized for (default: 2 with variant bit 0, else 3);
+        threads: per CTA of those kernels (default 256); group_cfg: {group: (minb, prefetch_kb)}
+        for single groups (dropped when the shape changes and none is given)."""
         if self.mode != "fused":
             raise ValueError("set_fused_config needs mode='fused'")
         if self.use_fp64 and (jit is False or not cfg.get("variant", 4) & 4):
@@ -365,9 +383,26 @@ class InplaceConditionalBlockGPU:
             self.jit_minb = int(minb)
         if threads is not None:
             self.jit_threads = int(threads)
+        if group_cfg is not None:
+            self.jit_group_cfg = {int(g): tuple(c) for g, c in group_cfg.items()}
+        elif any(k != "prefetch_kb" for k in cfg) or minb is not None:
+            self.jit_group_cfg = {}
+        if "prefetch_kb" in cfg and group_cfg is None:
+            self.jit_group_cfg = {}
         self.fused_config = {**self.fused_config, **cfg}
         self.fplan = self._build_fplan()
         self.maxbits = torch.zeros(self.items * (len(self.fplan.groups) + 1), dtype=torch.int64, device=self.device)
+
+    def tune_groups(self, x_bits=None, save=True, **kw):
+        """Choose per group of the fused plan the plan-specialised kernel variant (CTAs per SM,
+        staging of the next tile's first-run entries) with the shortest launch (autotune.tune_groups)."""
+        from . import autotune as at
+        if self.mode != "fused" or self.fplan.jit is None:
+            raise ValueError("tune_groups needs mode='fused' with the plan-specialised kernels")
+        x = np.zeros(self.n, np.uint8) if x_bits is None else x_bits
+        _, items = self.params.items(x)
+        prm = torch.from_numpy(items[0][1].view(np.int64).copy()).to(self.device)
+        return at.tune_groups(self, prm, save=save and not self.use_fp64, **kw)
 
     def autotune(self, x_bits=None, candidates=None, jit=None):
         """Time the fused tile-shape candidates on this engine's table and keep the fastest
@@ -383,6 +418,7 @@ class InplaceConditionalBlockGPU:
         jit = self.jit if jit is None else bool(jit)
         if self.fplan.jit is not None:
             self.fplan.jit.close()
+        self.jit_group_cfg = {}
         rep = at.tune(self, prm, jit=jit, **({"candidates": candidates} if candidates else {}))
         self.jit = jit
         self.jit_minb = rep["best"].get("minb")
@@ -549,7 +585,8 @@ class InplaceConditionalBlockGPU:
         start = time.perf_counter()
         out, prep = self._run([x_bits], w, part, parts)
         torch.cuda.current_stream(self.device).synchronize()
-        return out[0], self._meta(time.perf_counter() - start, part, parts, prep["counts"][0])
+        return out[0].as_subclass(DeviceBlock), self._meta(time.perf_counter() - start, part, parts,
+                                                           prep["counts"][0])
 
     def _meta(self, seconds, part, parts, count):
         return {"seconds": seconds, "part": part, "parts": parts, "slices_evaluated": count,

@@ -95,7 +95,7 @@ def _gaddr_fn(g):
     return gaddr
 
 
-def prefetch_layout(fp, gi, threads=256):
+def prefetch_layout(fp, gi, threads=256, kb=None):
     """Staging of the next tile's first-run entries (``fp.prefetch_kb`` > 0): every thread copies
     the entries its own cosets of the next tile will load, asynchronously, into its own slots of
     a staging buffer while the current tile runs; the first run then reads them from shared
@@ -104,7 +104,7 @@ def prefetch_layout(fp, gi, threads=256):
     inactive slots).  Returns None, or the layout: KPF staged loop iterations (as many as fit
     in prefetch_kb), the staged units (16-byte pairs (j, j1) or single entries (j, None)), the
     unit size UB, the slot stride NBT (threads of the first run) and the staging bytes."""
-    kb = int(getattr(fp, "prefetch_kb", 0) or 0)
+    kb = int((getattr(fp, "prefetch_kb", 0) if kb is None else kb) or 0)
     if kb <= 0 or not getattr(fp, "direct_io", True) or not _direct_ok(fp, gi) or not uses_tile_buffer(fp, gi):
         return None
     if getattr(fp, "coset_pairs", False):
@@ -156,14 +156,15 @@ def _split_bits(TD, LOW):
     return nbits, nbits // 2
 
 
-def group_smem(fp, gi, threads=256):
+def group_smem(fp, gi, threads=256, kb=None):
     """Dynamic shared memory of the kernel of group gi: the tile buffer (if the kernel keeps one),
-    the table(s) of high tile-coordinate addresses and the staging buffer (prefetch_layout)."""
+    the table(s) of high tile-coordinate addresses and the staging buffer (prefetch_layout with
+    `kb`, default the plan's prefetch_kb)."""
     g = fp.groups[gi]
     TD, LOW = int(g["tile_dim"]), int(g["low_bits"])
     entry = 16 if getattr(fp, "fp64", False) else 8
     tile = entry * (1 << TD) if uses_tile_buffer(fp, gi) else 0
-    lay = prefetch_layout(fp, gi, threads)
+    lay = prefetch_layout(fp, gi, threads, kb)
     if lay is None:
         return tile + 8 * (1 << (TD - LOW))
     nbits, A = _split_bits(TD, LOW)
@@ -180,7 +181,7 @@ def _fixmask(fp, first, count):
     return m
 
 
-def group_source(plan, fp, gi, minb=3, threads=256):
+def group_source(plan, fp, gi, minb=3, threads=256, kb=None):
     """CUDA source of the kernel of group gi (``dcs_g<gi>``); None if the group has no runs.
 
     Direct I/O (``fp.direct_io``, the default): the first run of a tile loads its cosets from
@@ -234,7 +235,7 @@ def group_source(plan, fp, gi, minb=3, threads=256):
         return a
 
     runs = _group_runs(fp, gi)
-    lay = prefetch_layout(fp, gi, threads) if direct else None
+    lay = prefetch_layout(fp, gi, threads, kb) if direct else None
     cskip0 = _u64(fp.tile_steps[first]["cskip"])
     ntiles = _u64(1 << int(g["coset_m"]))
     L = []
@@ -575,7 +576,7 @@ def _packed_source(fp, gi, minb):
         niter = NB2 >> 8 if NB2 > 256 else 1
         mhi = int(tr["mhi"])
         mhi3 = (mhi & (mhi - 1)) << 3  # tile bit 0 is the lane bit
-        offs = [int(tr["off"][j]) << esh for j in range(1 << R)]
+        offs = [int(tr["off"][j]) << 3 for j in range(1 << R)]
         G = [gaddr(int(tr["off"][j])) for j in range(1 << R)]
         L.append(f"        // run: steps {first + s}..{first + s + n - 1}, {NB2} coset pairs of {1 << R} entries"
                  f"{', from the table' if src_g else ''}{', to the table' if dst_g else ''}")
@@ -653,12 +654,16 @@ def _packed_source(fp, gi, minb):
     return "\n".join(L) + "\n"
 
 
-def plan_sources(plan, fp, minb=3, parts=8, threads=256):
+def plan_sources(plan, fp, minb=3, parts=8, threads=256, group_cfg=None):
     """Translation units (source strings) holding the group kernels, spread over `parts` units
-    so that NVRTC compiles them in parallel; returns [(source, [group indices])]."""
+    so that NVRTC compiles them in parallel; returns [(source, [group indices])].  group_cfg:
+    {group: (CTAs per SM of its registers, staging KiB)} overriding minb and the plan's
+    prefetch_kb for that group."""
     groups = [gi for gi in range(len(fp.groups)) if int(fp.groups[gi]["variant"]) & 4]
+    cfg = group_cfg or {}
     # balance by generated size
-    bodies = {gi: group_source(plan, fp, gi, minb, threads) for gi in groups}
+    bodies = {gi: group_source(plan, fp, gi, cfg.get(gi, (minb, None))[0], threads, cfg.get(gi, (minb, None))[1])
+              for gi in groups}
     units = [([], 0) for _ in range(max(1, min(parts, len(groups))))]
     for gi in sorted(groups, key=lambda q: -len(bodies[q])):
         k = min(range(len(units)), key=lambda u: units[u][1])
@@ -700,10 +705,10 @@ def compile_source(lib, source, name="dcs_plan.cu"):
     return data
 
 
-def compile_plan(plan, fp, lib=None, minb=3, parts=8, threads=256):
+def compile_plan(plan, fp, lib=None, minb=3, parts=8, threads=256, group_cfg=None):
     """[(cubin, [group indices])] for a fused plan (NVRTC in parallel threads)."""
     lib = lib or _lib.load()
-    units = plan_sources(plan, fp, minb, parts, threads)
+    units = plan_sources(plan, fp, minb, parts, threads, group_cfg)
     with ThreadPoolExecutor(max_workers=len(units) or 1) as ex:
         images = list(ex.map(lambda u: compile_source(lib, u[0], f"dcs_plan_{u[1][0]}.cu"), units))
     return [(img, gis) for img, (_, gis) in zip(images, units)]
@@ -712,9 +717,9 @@ def compile_plan(plan, fp, lib=None, minb=3, parts=8, threads=256):
 class JitPlan:
     """Loaded group kernels of one fused plan (current CUDA device)."""
 
-    def __init__(self, plan, fp, lib=None, minb=None, parts=8, threads=256):
+    def __init__(self, plan, fp, lib=None, minb=None, parts=8, threads=256, group_cfg=None):
         """minb: CTAs per SM the registers are sized for (default: 2 if the plan's variant has
-        bit 0, else 3)."""
+        bit 0, else 3).  group_cfg: {group: (minb, staging KiB)} for groups that differ."""
         self.lib = lib or _lib.load()
         self.fp = fp
         self.kernels = {}
@@ -724,13 +729,13 @@ class JitPlan:
             minb = 2 if len(fp.groups) and int(fp.groups[0]["variant"]) & 1 else 3
         self.minb = int(minb)
         self.threads = int(threads)
+        self.group_cfg = {int(g): (int(m), int(kb)) for g, (m, kb) in (group_cfg or {}).items()}
         sms = self.lib.dcs_sm_count()
-        entry = 16 if getattr(fp, "fp64", False) else 8
         if getattr(fp, "fp64", False):
             missing = [gi for gi in range(len(fp.groups)) if not int(fp.groups[gi]["variant"]) & 4]
             if missing:  # the library's fused kernels store complex64 only
                 raise ValueError(f"complex128 fused plan: groups {missing} have no register runs")
-        for img, gis in compile_plan(plan, fp, self.lib, minb, parts, self.threads):
+        for img, gis in compile_plan(plan, fp, self.lib, minb, parts, self.threads, self.group_cfg):
             buf = ctypes.create_string_buffer(img, len(img))
             self._images.append(buf)
             handle = ctypes.c_void_p()
@@ -738,8 +743,7 @@ class JitPlan:
             self._libs.append(handle)
             for gi in gis:
                 g = fp.groups[gi]
-                td, low = int(g["tile_dim"]), int(g["low_bits"])
-                smem = group_smem(fp, gi, self.threads)
+                smem = group_smem(fp, gi, self.threads, self.group_cfg.get(gi, (None, None))[1])
                 k = ctypes.c_void_p()
                 per_sm = ctypes.c_int()
                 _lib.check(self.lib.dcs_jit_kernel(handle, f"dcs_g{gi}".encode(), smem, self.threads, ctypes.byref(k),

@@ -161,3 +161,21 @@ def test_staged_first_run_is_bit_identical(golden, name, kb):
         got = eng.block(x)[0].cpu().numpy()
         assert np.array_equal(got, want)
         assert rel_l2(got, arrays[f"block_{rec['sample_id']}"]) < 1e-5
+
+
+def test_block_is_copied_to_host_as_the_reference_worker_does(golden):
+    """engine.block's vector: np.asarray (the reference fixture's cp.asnumpy stand-in) and the
+    CUDA array interface (cupy.asnumpy) give the host block, and the worker's draw on the host
+    copy equals the draw on the device tensor (production/worker.py:109-110)."""
+    from dcs245_classical_sampling_b200.engine import DeviceBlock
+    from dcs245_classical_sampling_b200.sampling import draw_checked
+    case, arrays = golden("c1")
+    eng = _engine(case, arrays, np.complex64, "fused", jit_shape=True)
+    rec = case["protocol"]["records"][0]
+    v, meta = eng.block(_x(rec))
+    assert isinstance(v, DeviceBlock) and v.is_cuda and v.dtype == torch.complex128
+    cai = v.__cuda_array_interface__
+    assert cai["typestr"] == "<c16" and cai["shape"] == (1 << len(case["open_vertices"]),)
+    host = np.asarray(v)
+    np.testing.assert_array_equal(host, v.cpu().numpy())
+    assert draw_checked(host, rec["draw_uniform"]) == draw_checked(v, rec["draw_uniform"])

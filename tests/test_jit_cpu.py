@@ -33,3 +33,28 @@ def test_compile_errors_raise_with_the_log():
     lib = _lib.load()
     with pytest.raises(_lib.DCSError, match="error"):
         jit.compile_source(lib, '#include "runs_jit.cuh"\nextern "C" __global__ void k() { undefined_name(); }\n')
+
+
+@pytest.mark.parametrize("name", ["small", "c2"])
+def test_fp64_and_staged_kernels_compile(golden, name):
+    """The complex128 (FP64) form and the staged-first-run form of the generated kernels compile;
+    staging changes only shared memory (per-group sizes from group_smem), and a per-group
+    configuration reaches every group's source."""
+    case, arrays = golden(name)
+    bp = P.build_block_plan(arrays["graph"], arrays["unitaries"], case["n"], case["order"],
+                            case["parity_operations"], case["open_vertices"])
+    lib = _lib.load()
+    fp64 = build_fused_plan(bp, max_dim=12, low=3, variant=12, grouping="bytes", fp64=True)
+    for src, _ in jit.plan_sources(bp, fp64, minb=2, parts=1):
+        assert "#define DCS_JIT_FP64 1" in src
+        assert jit.compile_source(lib, src)[:4] == b"\x7fELF"
+    fp = build_fused_plan(bp, max_dim=13, low=3, variant=12, grouping="bytes")
+    staged = [gi for gi in range(len(fp.groups)) if jit.prefetch_layout(fp, gi, kb=16)]
+    assert staged
+    for gi in staged:
+        assert jit.group_smem(fp, gi, kb=16) > jit.group_smem(fp, gi, kb=0) - 8 * (1 << 13)
+    cfg = {gi: (2, 16) if gi in staged else (3, 0) for gi in range(len(fp.groups))}
+    units = jit.plan_sources(bp, fp, parts=1, group_cfg=cfg)
+    src = units[0][0]
+    assert src.count("cp_async_wait_all") == len(staged)
+    assert jit.compile_source(lib, src)[:4] == b"\x7fELF"
