@@ -25,6 +25,7 @@ import json
 import math
 import os
 import sys
+import tempfile
 import types
 from pathlib import Path
 
@@ -35,6 +36,10 @@ REPO = HERE.parents[1]
 if not os.environ.get("REFERENCE_ROOT"):
     raise SystemExit("set REFERENCE_ROOT to the reference checkout")
 REF = Path(os.environ["REFERENCE_ROOT"]) / "source"
+# write nothing into the reference checkout: no bytecode, and Numba's cache (its kernels are
+# declared with cache=True) in a temporary directory
+sys.dont_write_bytecode = True
+os.environ.setdefault("NUMBA_CACHE_DIR", tempfile.mkdtemp(prefix="numba_cache_"))
 
 
 def install_reference():
