@@ -129,8 +129,8 @@ def tune(engine, params_dev, candidates=None, repeats=1, save=True, jit=False):
 
 
 # per-group kernel choices: (CTAs per SM the registers are sized for, KiB staging the next
-# tile's first-run entries; jit.prefetch_layout)
-GROUP_CANDIDATES = ((3, 0), (3, 8), (2, 0), (2, 16), (2, 32))
+# tile's first-run entries (jit.prefetch_layout), local dimension of the register runs)
+GROUP_CANDIDATES = ((3, 0, 4), (3, 8, 4), (2, 0, 4), (2, 16, 4), (2, 32, 4), (2, 0, 5), (2, 16, 5), (2, 32, 5))
 
 
 def _time_groups(engine, fp, jp, params_dev, repeats):
@@ -163,40 +163,55 @@ def _time_groups(engine, fp, jp, params_dev, repeats):
 
 def tune_groups(engine, params_dev, candidates=GROUP_CANDIDATES, repeats=2, save=True):
     """Choose, per group of the engine's fused plan (plan-specialised kernels), the kernel variant
-    of `candidates` with the shortest launch, timed with CUDA events on the engine's own table;
-    install the mix and return the report.  Every variant computes the same values bit for bit,
-    so groups can mix them."""
+    of `candidates` (CTAs per SM, staging KiB, register-run dimension 4 or 5) with the shortest
+    launch, timed with CUDA events on the engine's own table; install the mix and return the
+    report.  Every variant computes the same values bit for bit (the same operations in the same
+    order on each entry), so groups can mix them."""
     import torch
+    from .fused import build_fused_plan
     from .jit import JitPlan
-    fp = engine.fplan
-    if fp.jit is None:
+    if engine.fplan.jit is None:
         raise ValueError("tune_groups needs the plan-specialised kernels (jit)")
     lib = engine.lib
-    threads = fp.jit.threads
-    ng = len(fp.groups)
+    threads = engine.fplan.jit.threads
+    base = {k: v for k, v in engine.fused_config.items() if k != "group_variant"}
+    v4 = (int(base["variant"]) & ~16) | 12
+    plans = {4: build_fused_plan(engine.plan, **{**base, "variant": v4}),
+             5: build_fused_plan(engine.plan, **{**base, "variant": v4 | 16})}
+    ng = len(plans[4].groups)
     times = {}
     for cand in candidates:
-        cand = (int(cand[0]), int(cand[1]))
-        jp = JitPlan(engine.plan, fp, lib, minb=cand[0], threads=threads, group_cfg={gi: cand for gi in range(ng)})
-        times[cand] = _time_groups(engine, fp, jp, params_dev, repeats)
+        minb, kb, r = (int(x) for x in cand)
+        fp = plans[r]
+        jp = JitPlan(engine.plan, fp, lib, minb=minb, threads=threads, group_cfg={gi: (minb, kb) for gi in range(ng)})
+        t = _time_groups(engine, fp, jp, params_dev, repeats)
         jp.close()
+        for gi in range(ng):  # a dimension-5 plan group that fell back to 4 is the same kernel: skip
+            if r == 5 and not int(fp.groups[gi]["variant"]) & 16:
+                t[gi] = float("inf")
+        times[(minb, kb, r)] = t
     choice = {gi: min(times, key=lambda c: times[c][gi]) for gi in range(ng)}
-    fp.jit.close()
-    fp.jit = JitPlan(engine.plan, fp, lib, minb=engine.jit_minb, threads=threads, group_cfg=choice)
-    engine.jit_group_cfg = choice
-    total = sum(_time_groups(engine, fp, fp.jit, params_dev, repeats))
-    report = {"group_cfg": {str(g): list(c) for g, c in choice.items()}, "seconds": total,
-              "per_candidate_seconds": {f"{c[0]}/{c[1]}": sum(t) for c, t in times.items()},
-              "per_group_ms": {str(g): {f"{c[0]}/{c[1]}": round(times[c][g] * 1e3, 4) for c in times}
-                               for g in range(ng)}}
+    group_variant = {gi: v4 | 16 for gi, c in choice.items() if c[2] == 5}
+    group_cfg = {gi: (c[0], c[1]) for gi, c in choice.items()}
+    engine.fplan.jit.close()
+    engine.fused_config = {**base, "group_variant": group_variant}
+    engine.jit_group_cfg = group_cfg
+    engine.fplan = engine._build_fplan()
+    total = sum(_time_groups(engine, engine.fplan, engine.fplan.jit, params_dev, repeats))
+    report = {"group_cfg": {str(g): list(c) for g, c in group_cfg.items()},
+              "group_variant": {str(g): v for g, v in group_variant.items()}, "seconds": total,
+              "per_candidate_seconds": {"/".join(map(str, c)): sum(x for x in t if x != float("inf"))
+                                        for c, t in times.items()},
+              "per_group_ms": {str(g): {"/".join(map(str, c)): round(times[c][g] * 1e3, 4) for c in times
+                                        if times[c][g] != float("inf")} for g in range(ng)}}
     if save:
         key = f"{fingerprint(engine.plan)}|{torch.cuda.get_device_name(engine.device)}"
         data = _load()
         entry = dict(data.get(key) or {})
-        if entry and all(entry.get(k) == engine.fused_config.get(k) for k in PLAN_KEYS if k in entry):
+        if entry and all(entry.get(k) == base.get(k) for k in PLAN_KEYS if k in entry):
             entry["group_cfg"] = report["group_cfg"]
+            entry["group_variant"] = report["group_variant"]
             entry["seconds"] = round(total, 4)
-            entry["source"] = (entry.get("source", "") + "; per-group kernels chosen by autotune.tune_groups").lstrip("; ")
             data[key] = entry
             try:
                 CACHE.write_text(json.dumps(data, indent=1) + "\n")

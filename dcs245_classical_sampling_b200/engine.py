@@ -274,7 +274,8 @@ class InplaceConditionalBlockGPU:
                                  "max_steps": cfg.get("max_steps", 24), "variant": cfg.get("variant", 0),
                                  "pairs": cfg.get("pairs", False), "grouping": cfg.get("grouping", "greedy"),
                                  "group_cost": cfg.get("group_cost", 1 << 30), "max_extra": cfg.get("max_extra", 1),
-                                 "prefetch_kb": cfg.get("prefetch_kb", 0)}
+                                 "prefetch_kb": cfg.get("prefetch_kb", 0),
+                                 "group_variant": {int(g): int(v) for g, v in (cfg.get("group_variant") or {}).items()}}
             self.jit = bool(cfg.get("jit", False) if jit is None else jit)
             self.jit_minb = cfg.get("minb")
             self.jit_threads = cfg.get("threads") or 256
@@ -385,10 +386,10 @@ class InplaceConditionalBlockGPU:
             self.jit_threads = int(threads)
         if group_cfg is not None:
             self.jit_group_cfg = {int(g): tuple(c) for g, c in group_cfg.items()}
-        elif any(k != "prefetch_kb" for k in cfg) or minb is not None:
+        elif cfg or minb is not None:
             self.jit_group_cfg = {}
-        if "prefetch_kb" in cfg and group_cfg is None:
-            self.jit_group_cfg = {}
+        if cfg and "group_variant" not in cfg:
+            cfg["group_variant"] = {}  # per-group variants belong to one shape
         self.fused_config = {**self.fused_config, **cfg}
         self.fplan = self._build_fplan()
         self.maxbits = torch.zeros(self.items * (len(self.fplan.groups) + 1), dtype=torch.int64, device=self.device)

@@ -95,6 +95,9 @@ class FusedPlan:
     # generated kernels: KiB of shared memory per CTA for staging the next tile's first-run
     # entries with asynchronous copies (0: the first run loads from the table; jit.prefetch_layout)
     prefetch_kb: int = 0
+    # per run (first step): the 2^R local offsets; per step: parity table of those offsets
+    run_off: dict = field(default_factory=dict)
+    step_ptab: dict = field(default_factory=dict)
     spans: list = field(default_factory=list)      # (first, count) per group
     universe: list = field(default_factory=list)   # |U| per group
     tiles: list = field(default_factory=list)      # tile count per group
@@ -110,6 +113,8 @@ class FusedPlan:
         """The library kernels (register runs where the groups have them)."""
         if self.fp64:
             raise ValueError("the library's fused kernels store complex64 tables")
+        if any(int(v) & 16 for v in self.groups["variant"]):
+            raise ValueError("register runs of dimension 5 run in the plan-specialised kernels only")
         if self.tile_runs is not None:
             return lib.dcs_fused_runs(table, self.dsteps.ctypes.data, len(self.dsteps), self.groups.ctypes.data,
                                       len(self.groups), self.tile_steps.ctypes.data, self.tile_runs.ctypes.data,
@@ -306,8 +311,19 @@ def _run_vectors(st, kind, ts, tbit):
     return [], 0
 
 
-def _plan_runs(steps, first, count, tsteps, truns, dim, R, tbit, slot_of, keep_bit0=False):
-    """Split a group's steps into register runs of local dimension R; False if a step does not fit."""
+def run_dim(variant):
+    """Local dimension R of a group's register runs from its variant bits: bit 4 (generated
+    kernels only) R = 5, else bit 3 R = 4, else 3."""
+    return 5 if variant & 16 else (4 if variant & 8 else 3)
+
+
+def _plan_runs(steps, first, count, tsteps, truns, dim, R, tbit, slot_of, keep_bit0=False, run_off=None,
+               step_ptab=None):
+    """Split a group's steps into register runs of local dimension R; False if a step does not fit.
+
+    The 2^R local offsets of each run go to run_off[first step] and each step's parity table of
+    those offsets to step_ptab[step]; the library's fixed-size records (dcs_tile_run,
+    dcs_tile_step) hold them too where R <= 4."""
     vr = []
     for s in range(first, first + count):
         kind, _ = orbit_kind(steps[s])
@@ -384,7 +400,10 @@ def _plan_runs(steps, first, count, tsteps, truns, dim, R, tbit, slot_of, keep_b
                 if (j >> k) & 1:
                     o ^= basis[k][0]
             offs.append(o)
-            tr["off"][j] = o
+            if R <= 4:
+                tr["off"][j] = o
+        if run_off is not None:
+            run_off[s0] = offs
         for i in range(n):
             ts = tsteps[s0 + i]
             act = slot_mask(steps[s0 + i].active_in)
@@ -394,17 +413,24 @@ def _plan_runs(steps, first, count, tsteps, truns, dim, R, tbit, slot_of, keep_b
             ts["rk1"], ts["rk2"] = loc[0], loc[1]
             ts["rmix"] = vr[s0 + i - first][1]
             tb = int(ts["tbeta"])
-            ts["ptab"] = sum((bin(o & tb).count("1") & 1) << j for j, o in enumerate(offs))
+            ptab = sum((bin(o & tb).count("1") & 1) << j for j, o in enumerate(offs))
+            if R <= 4:
+                ts["ptab"] = ptab
+            if step_ptab is not None:
+                step_ptab[s0 + i] = ptab
             ts["run_len"] = n if i == 0 else 0
     return True
 
 
 def build_fused_plan(plan, max_dim=13, low=4, max_steps=MAX_GROUP_STEPS, max_extra=1, spans=None, variant=0,
-                     pairs=False, grouping="greedy", group_cost=1 << 30, fp64=False, prefetch_kb=0):
+                     pairs=False, grouping="greedy", group_cost=1 << 30, fp64=False, prefetch_kb=0,
+                     group_variant=None):
     """grouping: "greedy" (group_steps) or "bytes" (group_steps_min_bytes, `group_cost` bytes
     charged per group).  fp64: the plan runs on a complex128 table (plan-specialised register
     runs only, see jit.py).  prefetch_kb: staging of the next tile's first-run entries in the
-    generated kernels (jit.prefetch_layout)."""
+    generated kernels (jit.prefetch_layout).  group_variant: {group: variant} for single groups
+    (variant bit 4, register runs of dimension 5, falls back to dimension 4 where a run does not
+    fit)."""
     steps = plan.steps
     if spans is None:
         if grouping == "bytes":
@@ -415,7 +441,8 @@ def build_fused_plan(plan, max_dim=13, low=4, max_steps=MAX_GROUP_STEPS, max_ext
             raise ValueError(f"grouping {grouping!r}")
     groups = np.zeros(len(spans), dtype=_lib.GROUP_DTYPE)
     tsteps = np.zeros(len(steps), dtype=_lib.TILE_STEP_DTYPE)
-    truns = np.zeros(len(steps), dtype=_lib.TILE_RUN_DTYPE) if variant & 4 else None
+    runs_any = variant & 4 or any(int(v) & 4 for v in (group_variant or {}).values())
+    truns = np.zeros(len(steps), dtype=_lib.TILE_RUN_DTYPE) if runs_any else None
     fp = FusedPlan(groups=groups, tile_steps=tsteps, dsteps=device_steps(steps), spans=list(spans), tile_runs=truns,
                    coset_pairs=bool(pairs and variant & 4), fp64=bool(fp64), prefetch_kb=int(prefetch_kb))
     for gi, (first, count) in enumerate(spans):
@@ -486,7 +513,8 @@ def build_fused_plan(plan, max_dim=13, low=4, max_steps=MAX_GROUP_STEPS, max_ext
         g["first"], g["count"], g["tile_dim"], g["low_bits"] = first, count, dim, l
         g["coset_m"], g["ncoset_runs"], g["step_tile_off"] = bin(cmask).count("1"), len(runs), first
         g["out_mask"] = slot_mask(steps[first + count - 1].active_out)
-        g["variant"] = variant
+        gvar = int((group_variant or {}).get(gi, variant))
+        g["variant"] = gvar
         for i, b in enumerate(basis):
             g["basis"][i] = b
         for r, (src, dst, ln) in enumerate(runs):
@@ -541,12 +569,18 @@ def build_fused_plan(plan, max_dim=13, low=4, max_steps=MAX_GROUP_STEPS, max_ext
             ts["mhi"] = sum(1 << b for b in free[8:])  # 256 threads: index bits >= 8
             ts["rb1"] = max(st.pivot_a if kind == 1 else st.pivot, 0)  # role slot(s), for checking
             ts["rb2"] = max(st.pivot_a, 0) if kind == 6 else 0
-        if variant & 4:
-            R = 4 if variant & 8 else 3
+        if gvar & 4:
             slot_of = lambda q: q if q < l else pivots[q - l]
             # packed plans (bit 1) keep tile bit 0 out of the runs: it is the lane bit
-            if not _plan_runs(steps, first, count, tsteps, truns, dim, R, tbit, slot_of, keep_bit0=bool(variant & 2)):
-                g["variant"] = variant & ~12  # this group keeps the one-step-per-round-trip kernel
+            ok = _plan_runs(steps, first, count, tsteps, truns, dim, run_dim(gvar), tbit, slot_of,
+                            keep_bit0=bool(gvar & 2), run_off=fp.run_off, step_ptab=fp.step_ptab)
+            if not ok and gvar & 16:  # dimension 5 does not fit: dimension 4
+                gvar = (gvar & ~16) | 8
+                g["variant"] = gvar
+                ok = _plan_runs(steps, first, count, tsteps, truns, dim, 4, tbit, slot_of,
+                                keep_bit0=bool(gvar & 2), run_off=fp.run_off, step_ptab=fp.step_ptab)
+            if not ok:
+                g["variant"] = gvar & ~28  # this group keeps the one-step-per-round-trip kernel
         elif pairs:
             _pair_steps(steps, first, count, tsteps, dim, tilepos_of=lambda q: (q < l or q in pivots),
                         tbit=tbit, U=U)

@@ -19,6 +19,7 @@ from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 from . import _lib
+from .fused import run_dim
 
 HERE = Path(__file__).resolve().parent
 HEADER = HERE / "csrc" / "runs_jit.cuh"
@@ -32,8 +33,7 @@ def _u64(x):
     return f"{int(x) & 0xFFFFFFFFFFFFFFFF}ull"
 
 
-def _beff(kind, ts, R):
-    ptab = int(ts["ptab"])
+def _beff(kind, ts, R, ptab):
     bl = sum(((ptab >> (1 << k)) & 1) << k for k in range(R))
     own = 0
     if kind in ONE_VECTOR:
@@ -113,7 +113,7 @@ def prefetch_layout(fp, gi, threads=256, kb=None):
     if not int(g["variant"]) & 4 or packable(fp, gi):
         return None
     fp64 = bool(getattr(fp, "fp64", False))
-    R = 4 if int(g["variant"]) & 8 else 3
+    R = run_dim(int(g["variant"]))
     first = int(g["first"])
     TD, LOW = int(g["tile_dim"]), int(g["low_bits"])
     T = 1 << TD
@@ -130,11 +130,11 @@ def prefetch_layout(fp, gi, threads=256, kb=None):
     free = [b for b in range(TD) if b not in ins]
     if any(gaddr(1 << f) & in_inact for f in free):
         return None
-    G = [gaddr(int(tr["off"][j])) for j in range(1 << R)]
+    G = [gaddr(int(fp.run_off[first + s][j])) for j in range(1 << R)]
     live = [j for j in range(1 << R) if not G[j] & in_inact]
     if not live:
         return None
-    k0 = None if fp64 else next((k for k in range(R) if int(tr["off"][1 << k]) == 1), None)
+    k0 = None if fp64 else next((k for k in range(R) if int(fp.run_off[first + s][1 << k]) == 1), None)
     pair_in = LOW >= 1 and (in_mask & 1)
     if k0 is not None and pair_in:
         units = [(j, j | (1 << k0)) for j in live if not (j >> k0) & 1]
@@ -213,7 +213,7 @@ def group_source(plan, fp, gi, minb=3, threads=256, kb=None):
     direct = bool(getattr(fp, "direct_io", True)) and _direct_ok(fp, gi)
     if fp64 and not direct:
         raise ValueError(f"group {gi}: the complex128 group kernels read and write the table directly")
-    R = 4 if int(g["variant"]) & 8 else 3
+    R = run_dim(int(g["variant"]))
     first, count = int(g["first"]), int(g["count"])
     TD, LOW = int(g["tile_dim"]), int(g["low_bits"])
     T = 1 << TD
@@ -353,8 +353,8 @@ def group_source(plan, fp, gi, minb=3, threads=256, kb=None):
             """Byte offset of a local entry: t0 ^ o, written t0 + o when o has no bit that t0 can
             have (then the offset is an immediate of the shared-memory access)."""
             return f"(t0{c} + {o}u)" if not (o & free3) else f"(t0{c} ^ {o}u)"
-        offs = [int(tr["off"][j]) << esh for j in range(1 << R)]
-        G = [gaddr(int(tr["off"][j])) for j in range(1 << R)]
+        offs = [int(fp.run_off[first + s][j]) << esh for j in range(1 << R)]
+        G = [gaddr(int(fp.run_off[first + s][j])) for j in range(1 << R)]
         L.append(f"        // run: steps {first + s}..{first + s + n - 1}, {NB} cosets of {1 << R} entries"
                  f"{', from the table' if src_g else ''}{', to the table' if dst_g else ''}")
         if not direct:
@@ -369,7 +369,7 @@ def group_source(plan, fp, gi, minb=3, threads=256, kb=None):
             L.append("                jit::cp_async_wait_all();  // this thread's staged entries of this tile")
         # local bit k0 with basis vector e_0: entries j and j | 2^k0 are one aligned 16-byte word
         # (complex64 entries only)
-        k0 = None if fp64 else next((k for k in range(R) if int(tr["off"][1 << k]) == 1), None)
+        k0 = None if fp64 else next((k for k in range(R) if int(fp.run_off[first + s][1 << k]) == 1), None)
         pairs = [(j, j | (1 << k0)) for j in range(1 << R) if not (j >> k0) & 1] if k0 is not None else None
         cos = ["a", "b"] if coset_pairs and niter % 2 == 0 else ["a"]
         L.append("#pragma unroll 1")
@@ -430,7 +430,7 @@ def group_source(plan, fp, gi, minb=3, threads=256, kb=None):
             si = s + i
             st = fp.tile_steps[first + si]
             kind = int(fp.dsteps[first + si]["kind"])
-            B = _beff(kind, st, R)
+            B = _beff(kind, st, R, fp.step_ptab[first + si])
             dead = int(st["rdead"])
             sk, ska = int(st["sK"]) & 1, int(st["sKa"]) & 1
             k1, k2, mix = int(st["rk1"]), int(st["rk2"]), int(st["rmix"])
@@ -495,11 +495,11 @@ def packable(fp, gi):
     run of the group has tile bit 0 in its space or among its coset zero bits."""
     g = fp.groups[gi]
     v = int(g["variant"])
-    if getattr(fp, "fp64", False):  # the packed bodies are FP32x2
+    if getattr(fp, "fp64", False) or v & 16:  # the packed bodies are FP32x2, of runs up to dimension 4
         return False
     if not (v & 2 and v & 4) or not getattr(fp, "direct_io", True) or not _direct_ok(fp, gi):
         return False
-    R = 4 if v & 8 else 3
+    R = run_dim(v)
     first = int(g["first"])
     if int(g["tile_dim"]) < 1:
         return False
@@ -508,7 +508,7 @@ def packable(fp, gi):
         nins = int(tr["nins"])
         if nins >= int(g["tile_dim"]) or (nins and int(tr["ins"][0]) == 0):
             return False
-        if any(int(tr["off"][j]) & 1 for j in range(1 << R)):
+        if any(int(fp.run_off[first + s][j]) & 1 for j in range(1 << R)):
             return False
     return True
 
@@ -519,7 +519,7 @@ def _packed_source(fp, gi, minb):
     (re_2i, re_2i+1, im_2i, im_2i+1) per entry pair, one 16-byte word per local entry of a pair;
     the first run reads the table and the last one writes it (direct I/O)."""
     g = fp.groups[gi]
-    R = 4 if int(g["variant"]) & 8 else 3
+    R = run_dim(int(g["variant"]))
     first, count = int(g["first"]), int(g["count"])
     TD, LOW = int(g["tile_dim"]), int(g["low_bits"])
     T = 1 << TD
@@ -576,8 +576,8 @@ def _packed_source(fp, gi, minb):
         niter = NB2 >> 8 if NB2 > 256 else 1
         mhi = int(tr["mhi"])
         mhi3 = (mhi & (mhi - 1)) << 3  # tile bit 0 is the lane bit
-        offs = [int(tr["off"][j]) << 3 for j in range(1 << R)]
-        G = [gaddr(int(tr["off"][j])) for j in range(1 << R)]
+        offs = [int(fp.run_off[first + s][j]) << 3 for j in range(1 << R)]
+        G = [gaddr(int(fp.run_off[first + s][j])) for j in range(1 << R)]
         L.append(f"        // run: steps {first + s}..{first + s + n - 1}, {NB2} coset pairs of {1 << R} entries"
                  f"{', from the table' if src_g else ''}{', to the table' if dst_g else ''}")
         L.append(f"            if ((int)threadIdx.x < {NB2}) {{")
@@ -612,7 +612,7 @@ def _packed_source(fp, gi, minb):
             si = s + i
             st = fp.tile_steps[first + si]
             kind = int(fp.dsteps[first + si]["kind"])
-            B = _beff(kind, st, R)
+            B = _beff(kind, st, R, fp.step_ptab[first + si])
             dead = int(st["rdead"])
             sk, ska = int(st["sK"]) & 1, int(st["sKa"]) & 1
             k1, k2, mix = int(st["rk1"]), int(st["rk2"]), int(st["rmix"])

@@ -179,3 +179,22 @@ def test_block_is_copied_to_host_as_the_reference_worker_does(golden):
     host = np.asarray(v)
     np.testing.assert_array_equal(host, v.cpu().numpy())
     assert draw_checked(host, rec["draw_uniform"]) == draw_checked(v, rec["draw_uniform"])
+
+
+@pytest.mark.parametrize("name", ["small", "c2"])
+def test_dimension5_runs_and_group_tuning_are_bit_identical(golden, name):
+    """Register runs of dimension 5 (variant bit 4) and the per-group kernel choice of
+    autotune.tune_groups compute the same blocks, bit for bit, as the dimension-4 kernels."""
+    case, arrays = golden(name)
+    eng = _engine(case, arrays, np.complex64, "fused", jit_shape=True)
+    xs = [_x(r) for r in case["protocol"]["records"]]
+    want = [eng.block(x)[0].cpu().numpy() for x in xs]
+    eng.set_fused_config(variant=28)
+    assert any(int(v) & 16 for v in eng.fplan.groups["variant"])
+    for x, w in zip(xs, want):
+        assert np.array_equal(eng.block(x)[0].cpu().numpy(), w)
+    eng.set_fused_config(variant=12)
+    rep = eng.tune_groups(save=False, repeats=1)
+    assert set(rep["group_cfg"]) == {str(g) for g in range(len(eng.fplan.groups))}
+    for x, w in zip(xs, want):
+        assert np.array_equal(eng.block(x)[0].cpu().numpy(), w)

@@ -58,3 +58,28 @@ def test_fp64_and_staged_kernels_compile(golden, name):
     src = units[0][0]
     assert src.count("cp_async_wait_all") == len(staged)
     assert jit.compile_source(lib, src)[:4] == b"\x7fELF"
+
+
+@pytest.mark.parametrize("name", ["small", "c2"])
+def test_dimension5_runs_plan_and_compile(golden, name):
+    """Variant bit 4: register runs of dimension 5 (32 local offsets per run, kept beside the
+    library's 16-entry records), falling back to dimension 4 per group; the kernels compile, and
+    the library refuses such plans."""
+    from dcs245_classical_sampling_b200.fused import run_dim
+    case, arrays = golden(name)
+    bp = P.build_block_plan(arrays["graph"], arrays["unitaries"], case["n"], case["order"],
+                            case["parity_operations"], case["open_vertices"])
+    fp = build_fused_plan(bp, max_dim=13, low=3, variant=28, grouping="bytes")
+    dims = [run_dim(int(v)) for v in fp.groups["variant"] if int(v) & 4]
+    assert 5 in dims
+    for gi, g in enumerate(fp.groups):
+        if int(g["variant"]) & 4:
+            for s, n in jit._group_runs(fp, gi):
+                assert len(fp.run_off[int(g["first"]) + s]) == 1 << run_dim(int(g["variant"]))
+    one = build_fused_plan(bp, max_dim=13, low=3, variant=12, grouping="bytes", group_variant={1: 28})
+    assert all(run_dim(int(v)) <= 4 for gi, v in enumerate(one.groups["variant"]) if gi != 1)
+    lib = _lib.load()
+    for src, _ in jit.plan_sources(bp, fp, minb=2, parts=1):
+        assert jit.compile_source(lib, src)[:4] == b"\x7fELF"
+    with pytest.raises(ValueError):
+        fp.launch_library(lib, 0, 0, 0, 1, 0, 0, None)
