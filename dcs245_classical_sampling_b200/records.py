@@ -167,7 +167,8 @@ def write_rows(engine, reference, records, audit_ids, outdir, *, worker_id, mani
             host = v.cpu().numpy()
             del v
             t = time.perf_counter()
-            draw = draw_checked(host, record["draw_uniform"])
+            # NumPy's sequential CDF values: the row's grid count is computed from them
+            draw = draw_checked(host, record["draw_uniform"], exact_cdf=True)
             cdf_seconds = time.perf_counter() - t
             row = sample_row(record, draw, contraction, worker_id=worker_id, manifest_sha256=manifest_sha256,
                              protocol_sha256=protocol_sha256, n=n, free=free, ring=ring, audit_ids=audit_ids,
