@@ -866,6 +866,8 @@ def profile_case(argv):
                     help="generated kernels: KiB per CTA staging the next tile's first-run entries")
     ap.add_argument("--minb", type=int, default=None, help="generated kernels: CTAs per SM for the registers")
     ap.add_argument("--fp64", action="store_true", help="complex128 table, FP64 generated kernels (the audits)")
+    ap.add_argument("--kernel-cfg", default=None,
+                    help="generated kernels of every group as MINB/STAGING_KB/RUN_DIM, e.g. 2/16/5")
     ap.add_argument("--storage", default=None, choices=["float16"],
                     help="binary16 tables with FP64 arithmetic (device mode)")
     a = ap.parse_args(argv)
@@ -900,11 +902,15 @@ def profile_case(argv):
     stream = torch.cuda.current_stream(dev)
     sub = P.BlockPlan(**{**bp.__dict__, "steps": steps})
     if a.mode == "fused":
-        fp = build_fused_plan(sub, max_dim=a.max_dim, low=a.low, variant=a.variant, pairs=a.pairs,
-                              grouping=a.grouping, fp64=a.fp64, prefetch_kb=a.prefetch_kb)
+        variant, minb, kb = a.variant, a.minb, a.prefetch_kb
+        if a.kernel_cfg:
+            minb, kb, rdim = (int(x) for x in a.kernel_cfg.split("/"))
+            variant = (variant | 16) if rdim == 5 else (variant & ~16)
+        fp = build_fused_plan(sub, max_dim=a.max_dim, low=a.low, variant=variant, pairs=a.pairs,
+                              grouping=a.grouping, fp64=a.fp64, prefetch_kb=kb)
         if a.jit:
             from dcs245_classical_sampling_b200.jit import JitPlan
-            fp.jit = JitPlan(sub, fp, lib, minb=a.minb)
+            fp.jit = JitPlan(sub, fp, lib, minb=minb)
         nmax = len(fp.groups)
     else:
         dsteps = device_steps(steps)
