@@ -47,7 +47,11 @@ DRAW_DTYPE = np.dtype([
     ("selected_weight", "<f8"), ("cdf_lower", "<f8"), ("cdf_upper", "<f8"), ("cdf_lower_exact", "<f8"),
     ("cdf_upper_exact", "<f8"), ("uniform", "<f8"), ("tv53", "<f8"), ("weight_l2", "<f8"),
 ])
-STRUCTS = [STEP_DTYPE, PARAM_DTYPE, SCALE_DTYPE, GROUP_DTYPE, TILE_STEP_DTYPE, DRAW_DTYPE, TILE_RUN_DTYPE]
+GATHER_STEP_DTYPE = np.dtype([("beta", "<u8"), ("table_off", "<u8"), ("combo_off", "<u8"), ("r_in", "<i4"),
+                              ("r_out", "<i4"), ("nbytes", "<i4"), ("ncombos", "<i4"), ("free_", "<i4"),
+                              ("pad", "<i4")])
+STRUCTS = [STEP_DTYPE, PARAM_DTYPE, SCALE_DTYPE, GROUP_DTYPE, TILE_STEP_DTYPE, DRAW_DTYPE, TILE_RUN_DTYPE,
+           GATHER_STEP_DTYPE]
 
 _P = ctypes.c_void_p
 _I = ctypes.c_int
@@ -70,6 +74,7 @@ SIGNATURES = {
     "dcs_accumulate_batched": (_I, [_I, _P, _U64, _I, _P, _I, _P, _P, _P, _P, _I, _D, _P, _P, _U64, _P, _I, _I,
                                     _P]),
     "dcs_block_tail": (_I, [_P, _I, _P, _P, _I, _P]),
+    "dcs_gather_steps": (_I, [_I, _P, _P, _U64, _P, _P, _P, _U64, _I, _I, _P, _U64, _P, _I, _P]),
     "dcs_draw_scratch_bytes": (ctypes.c_size_t, [_I, _I]),
     "dcs_draw": (_I, [_P, _I, _I, _P, _P, _P, _P]),
     "dcs_draw_ex": (_I, [_P, _I, _I, _P, ctypes.c_uint, _P, _P, _P]),

@@ -17,7 +17,7 @@ CSRC = PKG / "csrc"
 INCLUDE = REPO / "include"
 LIB = PKG / "libdcs245.so"
 SOURCES = ["abi.cu", "step.cu", "fused.cu", "runs.cu", "runs_r4.cu", "runs_packed.cu", "jit.cu", "block.cu",
-           "draw.cu", "serve.cu", "planner.cu"]
+           "draw.cu", "serve.cu", "planner.cu", "gather.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

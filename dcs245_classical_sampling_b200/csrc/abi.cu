@@ -55,6 +55,7 @@ extern "C" size_t dcs_struct_size(int which) {
         case 4: return sizeof(dcs_tile_step);
         case 5: return sizeof(dcs_draw_result);
         case 6: return sizeof(dcs_tile_run);
+        case 7: return sizeof(dcs_gather_step);
     }
     return 0;
 }

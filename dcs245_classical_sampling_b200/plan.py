@@ -420,3 +420,137 @@ def build_block_plan(graph, unitaries, n, order, parity_operations, open_vertice
 def step_bytes(plan, elem_bytes=8):
     """Algorithmic HBM bytes of one slice: sum over steps of (2^|in| + 2^|out|) entries."""
     return sum(((1 << len(s.active_in)) + (1 << len(s.active_out))) * elem_bytes for s in plan.steps)
+
+
+# ---------------------------------------------------------------------------------------------
+# Gather form of the plan (source/dcs_rankwidth/scan_plan.py:58-105): the environment after step
+# j is E'[c'] = sum over p in L c' + span(kernel) of E[p & mask_in] f_v(p >> r_in) sign, with two
+# tables.  It is the plan of the reference's ConditionalBlockGPU (its two-buffer executor).
+
+@dataclass
+class GatherStep:
+    v: int
+    free: bool
+    r_in: int
+    r_out: int
+    beta: int
+    Lcols: list
+    kernel: list
+
+
+def _reduce_against(vec, basis, pivots):
+    """(residual, coefficient bits) of vec reduced against basis vectors with the given pivots,
+    in insertion order (scan_plan.py:35-42)."""
+    coef = 0
+    for k, (b, p) in enumerate(zip(basis, pivots)):
+        if (vec >> p) & 1:
+            vec ^= b
+            coef |= 1 << k
+    return vec, coef
+
+
+def make_gather_plan(N, edges, order, fixed=frozenset()):
+    """Gather plan of every position (scan_plan.py:58-105) -> (steps, rank profile)."""
+    fut = future_masks(N, edges, order)
+    basis = []
+    steps, profile = [], []
+    for j in range(N):
+        v = order[j]
+        free = v not in fixed
+        beta = 0
+        for i, b in enumerate(basis):
+            beta |= ((b >> j) & 1) << i
+        ws = [b & ~(1 << j) for b in basis] + ([fut[j]] if free else [])
+        nb, piv, mcols = [], [], []
+        for wv in ws:  # the new basis and each column's coordinates in it
+            res, coef = _reduce_against(wv, nb, piv)
+            if res:
+                piv.append((res & -res).bit_length() - 1)
+                nb.append(res)
+                coef |= 1 << (len(nb) - 1)
+            mcols.append(coef)
+        r_out = len(nb)
+        first_col = {}  # leading coordinate k -> first column that has it
+        for i, m in enumerate(mcols):
+            if m and (m.bit_length() - 1) not in first_col:
+                first_col[m.bit_length() - 1] = i
+        L = [0] * r_out  # right inverse: M L[k] = e_k
+        for k in range(r_out):
+            i = first_col[k]
+            m = mcols[i]
+            col = 1 << i
+            for l in range(k):
+                if (m >> l) & 1:
+                    col ^= L[l]
+            L[k] = col
+        pivot_cols = set(first_col.values())
+        kernel = []
+        for i, m in enumerate(mcols):
+            if i in pivot_cols:
+                continue
+            kv = 1 << i
+            for k in range(r_out):
+                if (m >> k) & 1:
+                    kv ^= L[k]
+            kernel.append(kv)
+        steps.append(GatherStep(v=v, free=free, r_in=len(basis), r_out=r_out, beta=beta, Lcols=L, kernel=kernel))
+        profile.append(r_out)
+        basis = nb
+    return steps, profile
+
+
+def gather_byte_tables(cols, nbits):
+    """Byte-wise XOR tables of c -> XOR_{i: c_i = 1} cols[i] (scan_plan.py:133-145): (nb, 256) uint64."""
+    nb = max(1, (nbits + 7) // 8)
+    T = np.zeros((nb, 256), dtype=np.uint64)
+    for b in range(nb):
+        for val in range(256):
+            acc = 0
+            for t in range(8):
+                i = 8 * b + t
+                if i < nbits and (val >> t) & 1:
+                    acc ^= cols[i]
+            T[b, val] = acc
+    return T
+
+
+def kernel_combos(kernel):
+    """Every XOR combination of the kernel vectors (scan_plan.py:148-152)."""
+    combos = [0]
+    for kv in kernel:
+        combos = combos + [c ^ kv for c in combos]
+    return combos
+
+
+@dataclass
+class GatherPlan:
+    steps: list
+    rank_profile: list
+    tables: list
+    combos: list
+    rmax: int
+    work: int
+    terminal_basis: list
+
+
+def build_gather_plan(bp):
+    """The gather plan of a block plan's reduced graph (conditional_block_gpu.py:47-64): steps up
+    to `stop`, byte tables, kernel combinations, rmax, work and the terminal syndrome basis."""
+    all_steps, profile = make_gather_plan(bp.N, bp.edges, bp.order, bp.fixed)
+    steps = all_steps[:bp.stop]
+    tables = [gather_byte_tables(st.Lcols, st.r_out) for st in steps]
+    combos = [np.asarray(kernel_combos(st.kernel), np.uint64) for st in steps]
+    rmax = max([1] + [max(s.r_in, s.r_out) for s in steps])
+    work = sum((1 << s.r_out) * (1 << len(s.kernel)) for s in steps)
+    basis = []
+    for j, st in enumerate(steps):
+        ws = [b & ~(1 << j) for b in basis] + ([bp.fut[j]] if st.free else [])
+        nb, piv = [], []
+        for old in ws:
+            res, _ = _reduce_against(old, nb, piv)
+            if res:
+                piv.append((res & -res).bit_length() - 1)
+                nb.append(res)
+        basis = nb
+    return GatherPlan(steps=steps, rank_profile=profile, tables=tables, combos=combos, rmax=rmax, work=work,
+                      terminal_basis=[b >> bp.stop for b in basis])

@@ -178,6 +178,21 @@ typedef struct dcs_tile_run {
     uint16_t off[16];       /* tile offsets of the 2^r local entries */
 } dcs_tile_run;
 
+/* One step of the gather form of the plan (the reference's ConditionalBlockGPU, the plan of
+ * source/dcs_rankwidth/scan_plan.py:58-105): output c' of 2^r_out sums, over the ncombos kernel
+ * combinations q = L c' ^ combo, E[q mod 2^r_in] times f(y) with y = bit r_in of q (free step)
+ * or the fixed value.  L c' is read byte by byte from an nbytes x 256 table. */
+typedef struct dcs_gather_step {
+    uint64_t beta;          /* sign functional on the input coordinates */
+    uint64_t table_off;     /* offset (64-bit words) of the step's byte table in `words` */
+    uint64_t combo_off;     /* offset (64-bit words) of its kernel combinations in `words` */
+    int32_t r_in, r_out;    /* input and output ranks */
+    int32_t nbytes;         /* bytes of c' read through the table: ceil(r_out / 8), at least 1 */
+    int32_t ncombos;        /* 2^(kernel dimension), at most 64 */
+    int32_t free_;          /* 1: y is bit r_in of q; 0: y is the step's fixed value */
+    int32_t pad;
+} dcs_gather_step;
+
 /* Result of one draw (device-side struct; the host copies it back). */
 typedef struct dcs_draw_result {
     int64_t index;             /* A_index */
@@ -200,7 +215,7 @@ const char *dcs_last_error(void);
 int dcs_sm_count(void);
 /* sizeof of the ABI structs, so that bindings can check their layouts:
  * 0 dcs_step, 1 dcs_param, 2 dcs_scale, 3 dcs_group, 4 dcs_tile_step, 5 dcs_draw_result,
- * 6 dcs_tile_run. */
+ * 6 dcs_tile_run, 7 dcs_gather_step. */
 size_t dcs_struct_size(int which);
 
 /* Host planner (no device work): the GF(2) cut rank of every proper prefix of a vertex order on
@@ -232,6 +247,20 @@ int dcs_slice_steps(int dtype, void *table, const dcs_step *steps, const dcs_par
 int dcs_slice_steps_batched(int dtype, void *table, uint64_t table_stride, const dcs_step *steps,
                             const dcs_param *params, uint64_t param_stride, int nsteps, int first, int count,
                             uint64_t *maxbits, dcs_scale *scale, int nitems, void *stream);
+
+/* Gather-form steps [s0, s0 + count) on two tables of nitems work items each (item i at
+ * i * stride entries): step s0 reads table_a and writes table_b, the next reads table_b, and so on,
+ * so the result is in table_b for odd count.  Replaces the host loop of the reference's
+ * ConditionalBlockGPU._prefix (sampling/conditional_block_gpu.py:92-126) and its kernel
+ * scan_step_scaled (dcs_rankwidth/gpu_kernel.py:58-103): FP64 sums, writes scaled by 2^-e with e
+ * from maxbits[s] (the previous step's max |x|^2, IEEE bits of the storage precision; maxbits[s0]
+ * = bits of 1.0 before the first step), max |x|^2 into maxbits[s + 1], e ln 2 into scale->logscale,
+ * no host synchronisation.  dtype DCS_C64 or DCS_C128; steps: host array; words, params,
+ * maxbits (maxbits_stride words per item), scale: device. */
+int dcs_gather_steps(int dtype, void *table_a, void *table_b, uint64_t stride, const dcs_gather_step *steps,
+                     const uint64_t *words, const dcs_param *params, uint64_t param_stride, int s0, int count,
+                     unsigned long long *maxbits, uint64_t maxbits_stride, dcs_scale *scale, int nitems,
+                     void *stream);
 
 /* Fused passes over coset tiles (complex64 tables): groups [g0, g0+ng) of a fused plan.
  * steps, groups and tile_steps are host arrays; params, maxbits (ngroups+1 words) and scale

@@ -107,6 +107,71 @@ class OracleEngine(InplaceConditionalBlockGPU):
         return env, ls, offset >> self.stop
 
 
+class GatherEngine:
+    """The reference's gather engine (sampling/conditional_block_gpu.py:25-177), unmodified, with
+    NumPy buffers and its per-step kernel served by the reference's Numba gather step
+    (dcs_rankwidth/scan_kernel.py:26-65); complex128."""
+
+    def __new__(cls, *args):
+        from conditional_block_gpu import ConditionalBlockGPU
+        from dcs_rankwidth import scan_kernel
+
+        class _Engine(ConditionalBlockGPU):
+            def alloc(self, dtype=np.complex128, device=0):
+                self.cp = sys.modules["cupy"]
+                self.use_fp64 = True
+                size = 1 << self.rmax
+                self.d_buf = [np.zeros(size, np.complex128), np.zeros(size, np.complex128)]
+                self.d_max = np.zeros(1, np.uint64)
+                self.d_tables = [T.reshape(-1) for T in self.tables]
+                self.d_combos = [np.asarray(c, np.uint64) for c in self.combos]
+                self._grid = self._block = None
+                self._kernel = self._numba_step
+                ids = np.arange(1 << self.terminal_rank, dtype=np.uint64)
+                self.d_syndrome_map = np.zeros_like(ids)
+                for j, b in enumerate(self.terminal_basis):
+                    self.d_syndrome_map ^= ((ids >> np.uint64(j)) & np.uint64(1)) * np.uint64(b)
+                self.d_phase = np.ones(1 << len(self.open_full), np.float64)
+                ids = np.arange(len(self.d_phase), dtype=np.uint64)
+                for a, b in self.open_edges:
+                    self.d_phase *= 1 - 2 * (((ids >> np.uint64(a)) & (ids >> np.uint64(b))
+                                              & np.uint64(1)).astype(np.float64))
+
+            def _numba_step(self, grid, block, args):
+                (A, B, n_out, T, nbytes, combos, _nc, r_in, beta, ov, free, f0r, f0i, f1r, f1i, y, scale,
+                 d_max) = args
+                n = int(n_out)
+                scan_kernel._step(A, B, n, T.reshape(-1, 256), int(nbytes), combos, int(r_in), np.uint64(beta),
+                                  np.uint64(ov), int(free), complex(f0r, f0i), complex(f1r, f1i), int(y))
+                scan_kernel._scale(B, n, float(scale))
+                m = scan_kernel._maxabs(B, n)
+                d_max[0] = np.array([m * m], np.float64).view(np.uint64)[0]
+
+        return _Engine(*args)
+
+
+def gather_case(name):
+    """The reference gather engine's plan and blocks for a golden case's prefixes, beside the in-place
+    engine's blocks of the same case (both are exact contractions of the same block)."""
+    case = json.loads((HERE / f"{name}.json").read_text())
+    arrays = dict(np.load(HERE / f"{name}.npz"))
+    eng = GatherEngine(arrays["graph"], arrays["unitaries"], case["n"], case["order"],
+                       [tuple(op) for op in case["parity_operations"]], case["open_vertices"])
+    out = {"name": name, "rmax": int(eng.rmax), "work": int(eng.work), "stop": int(eng.stop),
+           "terminal_basis": [int(b) for b in eng.terminal_basis],
+           "rank_profile": [int(r) for r in eng.rank_profile],
+           "steps": [{"v": int(st.v), "free": bool(st.free), "r_in": int(st.r_in), "r_out": int(st.r_out),
+                      "beta": int(st.beta), "Lcols": [int(c) for c in st.Lcols], "kernel": [int(k) for k in st.kernel]}
+                     for st in eng.steps], "blocks_rel_l2_vs_inplace": []}
+    eng.alloc()
+    for rec in case["protocol"]["records"]:
+        x = np.array([int(c) for c in rec["input_data_bits"]], np.uint8)
+        v, meta = eng.block(x)
+        want = arrays[f"block_{rec['sample_id']}"]
+        out["blocks_rel_l2_vs_inplace"].append(float(np.linalg.norm(np.asarray(v) - want) / np.linalg.norm(want)))
+    return out
+
+
 def plan_json(engine):
     steps = []
     for st in engine.inplace_steps:
@@ -271,7 +336,7 @@ CASES = {
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--cases", nargs="*", default=list(CASES) + ["sampler", "chooser"])
+    ap.add_argument("--cases", nargs="*", default=list(CASES) + ["sampler", "chooser", "gather"])
     args = ap.parse_args()
     for name in args.cases:
         if name == "sampler":
@@ -279,6 +344,11 @@ def main():
             continue
         if name == "chooser":
             (HERE / "chooser.json").write_text(json.dumps(chooser_case(), indent=1))
+            continue
+        if name == "gather":
+            g = {c: gather_case(c) for c in ("c1", "small", "c2")}
+            (HERE / "gather.json").write_text(json.dumps(g, indent=1))
+            print("gather", {c: max(v["blocks_rel_l2_vs_inplace"]) for c, v in g.items()}, flush=True)
             continue
         case, arrays = make_case(name, **CASES[name])
         (HERE / f"{name}.json").write_text(json.dumps(case, indent=1))

@@ -109,3 +109,25 @@ def test_native_cut_ranks_equal_gf2_rank_of_each_cut():
             assert list(got) == want
     with pytest.raises(Exception):
         P.prefix_cut_ranks(np.zeros((3, 3), np.uint8), [0, 1, 5])
+
+
+@pytest.mark.parametrize("name", ["c1", "small", "c2"])
+def test_gather_plan_matches_reference(golden, name):
+    """The gather form of the plan (the reference's ConditionalBlockGPU, scan_plan.make_plan):
+    every step's ranks, sign functional, right inverse and kernel, the rank profile, rmax, work
+    and the terminal basis, bit for bit."""
+    from dcs245_classical_sampling_b200.plan import build_block_plan, build_gather_plan
+    case, arrays = golden(name)
+    g = golden("gather")[0][name]
+    bp = build_block_plan(arrays["graph"], arrays["unitaries"], case["n"], case["order"],
+                          case["parity_operations"], case["open_vertices"])
+    gp = build_gather_plan(bp)
+    assert gp.rmax == g["rmax"] and gp.work == g["work"] and bp.stop == g["stop"]
+    assert gp.terminal_basis == g["terminal_basis"]
+    assert gp.rank_profile == g["rank_profile"]
+    assert len(gp.steps) == len(g["steps"])
+    for mine, theirs in zip(gp.steps, g["steps"]):
+        for key in ("v", "free", "r_in", "r_out", "beta", "Lcols", "kernel"):
+            assert getattr(mine, key) == theirs[key], key
+    # the reference's gather blocks equal its in-place blocks (the golden blocks) to rounding
+    assert max(g["blocks_rel_l2_vs_inplace"]) < 1e-14
