@@ -129,8 +129,10 @@ def tune(engine, params_dev, candidates=None, repeats=1, save=True, jit=False):
 
 
 # per-group kernel choices: (CTAs per SM the registers are sized for, KiB staging the next
-# tile's first-run entries (jit.prefetch_layout), local dimension of the register runs)
-GROUP_CANDIDATES = ((3, 0, 4), (3, 8, 4), (2, 0, 4), (2, 16, 4), (2, 32, 4), (2, 0, 5), (2, 16, 5), (2, 32, 5))
+# tile's first-run entries (jit.prefetch_layout), local dimension of the register runs; "4p": of
+# dimension 4 in the packed FP32x2 form where the group's runs leave tile bit 0 free)
+GROUP_CANDIDATES = ((3, 0, 4), (3, 8, 4), (2, 0, 4), (2, 16, 4), (2, 32, 4), (2, 0, 5), (2, 16, 5), (2, 32, 5),
+                    (3, 0, "4p"), (2, 0, "4p"))
 
 
 def _time_groups(engine, fp, jp, params_dev, repeats):
@@ -174,24 +176,26 @@ def tune_groups(engine, params_dev, candidates=GROUP_CANDIDATES, repeats=2, save
         raise ValueError("tune_groups needs the plan-specialised kernels (jit)")
     lib = engine.lib
     threads = engine.fplan.jit.threads
+    from .jit import packable
     base = {k: v for k, v in engine.fused_config.items() if k != "group_variant"}
-    v4 = (int(base["variant"]) & ~16) | 12
-    plans = {4: build_fused_plan(engine.plan, **{**base, "variant": v4}),
-             5: build_fused_plan(engine.plan, **{**base, "variant": v4 | 16})}
+    v4 = (int(base["variant"]) & ~18) | 12
+    variants = {4: v4, 5: v4 | 16, "4p": v4 | 2}
+    plans = {r: build_fused_plan(engine.plan, **{**base, "variant": v}) for r, v in variants.items()
+             if any(c[2] == r for c in candidates)}
     ng = len(plans[4].groups)
     times = {}
     for cand in candidates:
-        minb, kb, r = (int(x) for x in cand)
+        minb, kb, r = int(cand[0]), int(cand[1]), cand[2]
         fp = plans[r]
         jp = JitPlan(engine.plan, fp, lib, minb=minb, threads=threads, group_cfg={gi: (minb, kb) for gi in range(ng)})
         t = _time_groups(engine, fp, jp, params_dev, repeats)
         jp.close()
-        for gi in range(ng):  # a dimension-5 plan group that fell back to 4 is the same kernel: skip
-            if r == 5 and not int(fp.groups[gi]["variant"]) & 16:
+        for gi in range(ng):  # a group that fell back to the dimension-4 scalar kernel is timed there
+            if (r == 5 and not int(fp.groups[gi]["variant"]) & 16) or (r == "4p" and not packable(fp, gi)):
                 t[gi] = float("inf")
         times[(minb, kb, r)] = t
     choice = {gi: min(times, key=lambda c: times[c][gi]) for gi in range(ng)}
-    group_variant = {gi: v4 | 16 for gi, c in choice.items() if c[2] == 5}
+    group_variant = {gi: variants[c[2]] for gi, c in choice.items() if c[2] != 4}
     group_cfg = {gi: (c[0], c[1]) for gi, c in choice.items()}
     engine.fplan.jit.close()
     engine.fused_config = {**base, "group_variant": group_variant}

@@ -193,39 +193,39 @@ struct C2 {
 struct CF {  // a complex factor per lane, with its negated imaginary part
     float2 r, i, ni;
 };
+// The packed bodies are the scalar bodies lane by lane, with the same operations in the same
+// order (so every form of a group computes the same values bit for bit): f * x is
+// fma(f.re, x.re, (-f.im) x.im) + i fma(f.re, x.im, f.im x.re), and acc + f * x folds acc into the
+// inner product first, as zmul and zmadd do.
 __device__ __forceinline__ C2 c2mul(const CF& f, const C2& v) {
-    return C2{__ffma2_rn(f.ni, v.im, __fmul2_rn(f.r, v.re)), __ffma2_rn(f.i, v.re, __fmul2_rn(f.r, v.im))};
+    return C2{__ffma2_rn(f.r, v.re, __fmul2_rn(f.ni, v.im)), __ffma2_rn(f.r, v.im, __fmul2_rn(f.i, v.re))};
 }
 __device__ __forceinline__ C2 c2madd(const CF& f, const C2& v, const C2& acc) {
-    return C2{__ffma2_rn(f.ni, v.im, __ffma2_rn(f.r, v.re, acc.re)),
-              __ffma2_rn(f.i, v.re, __ffma2_rn(f.r, v.im, acc.im))};
+    return C2{__ffma2_rn(f.r, v.re, __ffma2_rn(f.ni, v.im, acc.re)),
+              __ffma2_rn(f.r, v.im, __ffma2_rn(f.i, v.re, acc.im))};
 }
 __device__ __forceinline__ C2 c2add(const C2& a, const C2& b) {
     return C2{__fadd2_rn(a.re, b.re), __fadd2_rn(a.im, b.im)};
 }
 template <int NEG>
 __device__ __forceinline__ C2 c2addg(const C2& a, const C2& b) {
-    if constexpr (NEG) {
+    if constexpr (NEG) {  // a - b, rounded once
         const float2 m = f2(-1.f, -1.f);
         return C2{__ffma2_rn(m, b.re, a.re), __ffma2_rn(m, b.im, a.im)};
     } else {
         return c2add(a, b);
     }
 }
-// factor f on both lanes
-__device__ __forceinline__ CF cf_same(float2 f) { return CF{f2(f.x, f.x), f2(f.y, f.y), f2(-f.y, -f.y)}; }
 // factor f with lane signs (bit 31 of m0, m1)
 __device__ __forceinline__ CF cf_signed(float2 f, uint32_t m0, uint32_t m1) {
     const float2 a = sflip(f, m0), b = sflip(f, m1);
     return CF{f2(a.x, b.x), f2(a.y, b.y), f2(-a.y, -b.y)};
 }
-__device__ __forceinline__ CF cf_neg(const CF& f) {
-    return CF{f2(-f.r.x, -f.r.y), f2(-f.i.x, -f.i.y), f2(-f.ni.x, -f.ni.y)};
-}
 
+// unit weights (prologue): as orb1 / body1
 template <int KIND, int R, int K, int B, int DEAD, int SK, int J = 0>
-__device__ __forceinline__ void porb1(C2 (&v)[1 << R], const CF& F0, const CF& F1p, const CF& F1n, const CF& Fap,
-                                      const CF& Fan, int y) {
+__device__ __forceinline__ void porb1(C2 (&v)[1 << R], const CF& F1p, const CF& F1n, const CF& Fap, const CF& Fan,
+                                      int y) {
     if constexpr (J < (1 << R)) {
         if constexpr (!(J & (1 << K)) && !(J & DEAD)) {
             constexpr int D = J | (1 << K);
@@ -233,32 +233,30 @@ __device__ __forceinline__ void porb1(C2 (&v)[1 << R], const CF& F0, const CF& F
             const CF& F1 = N ? F1n : F1p;
             const C2 x = v[J], b = v[D];
             if constexpr (KIND == JK_GROW) {
-                v[J] = c2mul(F0, x);
                 v[D] = c2mul(F1, x);
             } else if constexpr (KIND == JK_MIX) {
-                v[J] = c2madd(F0, x, c2mul(N ? Fan : Fap, b));
-                v[D] = c2madd(F0, b, c2mul(F1, x));
+                v[J] = c2madd(N ? Fan : Fap, b, x);
+                v[D] = c2madd(F1, x, b);
             } else if constexpr (KIND == JK_REPLACE) {
-                v[J] = c2mul(F0, c2add(x, b));
+                v[J] = c2add(x, b);
                 v[D] = c2mul(F1, c2addg<SK>(x, b));
             } else if constexpr (KIND == JK_FIXED_SHRINK) {
-                v[J] = y ? c2mul(F1, c2addg<SK>(x, b)) : c2mul(F0, c2add(x, b));
+                v[J] = y ? c2mul(F1, c2addg<SK>(x, b)) : c2add(x, b);
             } else {  // JK_SHRINK2
-                v[J] = c2madd(F0, c2add(x, b), c2mul(F1, c2addg<SK>(x, b)));
+                v[J] = c2madd(F1, c2addg<SK>(x, b), c2add(x, b));
             }
         }
-        porb1<KIND, R, K, B, DEAD, SK, J + 1>(v, F0, F1p, F1n, Fap, Fan, y);
+        porb1<KIND, R, K, B, DEAD, SK, J + 1>(v, F1p, F1n, Fap, Fan, y);
     }
 }
 // lane signs of local entry 0: m0 (lane 0) and m0 ^ TB0 (lane 1)
 template <int KIND, int R, int K, int B, int DEAD, int SK, int SKA, int TB0>
 __device__ __forceinline__ void pbody1(C2 (&v)[1 << R], float4 f, int y, uint32_t m0) {
-    const CF F0 = cf_same(f2(f.x, f.y));
     const uint32_t m1 = m0 ^ (TB0 ? kSign : 0u);
-    const CF F1p = cf_signed(f2(f.z, f.w), m0, m1), F1n = cf_neg(F1p);
+    const CF F1p = cf_signed(f2(f.z, f.w), m0, m1), F1n = cf_signed(f2(f.z, f.w), m0 ^ kSign, m1 ^ kSign);
     constexpr uint32_t ka = SKA ? kSign : 0u;
-    const CF Fap = cf_signed(f2(f.z, f.w), m0 ^ ka, m1 ^ ka), Fan = cf_neg(Fap);
-    porb1<KIND, R, K, B, DEAD, SK>(v, F0, F1p, F1n, Fap, Fan, y);
+    const CF Fap = cf_signed(f2(f.z, f.w), m0 ^ ka, m1 ^ ka), Fan = cf_signed(f2(f.z, f.w), m0 ^ ka ^ kSign, m1 ^ ka ^ kSign);
+    porb1<KIND, R, K, B, DEAD, SK>(v, F1p, F1n, Fap, Fan, y);
 }
 
 template <int R, int B, int DEAD, int J = 0>
@@ -268,49 +266,45 @@ __device__ __forceinline__ void porb0(C2 (&v)[1 << R], const CF& Fp, const CF& F
         porb0<R, B, DEAD, J + 1>(v, Fp, Fn);
     }
 }
+// as body0: (1 + s f1) x for the diagonal kind; y ? s x : x for a fixed step
 template <int KIND, int R, int B, int DEAD, int TB0>
 __device__ __forceinline__ void pbody0(C2 (&v)[1 << R], float4 f, int y, uint32_t m0) {
-    const float2 f0 = f2(f.x, f.y), f1 = f2(f.z, f.w);
+    const float2 f1 = f2(f.z, f.w);
     const uint32_t m1 = m0 ^ (TB0 ? kSign : 0u);
-    if constexpr (KIND == JK_DIAG) {  // (f0 + s f1) x, per lane
-        const float2 a = zadd(f0, sflip(f1, m0)), b = zadd(f0, sflip(f1, m1));
-        const float2 an = zadd(f0, sflip(f1, m0 ^ kSign)), bn = zadd(f0, sflip(f1, m1 ^ kSign));
-        const CF Fp{f2(a.x, b.x), f2(a.y, b.y), f2(-a.y, -b.y)}, Fn{f2(an.x, bn.x), f2(an.y, bn.y), f2(-an.y, -bn.y)};
+    if constexpr (KIND == JK_DIAG) {
+        const float2 a = sflip(f1, m0), b = sflip(f1, m1), an = sflip(f1, m0 ^ kSign), bn = sflip(f1, m1 ^ kSign);
+        const float2 pa = f2(1.f + a.x, a.y), pb = f2(1.f + b.x, b.y);
+        const float2 na = f2(1.f + an.x, an.y), nb = f2(1.f + bn.x, bn.y);
+        const CF Fp{f2(pa.x, pb.x), f2(pa.y, pb.y), f2(-pa.y, -pb.y)};
+        const CF Fn{f2(na.x, nb.x), f2(na.y, nb.y), f2(-na.y, -nb.y)};
         porb0<R, B, DEAD>(v, Fp, Fn);
-    } else {  // JK_FIXED: y ? s f1 x : f0 x
-        if (y) {
-            const CF Fp = cf_signed(f1, m0, m1);
-            porb0<R, B, DEAD>(v, Fp, cf_neg(Fp));
-        } else {
-            const CF F0 = cf_same(f0);
-            porb0<R, 0, DEAD>(v, F0, F0);
-        }
+    } else {  // JK_FIXED
+        if (y) porb0<R, B, DEAD>(v, cf_signed(f1, m0, m1), cf_signed(f1, m0 ^ kSign, m1 ^ kSign));
     }
 }
 
+// as orb4 / body4
 template <int R, int K1, int K2, int MIX, int B, int DEAD, int SK, int J = 0>
-__device__ __forceinline__ void porb4(C2 (&v)[1 << R], const CF& F0, const CF& F1p, const CF& F1n, const CF& Fap,
-                                      const CF& Fan) {
+__device__ __forceinline__ void porb4(C2 (&v)[1 << R], const CF& F1p, const CF& F1n, const CF& Fap, const CF& Fan) {
     if constexpr (J < (1 << R)) {
         if constexpr (!(J & ((1 << K1) | (1 << K2))) && !(J & DEAD)) {
             constexpr int MK = (1 << K1) | ((MIX & 1) ? (1 << K2) : 0);
             constexpr int MKA = (1 << K2) | ((MIX & 2) ? (1 << K1) : 0);
             constexpr bool N = cpar(J & B);
             const C2 x = v[J], b = v[J ^ MK], g = v[J ^ MKA], h = v[J ^ MK ^ MKA];
-            v[J] = c2madd(F0, c2add(x, b), c2mul(N ? Fan : Fap, c2addg<SK>(g, h)));
-            v[J ^ MKA] = c2madd(F0, c2add(g, h), c2mul(N ? F1n : F1p, c2addg<SK>(x, b)));
+            v[J] = c2madd(N ? Fan : Fap, c2addg<SK>(g, h), c2add(x, b));
+            v[J ^ MKA] = c2madd(N ? F1n : F1p, c2addg<SK>(x, b), c2add(g, h));
         }
-        porb4<R, K1, K2, MIX, B, DEAD, SK, J + 1>(v, F0, F1p, F1n, Fap, Fan);
+        porb4<R, K1, K2, MIX, B, DEAD, SK, J + 1>(v, F1p, F1n, Fap, Fan);
     }
 }
 template <int R, int K1, int K2, int MIX, int B, int DEAD, int SK, int SKA, int TB0>
 __device__ __forceinline__ void pbody4(C2 (&v)[1 << R], float4 f, int y, uint32_t m0) {
-    const CF F0 = cf_same(f2(f.x, f.y));
     const uint32_t m1 = m0 ^ (TB0 ? kSign : 0u);
-    const CF F1p = cf_signed(f2(f.z, f.w), m0, m1), F1n = cf_neg(F1p);
+    const CF F1p = cf_signed(f2(f.z, f.w), m0, m1), F1n = cf_signed(f2(f.z, f.w), m0 ^ kSign, m1 ^ kSign);
     constexpr uint32_t ka = SKA ? kSign : 0u;
-    const CF Fap = cf_signed(f2(f.z, f.w), m0 ^ ka, m1 ^ ka), Fan = cf_neg(Fap);
-    porb4<R, K1, K2, MIX, B, DEAD, SK>(v, F0, F1p, F1n, Fap, Fan);
+    const CF Fap = cf_signed(f2(f.z, f.w), m0 ^ ka, m1 ^ ka), Fan = cf_signed(f2(f.z, f.w), m0 ^ ka ^ kSign, m1 ^ ka ^ kSign);
+    porb4<R, K1, K2, MIX, B, DEAD, SK>(v, F1p, F1n, Fap, Fan);
 }
 
 #endif  // DCS_JIT_FP64

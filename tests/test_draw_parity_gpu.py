@@ -183,14 +183,20 @@ def test_block_is_copied_to_host_as_the_reference_worker_does(golden):
 
 @pytest.mark.parametrize("name", ["small", "c2"])
 def test_dimension5_runs_and_group_tuning_are_bit_identical(golden, name):
-    """Register runs of dimension 5 (variant bit 4) and the per-group kernel choice of
-    autotune.tune_groups compute the same blocks, bit for bit, as the dimension-4 kernels."""
+    """Register runs of dimension 5 (variant bit 4), the packed FP32x2 form (variant bit 1) and the
+    per-group kernel choice of autotune.tune_groups compute the same blocks, bit for bit, as the
+    dimension-4 kernels."""
     case, arrays = golden(name)
     eng = _engine(case, arrays, np.complex64, "fused", jit_shape=True)
     xs = [_x(r) for r in case["protocol"]["records"]]
     want = [eng.block(x)[0].cpu().numpy() for x in xs]
     eng.set_fused_config(variant=28)
     assert any(int(v) & 16 for v in eng.fplan.groups["variant"])
+    for x, w in zip(xs, want):
+        assert np.array_equal(eng.block(x)[0].cpu().numpy(), w)
+    from dcs245_classical_sampling_b200.jit import packable
+    eng.set_fused_config(variant=14)  # packed FP32x2 form where the runs leave tile bit 0 free
+    assert any(packable(eng.fplan, gi) for gi in range(len(eng.fplan.groups)))
     for x, w in zip(xs, want):
         assert np.array_equal(eng.block(x)[0].cpu().numpy(), w)
     eng.set_fused_config(variant=12)

@@ -83,3 +83,17 @@ def test_dimension5_runs_plan_and_compile(golden, name):
         assert jit.compile_source(lib, src)[:4] == b"\x7fELF"
     with pytest.raises(ValueError):
         fp.launch_library(lib, 0, 0, 0, 1, 0, 0, None)
+
+
+def test_packed_form_compiles(golden):
+    """The packed FP32x2 form (variant bit 1) of the groups whose runs leave tile bit 0 free."""
+    case, arrays = golden("c2")
+    bp = P.build_block_plan(arrays["graph"], arrays["unitaries"], case["n"], case["order"],
+                            case["parity_operations"], case["open_vertices"])
+    fp = build_fused_plan(bp, max_dim=13, low=3, variant=14, grouping="bytes")
+    packed = [gi for gi in range(len(fp.groups)) if jit.packable(fp, gi)]
+    assert packed
+    lib = _lib.load()
+    for src, _ in jit.plan_sources(bp, fp, parts=1):
+        assert "jit::pbody" in src
+        assert jit.compile_source(lib, src)[:4] == b"\x7fELF"
