@@ -129,10 +129,12 @@ def tune(engine, params_dev, candidates=None, repeats=1, save=True, jit=False):
 
 
 # per-group kernel choices: (CTAs per SM the registers are sized for, KiB staging the next
-# tile's first-run entries (jit.prefetch_layout), local dimension of the register runs; "4p": of
-# dimension 4 in the packed FP32x2 form where the group's runs leave tile bit 0 free)
-GROUP_CANDIDATES = ((3, 0, 4), (3, 8, 4), (2, 0, 4), (2, 16, 4), (2, 32, 4), (2, 0, 5), (2, 16, 5), (2, 32, 5),
-                    (3, 0, "4p"), (2, 0, "4p"))
+# tile's first-run entries (jit.prefetch_layout), local dimension of the register runs).  A third
+# entry "4p" selects dimension 4 in the packed FP32x2 form where the group's runs leave tile bit 0
+# free; on the 64-qubit plan it was slower on every large group (22: 8.1 against 6.0 ms, 24: 27.2
+# against 24.4 ms) and its FP32x2 instructions can round differently from the scalar form, so it
+# is not among the defaults.
+GROUP_CANDIDATES = ((3, 0, 4), (3, 8, 4), (2, 0, 4), (2, 16, 4), (2, 32, 4), (2, 0, 5), (2, 16, 5), (2, 32, 5))
 
 
 def _time_groups(engine, fp, jp, params_dev, repeats):

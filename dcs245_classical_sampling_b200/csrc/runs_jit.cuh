@@ -193,10 +193,10 @@ struct C2 {
 struct CF {  // a complex factor per lane, with its negated imaginary part
     float2 r, i, ni;
 };
-// The packed bodies are the scalar bodies lane by lane, with the same operations in the same
-// order (so every form of a group computes the same values bit for bit): f * x is
-// fma(f.re, x.re, (-f.im) x.im) + i fma(f.re, x.im, f.im x.re), and acc + f * x folds acc into the
-// inner product first, as zmul and zmadd do.
+// The packed bodies are the scalar bodies lane by lane, with the same formulas in the same order:
+// f * x is fma(f.re, x.re, (-f.im) x.im) + i fma(f.re, x.im, f.im x.re), and acc + f * x folds acc
+// into the inner product first, as zmul and zmadd do (the compiler may still schedule the FP32x2
+// instructions so that a result differs from the scalar form in the last unit).
 __device__ __forceinline__ C2 c2mul(const CF& f, const C2& v) {
     return C2{__ffma2_rn(f.r, v.re, __fmul2_rn(f.ni, v.im)), __ffma2_rn(f.r, v.im, __fmul2_rn(f.i, v.re))};
 }
