@@ -505,6 +505,7 @@ def gpu_arm(args):
                              "per_launch": [[b, round(t, 4), round(b / t / 1e6 / peak, 4)]
                                             for b, t in zip(dom["launch_bytes"], dom["launch_ms"])],
                              "per_launch_fields": ["algorithmic bytes", "ms (CUDA events)", "fraction of peak"]},
+                "compute": compute_view(dom),
                 "plain": plain, "speedup_vs_plain": (value / plain["value"]) if plain else None,
                 "draws": {"indices": [int(d["index"]) for d in draws[args.warmup:total]],
                           "ties": int(sum(int(d["tie"]) for d in draws[args.warmup:total])),
@@ -703,8 +704,28 @@ def kernel_roofline(eng, prep, out, stream):
     tot_t = sum(a.elapsed_time(b) for a, b, _ in evs) / 1000.0
     tot_b = sum(x for _, _, x in evs)
     n = len(evs)
+    # entry-steps of each launch: every vertex step touches 2^max(|in|, |out|) table entries
+    spans = eng.fplan.spans if eng.mode == "fused" else [(s, 1) for s in range(eng.nsteps)]
+    entry_steps = [sum(1 << max(len(st.active_in), len(st.active_out)) for st in plan.steps[f0:f0 + c])
+                   for f0, c in spans]
     return {"kernel": kernel, "launches": n, "avg_launch_s": tot_t / n, "alg_bytes_per_launch": tot_b / n,
-            "launch_ms": [a.elapsed_time(b) for a, b, _ in evs], "launch_bytes": [x for _, _, x in evs]}
+            "launch_ms": [a.elapsed_time(b) for a, b, _ in evs], "launch_bytes": [x for _, _, x in evs],
+            "launch_entry_steps": entry_steps}
+
+
+def compute_view(dom):
+    """The contraction's other bound: entry-steps (one table entry through one vertex step) per
+    second.  Inside a fused group the tables grow well beyond the group's input and output (up
+    to 2^34 entries on the 64-qubit plan while the pass reads 2^32 and writes 2^30), so the large
+    groups are bound by the arithmetic and shared-memory work per entry-step, not by HBM."""
+    t = sum(dom["launch_ms"]) / 1000.0
+    es = dom["launch_entry_steps"]
+    big = sorted(range(len(es)), key=lambda i: -dom["launch_ms"][i])[:3]
+    return {"unit": "entry-steps/s", "achieved": sum(es) / t, "entry_steps_per_slice": sum(es),
+            "ns_per_entry_step": 1e9 * t / sum(es),
+            "slowest_launches": [[i, es[i], round(dom["launch_ms"][i], 4),
+                                  round(1e6 * dom["launch_ms"][i] / es[i], 4)] for i in big],
+            "slowest_launches_fields": ["launch", "entry-steps", "ms", "ns per entry-step"]}
 
 
 SERVE_MIX = {"ring32_d37_t79_k14": 50, "ring48_d55_t177_k17": 30, "ring64_d73_t314_k20": 20}

@@ -133,8 +133,11 @@ def tune(engine, params_dev, candidates=None, repeats=1, save=True, jit=False):
 # entry "4p" selects dimension 4 in the packed FP32x2 form where the group's runs leave tile bit 0
 # free; on the 64-qubit plan it was slower on every large group (22: 8.1 against 6.0 ms, 24: 27.2
 # against 24.4 ms) and its FP32x2 instructions can round differently from the scalar form, so it
-# is not among the defaults.
-GROUP_CANDIDATES = ((3, 0, 4), (3, 8, 4), (2, 0, 4), (2, 16, 4), (2, 32, 4), (2, 0, 5), (2, 16, 5), (2, 32, 5))
+# is not among the defaults.  An optional fourth entry is the CTA size (default: the plan's, 256):
+# 128 threads at 3 CTAs per SM hold three tiles per SM instead of two (registers for dimension-5
+# runs still fit: 3 x 128 x 128 <= 65536), each thread taking two cosets of the 256-coset runs.
+GROUP_CANDIDATES = ((3, 0, 4), (3, 8, 4), (2, 0, 4), (2, 16, 4), (2, 32, 4), (2, 0, 5), (2, 16, 5), (2, 32, 5),
+                    (3, 0, 4, 128), (3, 0, 5, 128), (3, 8, 5, 128))
 
 
 def _time_groups(engine, fp, jp, params_dev, repeats):
@@ -167,7 +170,8 @@ def _time_groups(engine, fp, jp, params_dev, repeats):
 
 def tune_groups(engine, params_dev, candidates=GROUP_CANDIDATES, repeats=2, save=True):
     """Choose, per group of the engine's fused plan (plan-specialised kernels), the kernel variant
-    of `candidates` (CTAs per SM, staging KiB, register-run dimension 4 or 5) with the shortest
+    of `candidates` (CTAs per SM, staging KiB, register-run dimension 4 or 5, optionally threads
+    per CTA) with the shortest
     launch, timed with CUDA events on the engine's own table; install the mix and return the
     report.  Every variant computes the same values bit for bit (the same operations in the same
     order on each entry), so groups can mix them."""
@@ -188,17 +192,19 @@ def tune_groups(engine, params_dev, candidates=GROUP_CANDIDATES, repeats=2, save
     times = {}
     for cand in candidates:
         minb, kb, r = int(cand[0]), int(cand[1]), cand[2]
+        nt = int(cand[3]) if len(cand) > 3 else threads
         fp = plans[r]
-        jp = JitPlan(engine.plan, fp, lib, minb=minb, threads=threads, group_cfg={gi: (minb, kb) for gi in range(ng)})
+        jp = JitPlan(engine.plan, fp, lib, minb=minb, threads=threads,
+                     group_cfg={gi: (minb, kb, nt) for gi in range(ng)})
         t = _time_groups(engine, fp, jp, params_dev, repeats)
         jp.close()
         for gi in range(ng):  # a group that fell back to the dimension-4 scalar kernel is timed there
             if (r == 5 and not int(fp.groups[gi]["variant"]) & 16) or (r == "4p" and not packable(fp, gi)):
                 t[gi] = float("inf")
-        times[(minb, kb, r)] = t
+        times[(minb, kb, r, nt)] = t
     choice = {gi: min(times, key=lambda c: times[c][gi]) for gi in range(ng)}
     group_variant = {gi: variants[c[2]] for gi, c in choice.items() if c[2] != 4}
-    group_cfg = {gi: (c[0], c[1]) for gi, c in choice.items()}
+    group_cfg = {gi: (c[0], c[1]) if c[3] == threads else (c[0], c[1], c[3]) for gi, c in choice.items()}
     engine.fplan.jit.close()
     engine.fused_config = {**base, "group_variant": group_variant}
     engine.jit_group_cfg = group_cfg

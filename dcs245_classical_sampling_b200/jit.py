@@ -654,28 +654,36 @@ def _packed_source(fp, gi, minb):
     return "\n".join(L) + "\n"
 
 
+def group_config(group_cfg, gi, minb, threads):
+    """(CTAs per SM of the registers, staging KiB or None, threads per CTA) of group gi: its
+    entry of group_cfg, (minb, staging KiB) or (minb, staging KiB, threads), else the plan's."""
+    c = tuple((group_cfg or {}).get(gi, (minb, None)))
+    return (c[0], c[1], c[2] if len(c) > 2 else threads)
+
+
 def plan_sources(plan, fp, minb=3, parts=8, threads=256, group_cfg=None):
     """Translation units (source strings) holding the group kernels, spread over `parts` units
     so that NVRTC compiles them in parallel; returns [(source, [group indices])].  group_cfg:
-    {group: (CTAs per SM of its registers, staging KiB)} overriding minb and the plan's
-    prefetch_kb for that group."""
+    {group: (CTAs per SM of its registers, staging KiB[, threads per CTA])} overriding minb, the
+    plan's prefetch_kb and `threads` for that group (a unit holds kernels of one thread count)."""
     groups = [gi for gi in range(len(fp.groups)) if int(fp.groups[gi]["variant"]) & 4]
-    cfg = group_cfg or {}
-    # balance by generated size
-    bodies = {gi: group_source(plan, fp, gi, cfg.get(gi, (minb, None))[0], threads, cfg.get(gi, (minb, None))[1])
-              for gi in groups}
-    units = [([], 0) for _ in range(max(1, min(parts, len(groups))))]
-    for gi in sorted(groups, key=lambda q: -len(bodies[q])):
-        k = min(range(len(units)), key=lambda u: units[u][1])
-        units[k] = (units[k][0] + [gi], units[k][1] + len(bodies[gi]))
+    cfg = {gi: group_config(group_cfg, gi, minb, threads) for gi in groups}
+    bodies = {gi: group_source(plan, fp, gi, cfg[gi][0], cfg[gi][2], cfg[gi][1]) for gi in groups}
     out = []
-    for gis, _ in units:
-        if not gis:
-            continue
-        src = (f"#define DCS_JIT_THREADS {threads}\n" +
-               ("#define DCS_JIT_FP64 1\n" if getattr(fp, "fp64", False) else "") +
-               '#include "runs_jit.cuh"\n\n' + "\n".join(bodies[gi] for gi in sorted(gis)))
-        out.append((src, sorted(gis)))
+    for nt in sorted({c[2] for c in cfg.values()}):
+        mine = [gi for gi in groups if cfg[gi][2] == nt]
+        # balance by generated size
+        units = [([], 0) for _ in range(max(1, min(parts, len(mine))))]
+        for gi in sorted(mine, key=lambda q: -len(bodies[q])):
+            k = min(range(len(units)), key=lambda u: units[u][1])
+            units[k] = (units[k][0] + [gi], units[k][1] + len(bodies[gi]))
+        for gis, _ in units:
+            if not gis:
+                continue
+            src = (f"#define DCS_JIT_THREADS {nt}\n" +
+                   ("#define DCS_JIT_FP64 1\n" if getattr(fp, "fp64", False) else "") +
+                   '#include "runs_jit.cuh"\n\n' + "\n".join(bodies[gi] for gi in sorted(gis)))
+            out.append((src, sorted(gis)))
     return out
 
 
@@ -719,7 +727,8 @@ class JitPlan:
 
     def __init__(self, plan, fp, lib=None, minb=None, parts=8, threads=256, group_cfg=None):
         """minb: CTAs per SM the registers are sized for (default: 2 if the plan's variant has
-        bit 0, else 3).  group_cfg: {group: (minb, staging KiB)} for groups that differ."""
+        bit 0, else 3).  group_cfg: {group: (minb, staging KiB[, threads])} for groups that
+        differ."""
         self.lib = lib or _lib.load()
         self.fp = fp
         self.kernels = {}
@@ -729,7 +738,7 @@ class JitPlan:
             minb = 2 if len(fp.groups) and int(fp.groups[0]["variant"]) & 1 else 3
         self.minb = int(minb)
         self.threads = int(threads)
-        self.group_cfg = {int(g): (int(m), int(kb)) for g, (m, kb) in (group_cfg or {}).items()}
+        self.group_cfg = {int(g): tuple(int(x) for x in c) for g, c in (group_cfg or {}).items()}
         sms = self.lib.dcs_sm_count()
         if getattr(fp, "fp64", False):
             missing = [gi for gi in range(len(fp.groups)) if not int(fp.groups[gi]["variant"]) & 4]
@@ -743,13 +752,14 @@ class JitPlan:
             self._libs.append(handle)
             for gi in gis:
                 g = fp.groups[gi]
-                smem = group_smem(fp, gi, self.threads, self.group_cfg.get(gi, (None, None))[1])
+                _, kb, nt = group_config(self.group_cfg, gi, self.minb, self.threads)
+                smem = group_smem(fp, gi, nt, kb)
                 k = ctypes.c_void_p()
                 per_sm = ctypes.c_int()
-                _lib.check(self.lib.dcs_jit_kernel(handle, f"dcs_g{gi}".encode(), smem, self.threads, ctypes.byref(k),
+                _lib.check(self.lib.dcs_jit_kernel(handle, f"dcs_g{gi}".encode(), smem, nt, ctypes.byref(k),
                                                    ctypes.byref(per_sm)))
                 grid = min(sms * max(1, per_sm.value), 1 << int(g["coset_m"]))
-                self.kernels[gi] = (k, grid, smem)
+                self.kernels[gi] = (k, grid, smem, nt)
 
     def launch(self, table, params, g0, ng, maxbits, scale, stream):
         """Groups [g0, g0 + ng) on `stream` (ints: device pointers); library status."""
@@ -758,8 +768,8 @@ class JitPlan:
             if kern is None:
                 rc = self.fp.launch_library(self.lib, table, params, gi, 1, maxbits, scale, stream)
             else:
-                k, grid, smem = kern
-                rc = self.lib.dcs_jit_launch(k, grid, self.threads, smem, table, params, maxbits, scale, stream)
+                k, grid, smem, nt = kern
+                rc = self.lib.dcs_jit_launch(k, grid, nt, smem, table, params, maxbits, scale, stream)
             if rc != 0:
                 return rc
         return 0

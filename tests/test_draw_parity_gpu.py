@@ -205,3 +205,20 @@ def test_dimension5_runs_and_group_tuning_are_bit_identical(golden, name):
     assert set(rep["group_cfg"]) == {str(g) for g in range(len(eng.fplan.groups))}
     for x, w in zip(xs, want):
         assert np.array_equal(eng.block(x)[0].cpu().numpy(), w)
+
+
+@pytest.mark.parametrize("name", ["small", "c2"])
+def test_smaller_ctas_are_bit_identical(golden, name):
+    """Generated kernels of 128 threads per CTA (each thread taking two cosets of the larger runs),
+    with and without staging and with dimension-5 runs, give the 256-thread kernels' blocks bit
+    for bit."""
+    case, arrays = golden(name)
+    eng = _engine(case, arrays, np.complex64, "fused", jit_shape=True)
+    xs = [_x(r) for r in case["protocol"]["records"]][:3]
+    want = [eng.block(x)[0].cpu().numpy() for x in xs]
+    ng = len(eng.fplan.groups)
+    for variant, kb in ((12, 0), (12, 8), (28, 8)):
+        eng.set_fused_config(variant=variant, group_cfg={gi: (3, kb, 128) for gi in range(ng)})
+        assert {k[3] for k in eng.fplan.jit.kernels.values()} == {128}
+        for x, w in zip(xs, want):
+            assert np.array_equal(eng.block(x)[0].cpu().numpy(), w)

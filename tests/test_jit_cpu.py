@@ -58,6 +58,14 @@ def test_fp64_and_staged_kernels_compile(golden, name):
     src = units[0][0]
     assert src.count("cp_async_wait_all") == len(staged)
     assert jit.compile_source(lib, src)[:4] == b"\x7fELF"
+    # a third entry sets the group's CTA size: one translation unit per thread count
+    cfg = {gi: (3, 8, 128) if gi in staged else (3, 0) for gi in range(len(fp.groups))}
+    units = jit.plan_sources(bp, fp, parts=1, group_cfg=cfg)
+    assert len(units) == (2 if len(staged) < len(fp.groups) else 1)
+    for src, gis in units:
+        nt = 128 if set(gis) <= set(staged) else 256
+        assert src.startswith(f"#define DCS_JIT_THREADS {nt}\n") and f"__launch_bounds__({nt}, 3)" in src
+        assert jit.compile_source(lib, src)[:4] == b"\x7fELF"
 
 
 @pytest.mark.parametrize("name", ["small", "c2"])
