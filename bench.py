@@ -505,7 +505,8 @@ def gpu_arm(args):
                              "per_launch": [[b, round(t, 4), round(b / t / 1e6 / peak, 4)]
                                             for b, t in zip(dom["launch_bytes"], dom["launch_ms"])],
                              "per_launch_fields": ["algorithmic bytes", "ms (CUDA events)", "fraction of peak"]},
-                "compute": compute_view(dom),
+                "compute": compute_view(dom, torch.cuda.get_device_properties(dev).multi_processor_count,
+                                        float(clk.get("sm_mhz") or 1965.0) if isinstance(clk, dict) else 1965.0),
                 "plain": plain, "speedup_vs_plain": (value / plain["value"]) if plain else None,
                 "draws": {"indices": [int(d["index"]) for d in draws[args.warmup:total]],
                           "ties": int(sum(int(d["tie"]) for d in draws[args.warmup:total])),
@@ -708,12 +709,32 @@ def kernel_roofline(eng, prep, out, stream):
     spans = eng.fplan.spans if eng.mode == "fused" else [(s, 1) for s in range(eng.nsteps)]
     entry_steps = [sum(1 << max(len(st.active_in), len(st.active_out)) for st in plan.steps[f0:f0 + c])
                    for f0, c in spans]
+    prm = prep["params"][:eng.nsteps * _lib.PARAM_DTYPE.itemsize // 8].cpu().numpy().view(_lib.PARAM_DTYPE)
+    ops = [sum(step_fp32_ops(st, int(prm[f0 + i]["y"])) for i, st in enumerate(plan.steps[f0:f0 + c]))
+           for f0, c in spans]
     return {"kernel": kernel, "launches": n, "avg_launch_s": tot_t / n, "alg_bytes_per_launch": tot_b / n,
             "launch_ms": [a.elapsed_time(b) for a, b, _ in evs], "launch_bytes": [x for _, _, x in evs],
-            "launch_entry_steps": entry_steps}
+            "launch_entry_steps": entry_steps, "launch_fp32_ops": ops}
 
 
-def compute_view(dom):
+def step_fp32_ops(st, y):
+    """FP32 operations (add, multiply or fused multiply-add, one each) of one vertex step in the
+    unit-weight form the generated kernels evaluate (each free step's f0 divided out, f = f1/f0,
+    signs chosen, not multiplied), per the 2^|in| input entries: a grow multiplies the new entry
+    by f (4 per input); a mix, replace, four- or two-entry shrink forms each output as one
+    complex sum plus one complex multiply-add (4 per input); a fixed step with y = 1 multiplies
+    (4), with y = 0 copies (0); a fixed shrink adds (1 per input) or adds and multiplies (3)."""
+    from dcs245_classical_sampling_b200.plan import orbit_kind
+    kind = orbit_kind(st)[0]
+    n = 1 << len(st.active_in)
+    if kind == 4:
+        return 4 * n if y else 0
+    if kind == 5:
+        return 3 * n if y else n
+    return 4 * n
+
+
+def compute_view(dom, sms, sm_mhz):
     """The contraction's other bound: entry-steps (one table entry through one vertex step) per
     second.  Inside a fused group the tables grow well beyond the group's input and output (up
     to 2^34 entries on the 64-qubit plan while the pass reads 2^32 and writes 2^30), so the large
@@ -721,11 +742,17 @@ def compute_view(dom):
     t = sum(dom["launch_ms"]) / 1000.0
     es = dom["launch_entry_steps"]
     big = sorted(range(len(es)), key=lambda i: -dom["launch_ms"][i])[:3]
-    return {"unit": "entry-steps/s", "achieved": sum(es) / t, "entry_steps_per_slice": sum(es),
-            "ns_per_entry_step": 1e9 * t / sum(es),
+    ops = dom["launch_fp32_ops"]
+    peak = sms * 128 * sm_mhz * 1e6 / 1e12  # FP32 pipe: 128 lanes per SM per clock (FFMA or FFMA2)
+    return {"bound": "fp32", "unit": "TFLOP/s (FP32 operations of the unit-weight step formulas)",
+            "achieved": sum(ops) / t / 1e12, "peak": peak, "frac": sum(ops) / t / 1e12 / peak,
+            "peak_source": f"{sms} SMs x 128 FP32 lanes x {sm_mhz:.0f} MHz (median SM clock of the timed "
+                           "region); a register-resident FFMA / FFMA2 loop measured 127-130 per SM per clock",
+            "entry_steps_per_s": sum(es) / t, "entry_steps_per_slice": sum(es), "fp32_ops_per_slice": sum(ops),
+            "ps_per_entry_step": 1e12 * t / sum(es),
             "slowest_launches": [[i, es[i], round(dom["launch_ms"][i], 4),
-                                  round(1e6 * dom["launch_ms"][i] / es[i], 4)] for i in big],
-            "slowest_launches_fields": ["launch", "entry-steps", "ms", "ns per entry-step"]}
+                                  round(ops[i] / dom["launch_ms"][i] / 1e9 / peak, 4)] for i in big],
+            "slowest_launches_fields": ["launch", "entry-steps", "ms", "fraction of the FP32 peak"]}
 
 
 SERVE_MIX = {"ring32_d37_t79_k14": 50, "ring48_d55_t177_k17": 30, "ring64_d73_t314_k20": 20}
