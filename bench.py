@@ -720,10 +720,12 @@ def kernel_roofline(eng, prep, out, stream):
 def step_fp32_ops(st, y):
     """FP32 operations (add, multiply or fused multiply-add, one each) of one vertex step in the
     unit-weight form the generated kernels evaluate (each free step's f0 divided out, f = f1/f0,
-    signs chosen, not multiplied), per the 2^|in| input entries: a grow multiplies the new entry
-    by f (4 per input); a mix, replace, four- or two-entry shrink forms each output as one
-    complex sum plus one complex multiply-add (4 per input); a fixed step with y = 1 multiplies
-    (4), with y = 0 copies (0); a fixed shrink adds (1 per input) or adds and multiplies (3)."""
+    signs chosen, not multiplied), per the n = 2^|in| input entries.  A grow multiplies each new
+    entry by f (4n); a mix forms both entries of an orbit as x + f y (4n); a diagonal mix or a
+    fixed step with y = 1 multiplies (4n), a fixed step with y = 0 copies (0).  A replace, a
+    two-entry shrink and a four-entry shrink need a + b, and a - b only where the partner sign
+    parity(K & beta) is odd (else a + b is reused): 3n, or 4n with the odd sign; a fixed shrink
+    adds (n) or adds and multiplies (3n)."""
     from dcs245_classical_sampling_b200.plan import orbit_kind
     kind = orbit_kind(st)[0]
     n = 1 << len(st.active_in)
@@ -731,6 +733,8 @@ def step_fp32_ops(st, y):
         return 4 * n if y else 0
     if kind == 5:
         return 3 * n if y else n
+    if kind in (3, 6, 7):
+        return (4 if bin(st.K & st.beta).count("1") & 1 else 3) * n
     return 4 * n
 
 
