@@ -136,8 +136,11 @@ def tune(engine, params_dev, candidates=None, repeats=1, save=True, jit=False):
 # is not among the defaults.  An optional fourth entry is the CTA size (default: the plan's, 256):
 # 128 threads at 3 CTAs per SM hold three tiles per SM instead of two (registers for dimension-5
 # runs still fit: 3 x 128 x 128 <= 65536), each thread taking two cosets of the 256-coset runs.
+# "4t" / "5t": dimension 4 / 5 with run bases that may touch other roles (variant bit 6: fewer
+# register runs, so fewer shared-memory round trips per tile).
 GROUP_CANDIDATES = ((3, 0, 4), (3, 8, 4), (2, 0, 4), (2, 16, 4), (2, 32, 4), (2, 0, 5), (2, 16, 5), (2, 32, 5),
-                    (3, 0, 4, 128), (3, 0, 5, 128), (3, 8, 5, 128))
+                    (3, 0, 4, 128), (3, 0, 5, 128), (3, 8, 5, 128),
+                    (3, 8, "4t"), (2, 32, "4t"), (2, 16, "5t"), (2, 32, "5t"), (3, 8, "5t", 128))
 
 
 def _time_groups(engine, fp, jp, params_dev, repeats):
@@ -184,8 +187,8 @@ def tune_groups(engine, params_dev, candidates=GROUP_CANDIDATES, repeats=2, save
     threads = engine.fplan.jit.threads
     from .jit import packable
     base = {k: v for k, v in engine.fused_config.items() if k != "group_variant"}
-    v4 = (int(base["variant"]) & ~18) | 12
-    variants = {4: v4, 5: v4 | 16, "4p": v4 | 2}
+    v4 = (int(base["variant"]) & ~82) | 12
+    variants = {4: v4, 5: v4 | 16, "4p": v4 | 2, "4t": v4 | 64, "5t": v4 | 80}
     plans = {r: build_fused_plan(engine.plan, **{**base, "variant": v}) for r, v in variants.items()
              if any(c[2] == r for c in candidates)}
     ng = len(plans[4].groups)
@@ -199,7 +202,7 @@ def tune_groups(engine, params_dev, candidates=GROUP_CANDIDATES, repeats=2, save
         t = _time_groups(engine, fp, jp, params_dev, repeats)
         jp.close()
         for gi in range(ng):  # a group that fell back to the dimension-4 scalar kernel is timed there
-            if (r == 5 and not int(fp.groups[gi]["variant"]) & 16) or (r == "4p" and not packable(fp, gi)):
+            if (r in (5, "5t") and not int(fp.groups[gi]["variant"]) & 16) or (r == "4p" and not packable(fp, gi)):
                 t[gi] = float("inf")
         times[(minb, kb, r, nt)] = t
     choice = {gi: min(times, key=lambda c: times[c][gi]) for gi in range(ng)}

@@ -101,85 +101,109 @@ __device__ __forceinline__ unsigned long long max_key(double m) { return (unsign
 // The weights are unit weights (prologue): f0 = 1 at every free step, and at a fixed step the
 // weight its y selects is 1, so no body multiplies by f0.
 //
-// One-vector kinds along local bit K: orbits {j, j | 2^K} for j with bit K clear and no DEAD
-// bit.  Sign of representative j: (-1)^(m0 + <j, B>), so F1p / F1n = s f1 for <j, B> even /
-// odd.  SK / SKA: the partner signs (-1)^sK, (-1)^sKa.  Formulas: the per-step kernel's
+// Local entry j is dead (its address has an inactive slot) when one of the parity masks packed
+// in DP (6 bits each, up to five, 0 ends the list) has odd parity with j: the mask of basis
+// vectors that have an inactive role coordinate.  When no basis vector touches another's role
+// coordinate every mask is one bit, the bits of DEAD.
+__host__ __device__ constexpr bool deadp(int j, uint32_t dp) {
+    return dp ? (cpar(j & (int)(dp & 63u)) != 0 || deadp(j, dp >> 6)) : false;
+}
+
+// One-vector kinds along local bit K: orbits {c, c ^ 2^K}, one per j with bit K clear and not
+// dead; c is the entry whose role coordinate is zero: j, or j | 2^K when the other basis vectors
+// touching the role (local mask TK) flip it (TK = 0 when no basis vector touches another's role).
+// Sign of representative c: (-1)^(m0 + <c, B>), so F1p / F1n = s f1 for <c, B> even / odd.
+// SK / SKA: the partner signs (-1)^sK, (-1)^sKa.  Formulas: the per-step kernel's
 // (reference: source/kernel_opt/inplace_gpu.py:29-58) with f0 = 1.
-template <int KIND, int R, int K, int B, int DEAD, int SK, int SKA, int J = 0>
+template <int KIND, int R, int K, int B, int DEAD, int SK, int SKA, int TK = 0, uint32_t DP = 0, int J = 0>
 __device__ __forceinline__ void orb1(cplx_t (&v)[1 << R], cplx_t F1p, cplx_t F1n, cplx_t Fap, cplx_t Fan, int y) {
     if constexpr (J < (1 << R)) {
-        if constexpr (!(J & (1 << K)) && !(J & DEAD)) {
-            constexpr int D = J | (1 << K);
-            constexpr bool N = cpar(J & B);
+        if constexpr (!(J & (1 << K)) && !(J & DEAD) && !deadp(J, DP)) {
+            constexpr int C = cpar(J & TK) ? (J | (1 << K)) : J;
+            constexpr int D = C ^ (1 << K);
+            constexpr bool N = cpar(C & B);
             const cplx_t F1 = N ? F1n : F1p;
-            const cplx_t x = v[J], b = v[D];
-            if constexpr (KIND == JK_GROW) {  // v[J] = x stays
+            const cplx_t x = v[C], b = v[D];
+            if constexpr (KIND == JK_GROW) {  // v[C] = x stays
                 v[D] = zmul(F1, x);
             } else if constexpr (KIND == JK_MIX) {
-                v[J] = zmadd(N ? Fan : Fap, b, x);
+                v[C] = zmadd(N ? Fan : Fap, b, x);
                 v[D] = zmadd(F1, x, b);
             } else if constexpr (KIND == JK_REPLACE) {
-                v[J] = zadd(x, b);
+                v[C] = zadd(x, b);
                 v[D] = zmul(F1, zaddg<SK>(x, b));
             } else if constexpr (KIND == JK_FIXED_SHRINK) {
-                v[J] = y ? zmul(F1, zaddg<SK>(x, b)) : zadd(x, b);
+                v[C] = y ? zmul(F1, zaddg<SK>(x, b)) : zadd(x, b);
             } else {  // JK_SHRINK2
-                v[J] = zmadd(F1, zaddg<SK>(x, b), zadd(x, b));
+                v[C] = zmadd(F1, zaddg<SK>(x, b), zadd(x, b));
             }
         }
-        orb1<KIND, R, K, B, DEAD, SK, SKA, J + 1>(v, F1p, F1n, Fap, Fan, y);
+        orb1<KIND, R, K, B, DEAD, SK, SKA, TK, DP, J + 1>(v, F1p, F1n, Fap, Fan, y);
     }
 }
-template <int KIND, int R, int K, int B, int DEAD, int SK, int SKA>
+template <int KIND, int R, int K, int B, int DEAD, int SK, int SKA, int TK = 0, uint32_t DP = 0>
 __device__ __forceinline__ void body1(cplx_t (&v)[1 << R], wts_t f, int y, uint32_t m0) {
     const cplx_t f1 = f2(f.z, f.w);
     const cplx_t F1p = sflip(f1, m0), F1n = sflip(f1, m0 ^ kSign);
     constexpr uint32_t ka = SKA ? kSign : 0u;
-    orb1<KIND, R, K, B, DEAD, SK, SKA>(v, F1p, F1n, sflip(F1p, ka), sflip(F1n, ka), y);
+    orb1<KIND, R, K, B, DEAD, SK, SKA, TK, DP>(v, F1p, F1n, sflip(F1p, ka), sflip(F1n, ka), y);
 }
 
-// One-entry kinds: every local entry without a DEAD bit.
-template <int R, int B, int DEAD, int J = 0>
+// One-entry kinds: every local entry that is not dead.
+template <int R, int B, int DEAD, uint32_t DP = 0, int J = 0>
 __device__ __forceinline__ void orb0(cplx_t (&v)[1 << R], cplx_t Fp, cplx_t Fn) {
     if constexpr (J < (1 << R)) {
-        if constexpr (!(J & DEAD)) v[J] = zmul(cpar(J & B) ? Fn : Fp, v[J]);
-        orb0<R, B, DEAD, J + 1>(v, Fp, Fn);
+        if constexpr (!(J & DEAD) && !deadp(J, DP)) v[J] = zmul(cpar(J & B) ? Fn : Fp, v[J]);
+        orb0<R, B, DEAD, DP, J + 1>(v, Fp, Fn);
     }
 }
-template <int KIND, int R, int B, int DEAD>
+template <int KIND, int R, int B, int DEAD, uint32_t DP = 0>
 __device__ __forceinline__ void body0(cplx_t (&v)[1 << R], wts_t f, int y, uint32_t m0) {
     const cplx_t f1 = f2(f.z, f.w);
     const cplx_t F1p = sflip(f1, m0), F1n = sflip(f1, m0 ^ kSign);
     if constexpr (KIND == JK_DIAG) {  // (1 + s f1) x
-        orb0<R, B, DEAD>(v, f2((real_t)1 + F1p.x, F1p.y), f2((real_t)1 + F1n.x, F1n.y));
+        orb0<R, B, DEAD, DP>(v, f2((real_t)1 + F1p.x, F1p.y), f2((real_t)1 + F1n.x, F1n.y));
     } else {  // JK_FIXED: y ? s x : x (the selected weight is 1)
-        if (y) orb0<R, B, DEAD>(v, F1p, F1n);
+        if (y) orb0<R, B, DEAD, DP>(v, F1p, F1n);
     }
 }
 
+// The representative of a four-entry orbit {j ^ a MK ^ b MKA}: the entry whose two role
+// coordinates (parities with the local masks ROW1 = 2^K1 | T1, ROW2 = 2^K2 | T2) are zero.
+template <int J, int MK, int MKA, int ROW1, int ROW2>
+__host__ __device__ constexpr int rep4() {
+    int c = J;
+    for (int ab = 0; ab < 4; ++ab) {
+        const int e = J ^ ((ab & 1) ? MK : 0) ^ ((ab & 2) ? MKA : 0);
+        if (!cpar(e & ROW1) && !cpar(e & ROW2)) c = e;
+    }
+    return c;
+}
+
 // Four-entry shrink along local bits K1 (K's role) and K2 (Ka's role); MIX bit 0: K's local
-// mask also has K2, bit 1: Ka's has K1.
+// mask also has K2, bit 1: Ka's has K1; T1 / T2: the other basis vectors touching the roles.
 //   o_c = (x + b) + s_d f1 (g + gK h) ;  o_{c^Ka} = (g + h) + s_c f1 (x + gK b).
-template <int R, int K1, int K2, int MIX, int B, int DEAD, int SK, int J = 0>
+template <int R, int K1, int K2, int MIX, int B, int DEAD, int SK, int T1 = 0, int T2 = 0, uint32_t DP = 0, int J = 0>
 __device__ __forceinline__ void orb4(cplx_t (&v)[1 << R], cplx_t F1p, cplx_t F1n, cplx_t Fap, cplx_t Fan) {
     if constexpr (J < (1 << R)) {
-        if constexpr (!(J & ((1 << K1) | (1 << K2))) && !(J & DEAD)) {
+        if constexpr (!(J & ((1 << K1) | (1 << K2))) && !(J & DEAD) && !deadp(J, DP)) {
             constexpr int MK = (1 << K1) | ((MIX & 1) ? (1 << K2) : 0);
             constexpr int MKA = (1 << K2) | ((MIX & 2) ? (1 << K1) : 0);
-            constexpr bool N = cpar(J & B);
-            const cplx_t x = v[J], b = v[J ^ MK], g = v[J ^ MKA], h = v[J ^ MK ^ MKA];
-            v[J] = zmadd(N ? Fan : Fap, zaddg<SK>(g, h), zadd(x, b));
-            v[J ^ MKA] = zmadd(N ? F1n : F1p, zaddg<SK>(x, b), zadd(g, h));
+            constexpr int C = rep4<J, MK, MKA, (1 << K1) | T1, (1 << K2) | T2>();
+            constexpr bool N = cpar(C & B);
+            const cplx_t x = v[C], b = v[C ^ MK], g = v[C ^ MKA], h = v[C ^ MK ^ MKA];
+            v[C] = zmadd(N ? Fan : Fap, zaddg<SK>(g, h), zadd(x, b));
+            v[C ^ MKA] = zmadd(N ? F1n : F1p, zaddg<SK>(x, b), zadd(g, h));
         }
-        orb4<R, K1, K2, MIX, B, DEAD, SK, J + 1>(v, F1p, F1n, Fap, Fan);
+        orb4<R, K1, K2, MIX, B, DEAD, SK, T1, T2, DP, J + 1>(v, F1p, F1n, Fap, Fan);
     }
 }
-template <int R, int K1, int K2, int MIX, int B, int DEAD, int SK, int SKA>
+template <int R, int K1, int K2, int MIX, int B, int DEAD, int SK, int SKA, int T1 = 0, int T2 = 0, uint32_t DP = 0>
 __device__ __forceinline__ void body4(cplx_t (&v)[1 << R], wts_t f, int y, uint32_t m0) {
     const cplx_t f1 = f2(f.z, f.w);
     const cplx_t F1p = sflip(f1, m0), F1n = sflip(f1, m0 ^ kSign);
     constexpr uint32_t ka = SKA ? kSign : 0u;
-    orb4<R, K1, K2, MIX, B, DEAD, SK>(v, F1p, F1n, sflip(F1p, ka), sflip(F1n, ka));
+    orb4<R, K1, K2, MIX, B, DEAD, SK, T1, T2, DP>(v, F1p, F1n, sflip(F1p, ka), sflip(F1n, ka));
 }
 
 #ifndef DCS_JIT_FP64

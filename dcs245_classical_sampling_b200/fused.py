@@ -98,6 +98,9 @@ class FusedPlan:
     # per run (first step): the 2^R local offsets; per step: parity table of those offsets
     run_off: dict = field(default_factory=dict)
     step_ptab: dict = field(default_factory=dict)
+    # variant bit 6 (generated kernels only): per step of a run whose basis touches other roles,
+    # (T1, T2, packed dead parity masks) (_plan_runs)
+    step_touch: dict = field(default_factory=dict)
     spans: list = field(default_factory=list)      # (first, count) per group
     universe: list = field(default_factory=list)   # |U| per group
     tiles: list = field(default_factory=list)      # tile count per group
@@ -115,6 +118,8 @@ class FusedPlan:
             raise ValueError("the library's fused kernels store complex64 tables")
         if any(int(v) & 16 for v in self.groups["variant"]):
             raise ValueError("register runs of dimension 5 run in the plan-specialised kernels only")
+        if any(int(v) & 64 for v in self.groups["variant"]):
+            raise ValueError("register runs with touching bases run in the plan-specialised kernels only")
         if self.tile_runs is not None:
             return lib.dcs_fused_runs(table, self.dsteps.ctypes.data, len(self.dsteps), self.groups.ctypes.data,
                                       len(self.groups), self.tile_steps.ctypes.data, self.tile_runs.ctypes.data,
@@ -317,13 +322,25 @@ def run_dim(variant):
     return 5 if variant & 16 else (4 if variant & 8 else 3)
 
 
+def _role_rows(basis):
+    """Row k: the local bits m whose basis vector has basis k's role coordinate."""
+    return [sum(1 << m for m, (bm, _) in enumerate(basis) if (bm >> pk) & 1) for _, pk in basis]
+
+
 def _plan_runs(steps, first, count, tsteps, truns, dim, R, tbit, slot_of, keep_bit0=False, run_off=None,
-               step_ptab=None):
+               step_ptab=None, touch=None):
     """Split a group's steps into register runs of local dimension R; False if a step does not fit.
 
     The 2^R local offsets of each run go to run_off[first step] and each step's parity table of
     those offsets to step_ptab[step]; the library's fixed-size records (dcs_tile_run,
-    dcs_tile_step) hold them too where R <= 4."""
+    dcs_tile_step) hold them too where R <= 4.
+
+    touch (a dict, generated kernels only): a basis vector may have another's role coordinate as
+    long as the matrix of the basis at the role coordinates stays invertible (every coset of the
+    run's span then still has exactly one entry zero at the roles).  A step's representative and
+    dead entries then depend on several local bits; touch[step] = (T1, T2, DP): the other local
+    bits touching the step's role(s) and the packed parity masks of the dead entries
+    (runs_jit.cuh, deadp)."""
     vr = []
     for s in range(first, first + count):
         kind, _ = orbit_kind(steps[s])
@@ -351,10 +368,13 @@ def _plan_runs(steps, first, count, tsteps, truns, dim, R, tbit, slot_of, keep_b
                 else:
                     loc.append(idx)
             ok = ok and len(nb) <= R and _rank([v for v, _ in nb]) == len(nb) and len({p for _, p in nb}) == len(nb)
-            # no basis vector touches another's role coordinate (the representatives of every
-            # step are then the local indices with a zero at the step's own local bit)
-            ok = ok and all(not (vb >> pa) & 1 for ia, (_, pa) in enumerate(nb) for ib, (vb, _) in enumerate(nb)
-                            if ia != ib)
+            if touch is None:
+                # no basis vector touches another's role coordinate (the representatives of every
+                # step are then the local indices with a zero at the step's own local bit)
+                ok = ok and all(not (vb >> pa) & 1 for ia, (_, pa) in enumerate(nb)
+                                for ib, (vb, _) in enumerate(nb) if ia != ib)
+            else:
+                ok = ok and _rank(_role_rows(nb)) == len(nb)
             if not ok:
                 break
             basis = nb
@@ -409,6 +429,18 @@ def _plan_runs(steps, first, count, tsteps, truns, dim, R, tbit, slot_of, keep_b
             act = slot_mask(steps[s0 + i].active_in)
             ts["rdead"] = sum(1 << k for k, (_, p) in enumerate(basis)
                               if k not in locs[i] and not (act >> slot_of(p)) & 1)
+            if touch is not None:
+                rows = _role_rows(basis)
+                dead = [rows[k] for k, (_, p) in enumerate(basis) if k not in locs[i] and not (act >> slot_of(p)) & 1]
+                loc2 = locs[i] + [None, None]
+                t1 = rows[loc2[0]] & ~(1 << loc2[0]) if loc2[0] is not None else 0
+                t2 = rows[loc2[1]] & ~(1 << loc2[1]) if loc2[1] is not None else 0
+                dp = 0
+                for q, mask in enumerate(dead):
+                    dp |= mask << (6 * q)
+                touch[s0 + i] = (t1, t2, dp)
+                if dp or t1 or t2:
+                    ts["rdead"] = 0  # the kernel takes the parity masks instead
             loc = locs[i] + [0, 0]
             ts["rk1"], ts["rk2"] = loc[0], loc[1]
             ts["rmix"] = vr[s0 + i - first][1]
@@ -572,15 +604,17 @@ def build_fused_plan(plan, max_dim=13, low=4, max_steps=MAX_GROUP_STEPS, max_ext
         if gvar & 4:
             slot_of = lambda q: q if q < l else pivots[q - l]
             # packed plans (bit 1) keep tile bit 0 out of the runs: it is the lane bit
+            # variant bit 6: run bases may touch other roles (fewer runs; generated kernels only)
+            tch = fp.step_touch if gvar & 64 else None
             ok = _plan_runs(steps, first, count, tsteps, truns, dim, run_dim(gvar), tbit, slot_of,
-                            keep_bit0=bool(gvar & 2), run_off=fp.run_off, step_ptab=fp.step_ptab)
+                            keep_bit0=bool(gvar & 2), run_off=fp.run_off, step_ptab=fp.step_ptab, touch=tch)
             if not ok and gvar & 16:  # dimension 5 does not fit: dimension 4
                 gvar = (gvar & ~16) | 8
                 g["variant"] = gvar
                 ok = _plan_runs(steps, first, count, tsteps, truns, dim, 4, tbit, slot_of,
-                                keep_bit0=bool(gvar & 2), run_off=fp.run_off, step_ptab=fp.step_ptab)
+                                keep_bit0=bool(gvar & 2), run_off=fp.run_off, step_ptab=fp.step_ptab, touch=tch)
             if not ok:
-                g["variant"] = gvar & ~28  # this group keeps the one-step-per-round-trip kernel
+                g["variant"] = gvar & ~92  # this group keeps the one-step-per-round-trip kernel
         elif pairs:
             _pair_steps(steps, first, count, tsteps, dim, tilepos_of=lambda q: (q < l or q in pivots),
                         tbit=tbit, U=U)

@@ -33,8 +33,13 @@ def _u64(x):
     return f"{int(x) & 0xFFFFFFFFFFFFFFFF}ull"
 
 
-def _beff(kind, ts, R, ptab):
+def _beff(kind, ts, R, ptab, touched=False):
+    """The step's sign functional on the local bits.  The step's own bits are dropped when every
+    representative has them clear (no basis vector touching the role); with touching bases a
+    representative may have them set, so they stay."""
     bl = sum(((ptab >> (1 << k)) & 1) << k for k in range(R))
+    if touched:
+        return bl
     own = 0
     if kind in ONE_VECTOR:
         own = 1 << int(ts["rk1"])
@@ -95,6 +100,17 @@ def _gaddr_fn(g):
     return gaddr
 
 
+def pair_bit(offs, R):
+    """The local bit whose basis vector is tile bit 0, if every entry with that bit clear sits at
+    an even tile offset: local entries j and j | 2^k are then one aligned 16-byte word (complex64).
+    A run basis that touches other roles (variant bit 6) may give some of those entries an odd
+    offset; then the run moves single entries."""
+    k0 = next((k for k in range(R) if int(offs[1 << k]) == 1), None)
+    if k0 is None or any(int(offs[j]) & 1 for j in range(1 << R) if not (j >> k0) & 1):
+        return None
+    return k0
+
+
 def prefetch_layout(fp, gi, threads=256, kb=None):
     """Staging of the next tile's first-run entries (``fp.prefetch_kb`` > 0): every thread copies
     the entries its own cosets of the next tile will load, asynchronously, into its own slots of
@@ -134,7 +150,7 @@ def prefetch_layout(fp, gi, threads=256, kb=None):
     live = [j for j in range(1 << R) if not G[j] & in_inact]
     if not live:
         return None
-    k0 = None if fp64 else next((k for k in range(R) if int(fp.run_off[first + s][1 << k]) == 1), None)
+    k0 = None if fp64 else pair_bit(fp.run_off[first + s], R)
     pair_in = LOW >= 1 and (in_mask & 1)
     if k0 is not None and pair_in:
         units = [(j, j | (1 << k0)) for j in live if not (j >> k0) & 1]
@@ -369,7 +385,7 @@ def group_source(plan, fp, gi, minb=3, threads=256, kb=None):
             L.append("                jit::cp_async_wait_all();  // this thread's staged entries of this tile")
         # local bit k0 with basis vector e_0: entries j and j | 2^k0 are one aligned 16-byte word
         # (complex64 entries only)
-        k0 = None if fp64 else next((k for k in range(R) if int(fp.run_off[first + s][1 << k]) == 1), None)
+        k0 = None if fp64 else pair_bit(fp.run_off[first + s], R)
         pairs = [(j, j | (1 << k0)) for j in range(1 << R) if not (j >> k0) & 1] if k0 is not None else None
         cos = ["a", "b"] if coset_pairs and niter % 2 == 0 else ["a"]
         L.append("#pragma unroll 1")
@@ -430,20 +446,25 @@ def group_source(plan, fp, gi, minb=3, threads=256, kb=None):
             si = s + i
             st = fp.tile_steps[first + si]
             kind = int(fp.dsteps[first + si]["kind"])
-            B = _beff(kind, st, R, fp.step_ptab[first + si])
             dead = int(st["rdead"])
             sk, ska = int(st["sK"]) & 1, int(st["sKa"]) & 1
             k1, k2, mix = int(st["rk1"]), int(st["rk2"]), int(st["rmix"])
+            # bases touching other roles (variant bit 6): representative and dead-entry masks
+            t1, t2, dp = getattr(fp, "step_touch", {}).get(first + si, (0, 0, 0))
+            tch1 = f", {t1}, {dp}u" if (t1 or dp) else ""
+            tch0 = f", {dp}u" if dp else ""
+            tch4 = f", {t1}, {t2}, {dp}u" if (t1 or t2 or dp) else ""
+            B = _beff(kind, st, R, fp.step_ptab[first + si], touched=bool(t1 or t2))
             tb3 = (int(st["tbeta"]) << esh) & 0xFFFFFFFF
             for c in cos:
                 m0 = f"(((uint32_t)__popc(t0{c} & {tb3}u) ^ (csm >> {si})) & 1u) << 31"
                 args = f"(v{c}, fw[{si}], ovy[{si}] >> 1, {m0})"
                 if kind in ONE_VECTOR:
-                    call = f"jit::body1<{kind}, {R}, {k1}, {B}, {dead}, {sk}, {ska}>{args};"
+                    call = f"jit::body1<{kind}, {R}, {k1}, {B}, {dead}, {sk}, {ska}{tch1}>{args};"
                 elif kind in (2, 4):
-                    call = f"jit::body0<{kind}, {R}, {B}, {dead}>{args};"
+                    call = f"jit::body0<{kind}, {R}, {B}, {dead}{tch0}>{args};"
                 else:
-                    call = f"jit::body4<{R}, {k1}, {k2}, {mix}, {B}, {dead}, {sk}, {ska}>{args};"
+                    call = f"jit::body4<{R}, {k1}, {k2}, {mix}, {B}, {dead}, {sk}, {ska}{tch4}>{args};"
                 L.append(f"                    {call}")
         for c in cos:
             if dst_g:
@@ -495,7 +516,7 @@ def packable(fp, gi):
     run of the group has tile bit 0 in its space or among its coset zero bits."""
     g = fp.groups[gi]
     v = int(g["variant"])
-    if getattr(fp, "fp64", False) or v & 16:  # the packed bodies are FP32x2, of runs up to dimension 4
+    if getattr(fp, "fp64", False) or v & 80:  # the packed bodies: FP32x2, runs up to dimension 4, no touching bases
         return False
     if not (v & 2 and v & 4) or not getattr(fp, "direct_io", True) or not _direct_ok(fp, gi):
         return False

@@ -222,3 +222,22 @@ def test_smaller_ctas_are_bit_identical(golden, name):
         assert {k[3] for k in eng.fplan.jit.kernels.values()} == {128}
         for x, w in zip(xs, want):
             assert np.array_equal(eng.block(x)[0].cpu().numpy(), w)
+
+
+@pytest.mark.parametrize("name", ["small", "c2"])
+def test_touching_run_bases_are_bit_identical(golden, name):
+    """Register runs whose bases may touch other roles (variant bit 6: representatives and dead
+    entries by parities of several local bits, fewer runs), at dimension 4 and 5, with and
+    without staging, give the default kernels' blocks bit for bit; the library refuses them."""
+    case, arrays = golden(name)
+    eng = _engine(case, arrays, np.complex64, "fused", jit_shape=True)
+    xs = [_x(r) for r in case["protocol"]["records"]][:3]
+    want = [eng.block(x)[0].cpu().numpy() for x in xs]
+    for variant, kb in ((76, 0), (76, 8), (92, 16), (92, 0)):
+        eng.set_fused_config(variant=variant, prefetch_kb=kb)
+        assert any(t1 or t2 for t1, t2, _ in eng.fplan.step_touch.values())
+        for x, w in zip(xs, want):
+            assert np.array_equal(eng.block(x)[0].cpu().numpy(), w)
+    with pytest.raises(ValueError, match="touching"):
+        eng.set_fused_config(variant=76, jit=False)
+        eng.block(xs[0])

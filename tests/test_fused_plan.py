@@ -6,6 +6,7 @@ import numpy as np
 import pytest
 
 from conftest import rel_l2
+from dcs245_classical_sampling_b200 import jit
 from dcs245_classical_sampling_b200 import plan as P
 from dcs245_classical_sampling_b200.engine import SliceParams
 from dcs245_classical_sampling_b200.fused import build_fused_plan, group_steps
@@ -269,7 +270,8 @@ def _emulate_run(bp, fp, params, s0, bases, sh, dim, packed=False):
         tus.append(tu)
         tu = ((tu | (~mhi & 0xFFFFFFFF)) + 1) & mhi
     t0 = (o[:, None] | np.array(tus, dtype=np.int64)[None, :]).reshape(-1)
-    off = np.array([int(v) for v in tr["off"][:1 << R]], dtype=np.int64)
+    offs = fp.run_off.get(s0) if fp.run_off else None  # every run's 2^R offsets (records hold R <= 4)
+    off = np.array([int(v) for v in (offs if offs is not None else tr["off"][:1 << R])], dtype=np.int64)
     idx = t0[:, None] ^ off[None, :]                      # base, local entry
     # the cosets are disjoint and cover the tile minus the run's inactive coordinates
     assert len(np.unique(idx)) == idx.size
@@ -302,16 +304,26 @@ def _emulate_run(bp, fp, params, s0, bases, sh, dim, packed=False):
         f0, f1 = complex(pr["f0r"], pr["f0i"]), complex(pr["f1r"], pr["f1i"])
         y = int(pr["y"])
         gK, gKa = (-1.0 if int(ts["sK"]) else 1.0), (-1.0 if int(ts["sKa"]) else 1.0)
-        tb, ptab = int(ts["tbeta"]), int(ts["ptab"])
+        tb = int(ts["tbeta"])
+        ptab = int(fp.step_ptab[s]) if s in fp.step_ptab else int(ts["ptab"])
         cs = np.array([bin(int(bb) & st.beta).count("1") & 1 for bb in bases], np.int64)[:, None] ^ int(pr["ov"])
         s0b = np.array([bin(int(q) & tb).count("1") & 1 for q in t0], np.int64)[None, :] ^ cs  # tile, base
         sg = lambda j: np.where(s0b ^ ((ptab >> j) & 1), -1.0, 1.0)
         k1, k2, mix = int(ts["rk1"]), int(ts["rk2"]), int(ts["rmix"])
         dead = int(ts["rdead"])
+        # bases touching other roles (variant bit 6): the representative and the dead entries
+        # follow parities of several local bits (runs_jit.cuh orb1/orb4, deadp)
+        t1, t2, dp = fp.step_touch.get(s, (0, 0, 0))
+        dmasks = [(dp >> (6 * q)) & 63 for q in range(5) if (dp >> (6 * q)) & 63]
+        par = lambda x: bin(x).count("1") & 1
+        # the representative's sign from the generated kernels' local functional (jit._beff), which
+        # keeps the step's own bits only where a representative can have them set
+        Bl = jit._beff(kind, ts, R, ptab, touched=bool(t1 or t2))
+        sg = lambda j, Bl=Bl: np.where(s0b ^ par(j & Bl), -1.0, 1.0)
         e = 1 << k1
         new = v.copy()
         for j in range(1 << R):
-            if j & dead:
+            if j & dead or any(par(j & m) for m in dmasks):
                 continue  # a removed or not yet grown slot: the kernel skips these entries
             x = v[:, :, j]
             if kind in (P.KIND_DIAG, P.KIND_FIXED):
@@ -325,25 +337,30 @@ def _emulate_run(bp, fp, params, s0, bases, sh, dim, packed=False):
                     continue
                 mK = e | ((1 << k2) if mix & 1 else 0)
                 mKa = (1 << k2) | (e if mix & 2 else 0)
-                b, g_, h = v[:, :, j ^ mK], v[:, :, j ^ mKa], v[:, :, j ^ mK ^ mKa]
-                new[:, :, j] = f0 * (x + b) + sg(j) * gKa * f1 * (g_ + gK * h)
-                new[:, :, j ^ mKa] = f0 * (g_ + h) + sg(j) * f1 * (x + gK * b)
+                c = [q for q in (j, j ^ mK, j ^ mKa, j ^ mK ^ mKa)
+                     if not par(q & (e | t1)) and not par(q & ((1 << k2) | t2))]
+                assert len(c) == 1
+                c = c[0]
+                x, b, g_, h = v[:, :, c], v[:, :, c ^ mK], v[:, :, c ^ mKa], v[:, :, c ^ mK ^ mKa]
+                new[:, :, c] = f0 * (x + b) + sg(c) * gKa * f1 * (g_ + gK * h)
+                new[:, :, c ^ mKa] = f0 * (g_ + h) + sg(c) * f1 * (x + gK * b)
                 continue
             if j & e:
                 continue
-            d = j | e
-            b = v[:, :, d]
+            c = j | e if par(j & t1) else j
+            d = c ^ e
+            x, b = v[:, :, c], v[:, :, d]
             if kind == P.KIND_GROW:
-                new[:, :, j], new[:, :, d] = f0 * x, sg(j) * f1 * x
+                new[:, :, c], new[:, :, d] = f0 * x, sg(c) * f1 * x
             elif kind == P.KIND_MIX:
-                new[:, :, j] = f0 * x + sg(j) * gKa * f1 * b
-                new[:, :, d] = f0 * b + sg(j) * f1 * x
+                new[:, :, c] = f0 * x + sg(c) * gKa * f1 * b
+                new[:, :, d] = f0 * b + sg(c) * f1 * x
             elif kind == P.KIND_REPLACE:
-                new[:, :, j], new[:, :, d] = f0 * (x + b), sg(j) * f1 * (x + gK * b)
+                new[:, :, c], new[:, :, d] = f0 * (x + b), sg(c) * f1 * (x + gK * b)
             elif kind == P.KIND_FIXED_SHRINK:
-                new[:, :, j] = sg(j) * f1 * (x + gK * b) if y else f0 * (x + b)
+                new[:, :, c] = sg(c) * f1 * (x + gK * b) if y else f0 * (x + b)
             else:
-                new[:, :, j] = f0 * (x + b) + sg(j) * f1 * (x + gK * b)
+                new[:, :, c] = f0 * (x + b) + sg(c) * f1 * (x + gK * b)
         v = np.where(live, new, v)
     out = sh.copy()
     out[:, idx] = v
@@ -515,6 +532,43 @@ def test_min_bytes_grouping_emulation_matches_oracle(golden, name):
         got, gls = emulate(bp, fp, params)
         if np.any(want):
             assert rel_l2(got * math.exp(gls), want * math.exp(wls)) < 1e-12
+
+
+@pytest.mark.parametrize("name", ["c1", "small", "c2"])
+def test_touching_run_bases_emulation_matches_oracle(golden, name):
+    """Variant bit 6: register runs whose basis vectors may have other vectors' role coordinates
+    (invertible at the roles) take fewer runs, and, with the representative and the dead entries
+    found by parities of several local bits, give the oracle's environment."""
+    case, arrays = golden(name)
+    bp = P.build_block_plan(arrays["graph"], arrays["unitaries"], case["n"], case["order"],
+                            case["parity_operations"], case["open_vertices"])
+    sp = SliceParams(bp)
+    oe = block_ref.OracleEngine(arrays["graph"], arrays["unitaries"], case["n"], case["order"],
+                                case["parity_operations"], case["open_vertices"])
+    x = np.array([int(c) for c in case["protocol"]["records"][0]["input_data_bits"]], np.uint8)
+    _, items = sp.items(x)
+    slices = [s for s in oe.slice_inputs(x) if s[0]]
+    plain = build_fused_plan(bp, max_dim=13, low=3, variant=12, grouping="bytes")
+    fp = build_fused_plan(bp, max_dim=13, low=3, variant=76, grouping="bytes")
+    fp5 = build_fused_plan(bp, max_dim=13, low=3, variant=92, grouping="bytes")  # dimension 5
+    assert fp.spans == plain.spans == fp5.spans
+    def runs(f, gi):
+        g = f.groups[gi]
+        first, count = int(g["first"]), int(g["count"])
+        return int((f.tile_steps["run_len"][first:first + count] > 0).sum()) if int(g["variant"]) & 4 else None
+    both = [gi for gi in range(len(fp.groups)) if runs(fp, gi) and runs(plain, gi)]
+    assert all(runs(fp, gi) <= runs(plain, gi) for gi in both)
+    if name != "c1":
+        assert any(t1 or t2 for t1, t2, _ in fp.step_touch.values())
+        assert any(runs(fp, gi) < runs(plain, gi) for gi in both)
+    for (coef, params, xor), (ocoef, f, yfix, flips) in list(zip(items, slices))[:2]:
+        want, wls, _ = block_ref.execute(oe.steps, f, yfix, oe.fut, oe.maxslots)
+        for f in (fp, fp5):
+            got, gls = emulate(bp, f, params)
+            if np.any(want):
+                assert rel_l2(got * math.exp(gls), want * math.exp(wls)) < 1e-12
+    with pytest.raises(ValueError):
+        fp.launch_library(None, 0, 0, 0, 1, 0, 0, None)
 
 
 def test_min_bytes_grouping_moves_fewer_bytes(golden):

@@ -105,3 +105,32 @@ def test_packed_form_compiles(golden):
     for src, _ in jit.plan_sources(bp, fp, parts=1):
         assert "jit::pbody" in src
         assert jit.compile_source(lib, src)[:4] == b"\x7fELF"
+
+
+@pytest.mark.parametrize("name", ["small", "c2"])
+def test_touching_run_bases_compile_and_pair_only_even_offsets(golden, name):
+    """Variant bit 6 kernels compile; a run whose basis touches tile bit 0 from another vector
+    (some entries with the pair bit clear at odd offsets) moves single entries, never a 16-byte
+    word at an odd entry."""
+    from dcs245_classical_sampling_b200.fused import run_dim
+    case, arrays = golden(name)
+    bp = P.build_block_plan(arrays["graph"], arrays["unitaries"], case["n"], case["order"],
+                            case["parity_operations"], case["open_vertices"])
+    lib = _lib.load()
+    odd = 0
+    for variant in (76, 92):
+        fp = build_fused_plan(bp, max_dim=13, low=3, variant=variant, grouping="bytes", prefetch_kb=16)
+        for gi, g in enumerate(fp.groups):
+            if not int(g["variant"]) & 4:
+                continue
+            R = run_dim(int(g["variant"]))
+            for s, _ in jit._group_runs(fp, gi):
+                offs = fp.run_off[int(g["first"]) + s]
+                k0 = jit.pair_bit(offs, R)
+                raw = next((k for k in range(R) if int(offs[1 << k]) == 1), None)
+                odd += raw is not None and k0 is None
+                if k0 is not None:
+                    assert all(int(offs[j]) % 2 == 0 for j in range(1 << R) if not (j >> k0) & 1)
+        for src, _ in jit.plan_sources(bp, fp, minb=2, parts=1):
+            assert jit.compile_source(lib, src)[:4] == b"\x7fELF"
+    assert odd  # the case the guard exists for
