@@ -541,6 +541,49 @@ __device__ __forceinline__ void sign_bits(const uint64_t* beta, uint64_t base, c
     }
 }
 
+// The tile's sign bits computed by every warp for itself (kernels with the split barrier between
+// tiles share no per-tile word between warps).
+template <int COUNT>
+__device__ __forceinline__ uint32_t warp_sign_bits(const uint64_t* beta, uint64_t base, const int* ovy) {
+    const int s = threadIdx.x & 31;
+    const int bit = s < COUNT ? ((__popcll(base & beta[s]) & 1) ^ (ovy[s] & 1)) : 0;
+    return __ballot_sync(0xffffffffu, bit);
+}
+
+// Split barrier between tiles (shared-memory mbarrier, one arrival per thread per tile): a thread
+// arrives once it has read the tile buffer for the last time in a tile, and waits for the
+// previous tile's phase only before its first write into the buffer in the next tile, so no
+// thread waits at a tile's start.  The wait gives up after kWaitLimit polls and reports it.
+constexpr int kWaitLimit = 1 << 22;
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    const uint32_t a = (uint32_t)__cvta_generic_to_shared(bar);
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(a), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    const uint32_t a = (uint32_t)__cvta_generic_to_shared(bar);
+    asm volatile("{\n .reg .b64 st;\n mbarrier.arrive.shared::cta.b64 st, [%0];\n}\n" ::"r"(a) : "memory");
+}
+// true once the phase of the given parity has completed; false if kWaitLimit polls did not see it
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+    const uint32_t a = (uint32_t)__cvta_generic_to_shared(bar);
+    for (int i = 0; i < kWaitLimit; ++i) {
+        uint32_t done;
+        asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+                     " selp.u32 %0, 1, 0, p;\n}\n"
+                     : "=r"(done)
+                     : "r"(a), "r"(parity)
+                     : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+// a wait that gave up: flag 4 in the item's scale, and a NaN block max, so that every consumer of
+// the table (the next group's prologue, the block's flags, the draw) sees an invalid result
+__device__ __forceinline__ void wait_failed(jit_scale* scale, real_t& lm) {
+    atomicOr(&scale->flags, 4u);
+    lm = (real_t)__int_as_float(0x7fc00000);
+}
+
 __device__ __forceinline__ void block_max(real_t lm, unsigned long long* maxbits, int slot) {
     __shared__ unsigned long long red[32];
     unsigned long long v = max_key(lm);

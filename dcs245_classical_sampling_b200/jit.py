@@ -296,6 +296,14 @@ def group_source(plan, fp, gi, minb=3, threads=256, kb=None):
              f"{'false' if lay is not None else 'true'}>(params, g{gi}_basis, maxbits, {gi}, scale, fw, ovy, hi_tab);")
     L.append("    real_t lm = 0;")
     L.append("    uint32_t par = 0;")
+    # between tiles, a split barrier (arrive after a tile's last shared-memory reads, wait before
+    # the next tile's first shared-memory writes) instead of a barrier at every tile's start
+    tilebar = direct and uses_tile_buffer(fp, gi)
+    if tilebar:
+        L.append("    __shared__ uint64_t tile_bar;")
+        L.append(f"    if (threadIdx.x == 0) jit::mbar_init(&tile_bar, {threads}u);")
+        L.append("    __syncthreads();")
+        L.append("    uint32_t tile_it = 0;")
     if lay is not None:
         # the first run's thread representative, and the copies of a tile's staged entries
         NBT = lay["NBT"]
@@ -337,7 +345,9 @@ def group_source(plan, fp, gi, minb=3, threads=256, kb=None):
         L.extend(prefetch("(uint64_t)blockIdx.x", "    "))
     L.append(f"    for (uint64_t tile = blockIdx.x; tile < {ntiles}; tile += gridDim.x) {{")
     L.append(f"        const uint64_t base = {_deposit_expr(g)};")
-    if direct:
+    if tilebar or (direct and not uses_tile_buffer(fp, gi)):  # one-run kernels share no buffer
+        L.append(f"        const uint32_t csm = jit::warp_sign_bits<COUNT>(g{gi}_beta, base, ovy);")
+    elif direct:
         L.append(f"        jit::sign_bits<COUNT>(g{gi}_beta, base, ovy, &cs_sh[par]);")
         L.append("        __syncthreads();")
     else:
@@ -346,7 +356,8 @@ def group_source(plan, fp, gi, minb=3, threads=256, kb=None):
         L.append(f"        jit::sign_bits<COUNT>(g{gi}_beta, base, ovy, &cs_sh[par]);")
         L.append('        asm volatile("cp.async.wait_all;\\n" ::: "memory");')
         L.append("        __syncthreads();")
-    L.append("        const uint32_t csm = cs_sh[par];")
+    if not (tilebar or (direct and not uses_tile_buffer(fp, gi))):
+        L.append("        const uint32_t csm = cs_sh[par];")
     L.append("        unsigned char* shb = smem;")
     if direct:
         L.append(f"        if (!(base & {_u64(fp.tile_steps[first]['cskip'])})) {{")
@@ -466,6 +477,9 @@ def group_source(plan, fp, gi, minb=3, threads=256, kb=None):
                 else:
                     call = f"jit::body4<{R}, {k1}, {k2}, {mix}, {B}, {dead}, {sk}, {ska}{tch4}>{args};"
                 L.append(f"                    {call}")
+        if tilebar and ri == 0:  # the previous tile's last reads of the buffer are done
+            L.append("                    if (tile_it && !jit::mbar_wait(&tile_bar, (tile_it - 1u) & 1u)) "
+                     "jit::wait_failed(scale, lm);")
         for c in cos:
             if dst_g:
                 if pairs and pair_out:
@@ -501,6 +515,9 @@ def group_source(plan, fp, gi, minb=3, threads=256, kb=None):
             L.extend(prefetch("tile + gridDim.x", "            "))
         L.append("        }")
         L.append("        par ^= 1u;")
+        if tilebar:
+            L.append("        jit::mbar_arrive(&tile_bar);")
+            L.append("        ++tile_it;")
     else:
         L.append(f"        lm = jit::store_tile<T, LOW, {'true' if pair_out else 'false'}>(E, sh, hi_tab, base, "
                  f"{_u64(out_inact)}, sc, lm);")
