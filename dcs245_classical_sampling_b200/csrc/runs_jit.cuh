@@ -554,7 +554,10 @@ __device__ __forceinline__ uint32_t warp_sign_bits(const uint64_t* beta, uint64_
 // arrives once it has read the tile buffer for the last time in a tile, and waits for the
 // previous tile's phase only before its first write into the buffer in the next tile, so no
 // thread waits at a tile's start.  The wait gives up after kWaitLimit polls and reports it.
-constexpr int kWaitLimit = 1 << 22;
+#ifndef DCS_JIT_WAIT_LIMIT
+#define DCS_JIT_WAIT_LIMIT (1 << 22)
+#endif
+constexpr int kWaitLimit = DCS_JIT_WAIT_LIMIT;
 __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
     const uint32_t a = (uint32_t)__cvta_generic_to_shared(bar);
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(a), "r"(count) : "memory");

@@ -65,6 +65,16 @@ def device_steps(steps):
     return out
 
 
+def raise_for_flags(flags):
+    """The errors an item's scale flags report: bit 2, a generated kernel's bounded wait between
+    tiles gave up (the block is invalid); bit 0, a nonfinite table (the reference's error)."""
+    flags = np.asarray(flags)
+    if np.any(flags & 4):
+        raise RuntimeError("a group kernel's wait between tiles gave up; the block is invalid")
+    if np.any(flags & 1):
+        raise ArithmeticError("Nonfinite in-place environment")
+
+
 def pack_runs(slots):
     runs = deposit_runs(slot_mask(slots))
     arr = np.zeros(max(1, len(runs)), dtype=np.uint32)
@@ -566,17 +576,14 @@ class InplaceConditionalBlockGPU:
 
     def check_scale_flags(self, n_items=None):
         """Raise the reference's ArithmeticError if the last chunk saw a nonfinite table."""
-        sc = self._sc()[: n_items or self.items, 2].cpu().numpy()
-        if np.any(sc & 1):
-            raise ArithmeticError("Nonfinite in-place environment")
+        raise_for_flags(self._sc()[: n_items or self.items, 2].cpu().numpy())
 
     def _run(self, x_list, w=None, part=0, parts=1):
         prep = self.prepare(x_list, w, part, parts)
         out = torch.empty((len(x_list), 1 << self.k), dtype=torch.complex128, device=self.device)
         flags = self._flags_tensor()
         self.enqueue(prep, out, flags)
-        if bool(((flags & 1) != 0).any()):  # one small device->host read per call
-            raise ArithmeticError("Nonfinite in-place environment")
+        raise_for_flags(flags.cpu().numpy())  # one small device->host read per call
         return out, prep
 
     def block(self, x_bits, w=None, part=0, parts=1):

@@ -197,7 +197,7 @@ def _fixmask(fp, first, count):
     return m
 
 
-def group_source(plan, fp, gi, minb=3, threads=256, kb=None):
+def group_source(plan, fp, gi, minb=3, threads=256, kb=None, wait_check=False):
     """CUDA source of the kernel of group gi (``dcs_g<gi>``); None if the group has no runs.
 
     Direct I/O (``fp.direct_io``, the default): the first run of a tile loads its cosets from
@@ -301,7 +301,9 @@ def group_source(plan, fp, gi, minb=3, threads=256, kb=None):
     tilebar = direct and uses_tile_buffer(fp, gi)
     if tilebar:
         L.append("    __shared__ uint64_t tile_bar;")
-        L.append(f"    if (threadIdx.x == 0) jit::mbar_init(&tile_bar, {threads}u);")
+        # wait_check (tests only): a phase of 64 tiles' arrivals, which a test plan never completes,
+        # so every wait gives up
+        L.append(f"    if (threadIdx.x == 0) jit::mbar_init(&tile_bar, {threads * (64 if wait_check else 1)}u);")
         L.append("    __syncthreads();")
         L.append("    uint32_t tile_it = 0;")
     if lay is not None:
@@ -699,14 +701,14 @@ def group_config(group_cfg, gi, minb, threads):
     return (c[0], c[1], c[2] if len(c) > 2 else threads)
 
 
-def plan_sources(plan, fp, minb=3, parts=8, threads=256, group_cfg=None):
+def plan_sources(plan, fp, minb=3, parts=8, threads=256, group_cfg=None, wait_check=False):
     """Translation units (source strings) holding the group kernels, spread over `parts` units
     so that NVRTC compiles them in parallel; returns [(source, [group indices])].  group_cfg:
     {group: (CTAs per SM of its registers, staging KiB[, threads per CTA])} overriding minb, the
     plan's prefetch_kb and `threads` for that group (a unit holds kernels of one thread count)."""
     groups = [gi for gi in range(len(fp.groups)) if int(fp.groups[gi]["variant"]) & 4]
     cfg = {gi: group_config(group_cfg, gi, minb, threads) for gi in groups}
-    bodies = {gi: group_source(plan, fp, gi, cfg[gi][0], cfg[gi][2], cfg[gi][1]) for gi in groups}
+    bodies = {gi: group_source(plan, fp, gi, cfg[gi][0], cfg[gi][2], cfg[gi][1], wait_check) for gi in groups}
     out = []
     for nt in sorted({c[2] for c in cfg.values()}):
         mine = [gi for gi in groups if cfg[gi][2] == nt]
@@ -718,7 +720,7 @@ def plan_sources(plan, fp, minb=3, parts=8, threads=256, group_cfg=None):
         for gis, _ in units:
             if not gis:
                 continue
-            src = (f"#define DCS_JIT_THREADS {nt}\n" +
+            src = (f"#define DCS_JIT_THREADS {nt}\n" + ("#define DCS_JIT_WAIT_LIMIT 4096\n" if wait_check else "") +
                    ("#define DCS_JIT_FP64 1\n" if getattr(fp, "fp64", False) else "") +
                    '#include "runs_jit.cuh"\n\n' + "\n".join(bodies[gi] for gi in sorted(gis)))
             out.append((src, sorted(gis)))
@@ -751,10 +753,10 @@ def compile_source(lib, source, name="dcs_plan.cu"):
     return data
 
 
-def compile_plan(plan, fp, lib=None, minb=3, parts=8, threads=256, group_cfg=None):
+def compile_plan(plan, fp, lib=None, minb=3, parts=8, threads=256, group_cfg=None, wait_check=False):
     """[(cubin, [group indices])] for a fused plan (NVRTC in parallel threads)."""
     lib = lib or _lib.load()
-    units = plan_sources(plan, fp, minb, parts, threads, group_cfg)
+    units = plan_sources(plan, fp, minb, parts, threads, group_cfg, wait_check)
     with ThreadPoolExecutor(max_workers=len(units) or 1) as ex:
         images = list(ex.map(lambda u: compile_source(lib, u[0], f"dcs_plan_{u[1][0]}.cu"), units))
     return [(img, gis) for img, (_, gis) in zip(images, units)]
@@ -763,10 +765,11 @@ def compile_plan(plan, fp, lib=None, minb=3, parts=8, threads=256, group_cfg=Non
 class JitPlan:
     """Loaded group kernels of one fused plan (current CUDA device)."""
 
-    def __init__(self, plan, fp, lib=None, minb=None, parts=8, threads=256, group_cfg=None):
+    def __init__(self, plan, fp, lib=None, minb=None, parts=8, threads=256, group_cfg=None, wait_check=False):
         """minb: CTAs per SM the registers are sized for (default: 2 if the plan's variant has
         bit 0, else 3).  group_cfg: {group: (minb, staging KiB[, threads])} for groups that
-        differ."""
+        differ.  wait_check (tests only): every wait between tiles gives up after 4096 polls,
+        to check that such a wait ends and reports itself."""
         self.lib = lib or _lib.load()
         self.fp = fp
         self.kernels = {}
@@ -782,7 +785,7 @@ class JitPlan:
             missing = [gi for gi in range(len(fp.groups)) if not int(fp.groups[gi]["variant"]) & 4]
             if missing:  # the library's fused kernels store complex64 only
                 raise ValueError(f"complex128 fused plan: groups {missing} have no register runs")
-        for img, gis in compile_plan(plan, fp, self.lib, minb, parts, self.threads, self.group_cfg):
+        for img, gis in compile_plan(plan, fp, self.lib, minb, parts, self.threads, self.group_cfg, wait_check):
             buf = ctypes.create_string_buffer(img, len(img))
             self._images.append(buf)
             handle = ctypes.c_void_p()

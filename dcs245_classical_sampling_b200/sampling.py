@@ -201,8 +201,8 @@ def sample_checked(engine, x_list, uniforms, hashes=True, exact_cdf=False, strad
 
     def finish(i, slot):
         copied[slot].synchronize()
-        if bool((host_flags[slot] & 1).any()):
-            raise ArithmeticError("Nonfinite in-place environment")
+        from .engine import raise_for_flags
+        raise_for_flags(host_flags[slot].numpy())
         rec = record_dict(host_res[slot].numpy().view(_lib.DRAW_DTYPE)[0], straddle_rel_l2)
         if hashes:
             rec.update(block_hashes(host_blk[slot].numpy()))

@@ -241,3 +241,22 @@ def test_touching_run_bases_are_bit_identical(golden, name):
     with pytest.raises(ValueError, match="touching"):
         eng.set_fused_config(variant=76, jit=False)
         eng.block(xs[0])
+
+
+def test_wait_between_tiles_gives_up_and_reports(golden):
+    """A generated kernel whose wait between tiles can never be satisfied (a test build: the
+    barrier's phase needs 64 tiles' arrivals) ends every wait after its poll limit, and the engine
+    raises instead of returning the block; the engine then runs normally again."""
+    from dcs245_classical_sampling_b200.jit import JitPlan
+    case, arrays = golden("c2")
+    eng = _engine(case, arrays, np.complex64, "fused", jit_shape=True)
+    x = _x(case["protocol"]["records"][0])
+    want = eng.block(x)[0].cpu().numpy()
+    good = eng.fplan.jit
+    eng.fplan.jit = JitPlan(eng.plan, eng.fplan, eng.lib, minb=good.minb, threads=good.threads,
+                            group_cfg=good.group_cfg, wait_check=True)
+    with pytest.raises(RuntimeError, match="gave up"):
+        eng.block(x)
+    eng.fplan.jit.close()
+    eng.fplan.jit = good
+    assert np.array_equal(eng.block(x)[0].cpu().numpy(), want)

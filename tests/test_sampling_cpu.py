@@ -79,3 +79,14 @@ def test_straddle_margin_bounds_the_cdf_shift():
             shift = np.max(np.abs(np.cumsum(pa) / pa.sum() - np.cumsum(pb) / pb.sum()))
             assert shift <= 2 * r
     assert sampling.CDF_SHIFT_BOUND == 2 * sampling.COMPLEX64_REL_L2
+
+
+def test_scale_flags_raise_the_right_error():
+    """Bit 0 of an item's scale flags is the reference's nonfinite error; bit 2 a generated
+    kernel's wait between tiles that gave up."""
+    from dcs245_classical_sampling_b200.engine import raise_for_flags
+    raise_for_flags(np.array([0, 2], np.int64))
+    with pytest.raises(ArithmeticError, match="Nonfinite"):
+        raise_for_flags(np.array([0, 1], np.int64))
+    with pytest.raises(RuntimeError, match="gave up"):
+        raise_for_flags(np.array([5, 0], np.int64))
