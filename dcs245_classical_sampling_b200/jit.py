@@ -455,6 +455,8 @@ def group_source(plan, fp, gi, minb=3, threads=256, kb=None, wait_check=False):
             else:
                 for j, o in enumerate(offs):
                     L.append(f"                    v{c}[{j}] = *reinterpret_cast<const cplx_t*>(shb + {sh_off(c, o)});")
+        if tilebar and dst_g:  # this thread's last reads of the buffer in this tile
+            L.append(f"                    if (k == {niter // len(cos) - 1}) jit::mbar_arrive(&tile_bar);")
         for i in range(n):
             si = s + i
             st = fp.tile_steps[first + si]
@@ -504,6 +506,9 @@ def group_source(plan, fp, gi, minb=3, threads=256, kb=None, wait_check=False):
                 for j, o in enumerate(offs):
                     L.append(f"                    *reinterpret_cast<cplx_t*>(shb + {sh_off(c, o)}) = v{c}[{j}];")
         L.append("                }")
+        if tilebar and dst_g:  # threads without a coset in the last run read nothing of it
+            L.append("            } else {")
+            L.append("                jit::mbar_arrive(&tile_bar);")
         L.append("            }")
         if src_g and lay is not None:  # every staged entry is in registers: stage the next tile
             L.extend(prefetch("tile + gridDim.x", "            "))
@@ -512,13 +517,15 @@ def group_source(plan, fp, gi, minb=3, threads=256, kb=None, wait_check=False):
         if not dst_g:
             L.append("        __syncthreads();")
     if direct:
-        if lay is not None:
+        if lay is not None or tilebar:  # a skipped tile: stage the next one, arrive for this one
             L.append("        } else {")
-            L.extend(prefetch("tile + gridDim.x", "            "))
+            if lay is not None:
+                L.extend(prefetch("tile + gridDim.x", "            "))
+            if tilebar:
+                L.append("            jit::mbar_arrive(&tile_bar);")
         L.append("        }")
         L.append("        par ^= 1u;")
         if tilebar:
-            L.append("        jit::mbar_arrive(&tile_bar);")
             L.append("        ++tile_it;")
     else:
         L.append(f"        lm = jit::store_tile<T, LOW, {'true' if pair_out else 'false'}>(E, sh, hi_tab, base, "
