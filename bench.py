@@ -919,7 +919,8 @@ def profile_case(argv):
     ap.add_argument("--minb", type=int, default=None, help="generated kernels: CTAs per SM for the registers")
     ap.add_argument("--fp64", action="store_true", help="complex128 table, FP64 generated kernels (the audits)")
     ap.add_argument("--kernel-cfg", default=None,
-                    help="generated kernels of every group as MINB/STAGING_KB/RUN_DIM, e.g. 2/16/5")
+                    help="generated kernels of every group as MINB/STAGING_KB/RUN_DIM[/THREADS], e.g. 2/16/5; "
+                         "RUN_DIM 4t or 5t: run bases that may touch other roles")
     ap.add_argument("--storage", default=None, choices=["float16"],
                     help="binary16 tables with FP64 arithmetic (device mode)")
     a = ap.parse_args(argv)
@@ -955,14 +956,20 @@ def profile_case(argv):
     sub = P.BlockPlan(**{**bp.__dict__, "steps": steps})
     if a.mode == "fused":
         variant, minb, kb = a.variant, a.minb, a.prefetch_kb
+        threads = 256
         if a.kernel_cfg:
-            minb, kb, rdim = (int(x) for x in a.kernel_cfg.split("/"))
-            variant = (variant | 16) if rdim == 5 else (variant & ~16)
+            parts = a.kernel_cfg.split("/")
+            minb, kb = int(parts[0]), int(parts[1])
+            rdim = parts[2]
+            variant = (variant | 16) if rdim.startswith("5") else (variant & ~16)
+            variant = (variant | 64) if rdim.endswith("t") else (variant & ~64)
+            if len(parts) > 3:
+                threads = int(parts[3])
         fp = build_fused_plan(sub, max_dim=a.max_dim, low=a.low, variant=variant, pairs=a.pairs,
                               grouping=a.grouping, fp64=a.fp64, prefetch_kb=kb)
         if a.jit:
             from dcs245_classical_sampling_b200.jit import JitPlan
-            fp.jit = JitPlan(sub, fp, lib, minb=minb)
+            fp.jit = JitPlan(sub, fp, lib, minb=minb, threads=threads)
         nmax = len(fp.groups)
     else:
         dsteps = device_steps(steps)
