@@ -134,3 +134,33 @@ def test_touching_run_bases_compile_and_pair_only_even_offsets(golden, name):
         for src, _ in jit.plan_sources(bp, fp, minb=2, parts=1):
             assert jit.compile_source(lib, src)[:4] == b"\x7fELF"
     assert odd  # the case the guard exists for
+
+
+@pytest.mark.parametrize("name", ["small", "c2"])
+@pytest.mark.parametrize("kb", [0, 16])
+def test_split_barrier_between_tiles_structure(golden, name, kb):
+    """Every generated kernel with a tile buffer arrives once per thread per tile on the split
+    barrier (after the last run's buffer loads; threads without a coset in that run and skipped
+    tiles at once) and waits once, before the first run's buffer writes; no kernel has a barrier
+    at the tile's start, and one-run kernels have none in the tile loop."""
+    case, arrays = golden(name)
+    bp = P.build_block_plan(arrays["graph"], arrays["unitaries"], case["n"], case["order"],
+                            case["parity_operations"], case["open_vertices"])
+    fp = build_fused_plan(bp, max_dim=13, low=3, variant=28, grouping="bytes", prefetch_kb=kb)
+    seen = 0
+    for gi in range(len(fp.groups)):
+        src = jit.group_source(bp, fp, gi, 2, 256, kb)
+        if src is None:
+            continue
+        loop = src[src.index("for (uint64_t tile"):src.index("jit::block_max")]
+        nruns = len(jit._group_runs(fp, gi))
+        assert "sign_bits<COUNT>(g" not in loop or "warp_sign_bits" in loop
+        if jit.uses_tile_buffer(fp, gi):
+            seen += 1
+            assert loop.count("jit::mbar_arrive(&tile_bar)") == 3
+            assert loop.count("jit::mbar_wait(&tile_bar") == 1
+            assert loop.count("__syncthreads();") == nruns - 1  # between runs only
+            assert loop.index("jit::mbar_wait") < loop.index("__syncthreads();")
+        else:
+            assert "__syncthreads" not in loop and "mbar_" not in loop
+    assert seen
